@@ -1,0 +1,424 @@
+// C ABI of the engine: graph handles, decomposition and result access.
+// Each function names the reference entry point it stands in for; the
+// declarations with full documentation are in include/dcore_b200.h.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <sys/stat.h>
+
+#include "dc_engine.cuh"
+#include "dc_internal.h"
+
+using namespace dc;
+
+#define API_CUDA(call)                                                                       \
+    do {                                                                                     \
+        cudaError_t _e = (call);                                                             \
+        if (_e != cudaSuccess)                                                               \
+            return set_error(DC_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(_e));  \
+    } while (0)
+
+namespace {
+
+int select_device(const dc_graph_opts* o) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return set_error(DC_ERR_NO_DEVICE,
+                         "no CUDA device available (%s); the engine runs on the GPU only and has no CPU fallback",
+                         e == cudaSuccess ? "device count is 0" : cudaGetErrorString(e));
+    }
+    if (o && o->device >= 0) {
+        if (o->device >= n) return set_error(DC_ERR_INVALID, "device %d out of range (%d devices)", o->device, n);
+        API_CUDA(cudaSetDevice(o->device));
+    }
+    return DC_OK;
+}
+
+int new_handle(const dc_graph_opts* o, dc_graph** out) {
+    if (!out) return set_error(DC_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    if (int rc = select_device(o)) return rc;
+    dc_graph* h = new dc_graph();
+    dc_graph_opts def;
+    dc_graph_opts_default(&def);
+    if (!o) o = &def;
+    h->gap_min = o->gap_min;
+    h->gap_div = o->gap_div;
+    if (int rc = init_handle(h)) {
+        dc_graph_free(h);
+        return rc;
+    }
+    *out = h;
+    return DC_OK;
+}
+
+bool file_exists(const std::string& p) {
+    struct stat st;
+    return stat(p.c_str(), &st) == 0 && S_ISREG(st.st_mode);
+}
+
+}  // namespace
+
+extern "C" void dc_graph_opts_default(dc_graph_opts* o) {
+    if (!o) return;
+    o->gap_min = 1;  // OFFSET_GAP (src/common.h:36)
+    o->gap_div = 0;
+    o->device = -1;
+}
+
+extern "C" int dc_device_count(int* n) {
+    if (!n) return set_error(DC_ERR_INVALID, "null argument");
+    *n = 0;
+    cudaError_t e = cudaGetDeviceCount(n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *n = 0;
+    }
+    return DC_OK;
+}
+
+extern "C" int dc_graph_create_device(uint32_t V, uint64_t E, const uint32_t* d_src, const uint32_t* d_dst,
+                                      const dc_graph_opts* opts, dc_graph** out) {
+    if (E && (!d_src || !d_dst)) return set_error(DC_ERR_INVALID, "dc_graph_create_device: null edge arrays");
+    dc_graph* h = nullptr;
+    if (int rc = new_handle(opts, &h)) return rc;
+    if (int rc = build_from_device_edges(h, V, E, d_src, d_dst)) {
+        dc_graph_free(h);
+        return rc;
+    }
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        dc_graph_free(h);
+        return set_error(DC_ERR_CUDA, "graph build: %s", cudaGetErrorString(e));
+    }
+    *out = h;
+    return DC_OK;
+}
+
+extern "C" int dc_graph_create(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst,
+                               const dc_graph_opts* opts, dc_graph** out) {
+    if (E && (!src || !dst)) return set_error(DC_ERR_INVALID, "dc_graph_create: null edge arrays");
+    dc_graph* h = nullptr;
+    if (int rc = new_handle(opts, &h)) return rc;
+    uint32_t *d_src = nullptr, *d_dst = nullptr;
+    size_t bytes = (E ? E : 1) * sizeof(uint32_t);
+    if (cudaMalloc(&d_src, bytes) != cudaSuccess || cudaMalloc(&d_dst, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        if (d_src) cudaFree(d_src);
+        dc_graph_free(h);
+        return set_error(DC_ERR_NOMEM, "dc_graph_create: cannot stage %llu edges on the device", (unsigned long long)E);
+    }
+    int rc = DC_OK;
+    if (E) {
+        if (cudaMemcpyAsync(d_src, src, E * 4, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+            cudaMemcpyAsync(d_dst, dst, E * 4, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+            rc = set_error(DC_ERR_CUDA, "dc_graph_create: edge upload failed");
+    }
+    if (rc == DC_OK) rc = build_from_device_edges(h, V, E, d_src, d_dst);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_src);
+    cudaFree(d_dst);
+    if (rc == DC_OK && e != cudaSuccess) rc = set_error(DC_ERR_CUDA, "graph build: %s", cudaGetErrorString(e));
+    if (rc != DC_OK) {
+        dc_graph_free(h);
+        return rc;
+    }
+    *out = h;
+    return DC_OK;
+}
+
+// Graph(const string&) (src/graph.cpp:381-395): use the binary cache
+// "<path>-binary-g=<gap>" when present, else parse the text file.  A path
+// that itself names a "-binary-g=" file is read as binary.
+extern "C" int dc_graph_load(const char* path, int prune, const dc_graph_opts* opts, dc_graph** out) {
+    if (!path || !out) return set_error(DC_ERR_INVALID, "dc_graph_load: null argument");
+    dc_graph_opts def;
+    dc_graph_opts_default(&def);
+    const dc_graph_opts* o = opts ? opts : &def;
+    std::string p(path);
+    std::string cache = p + "-binary-g=" + std::to_string(o->gap_min);
+    std::string bin;
+    if (p.find("-binary-g=") != std::string::npos) bin = p;
+    else if (file_exists(cache)) bin = cache;
+    if (!bin.empty()) {
+        BinaryGraph b;
+        if (int rc = read_binary_graph(bin.c_str(), b)) return rc;
+        std::vector<uint32_t> s(b.E), d(b.E);
+        uint64_t e = 0;
+        for (uint32_t v = 0; v < b.V; ++v)
+            for (int32_t i = 0; i < b.out_deg[v]; ++i) {
+                s[e] = v;
+                d[e] = b.out_nbr[b.out_off[v] + i];
+                ++e;
+            }
+        return dc_graph_create(b.V, b.E, s.data(), d.data(), o, out);
+    }
+    uint32_t V = 0;
+    std::vector<uint32_t> s, d;
+    if (int rc = parse_text_graph(path, prune, &V, s, d)) return rc;
+    return dc_graph_create(V, s.size(), s.data(), d.data(), o, out);
+}
+
+extern "C" int dc_graph_free(dc_graph* h) {
+    if (!h) return DC_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_graph_arrays(h->g);
+    free_decomp(h->d);
+    free_scratch(h);
+    if (h->ctl) cudaFree(h->ctl);
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return DC_OK;
+}
+
+extern "C" int dc_graph_info(const dc_graph* h, uint32_t* V, uint64_t* E) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    if (V) *V = h->g.V;
+    if (E) *E = h->g.E;
+    return DC_OK;
+}
+
+extern "C" int dc_graph_degrees(dc_graph* h, int32_t* in_deg, int32_t* out_deg) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    if (in_deg) API_CUDA(cudaMemcpyAsync(in_deg, h->g.in_len, 4ull * h->g.V, cudaMemcpyDeviceToHost, h->stream));
+    if (out_deg) API_CUDA(cudaMemcpyAsync(out_deg, h->g.out_len, 4ull * h->g.V, cudaMemcpyDeviceToHost, h->stream));
+    API_CUDA(cudaStreamSynchronize(h->stream));
+    return DC_OK;
+}
+
+// Live edges of the device graph as (src, dst) pairs, src ascending, each
+// out-list in ascending dst order.
+extern "C" int dc_graph_get_edges(dc_graph* h, uint32_t* src, uint32_t* dst, uint64_t capacity, uint64_t* n_edges) {
+    if (!h || !n_edges) return set_error(DC_ERR_INVALID, "null argument");
+    const uint32_t V = h->g.V;
+    std::vector<uint32_t> off((size_t)V + 1), nbr(h->g.out_cap ? h->g.out_cap : 1);
+    std::vector<int32_t> len(V ? V : 1);
+    if (V) {
+        API_CUDA(cudaMemcpyAsync(off.data(), h->g.out_off, 4ull * (V + 1), cudaMemcpyDeviceToHost, h->stream));
+        API_CUDA(cudaMemcpyAsync(len.data(), h->g.out_len, 4ull * V, cudaMemcpyDeviceToHost, h->stream));
+        if (h->g.out_cap)
+            API_CUDA(cudaMemcpyAsync(nbr.data(), h->g.out_nbr, 4ull * h->g.out_cap, cudaMemcpyDeviceToHost, h->stream));
+    }
+    API_CUDA(cudaStreamSynchronize(h->stream));
+    uint64_t E = 0;
+    for (uint32_t v = 0; v < V; ++v) E += (uint64_t)len[v];
+    *n_edges = E;
+    if (!src || !dst) return DC_OK;
+    if (capacity < E) return set_error(DC_ERR_CAPACITY, "dc_graph_get_edges: capacity too small");
+    uint64_t e = 0;
+    for (uint32_t v = 0; v < V; ++v) {
+        uint32_t* a = nbr.data() + off[v];
+        std::sort(a, a + len[v]);
+        for (int32_t i = 0; i < len[v]; ++i) {
+            src[e] = v;
+            dst[e] = a[i];
+            ++e;
+        }
+    }
+    return DC_OK;
+}
+
+// Graph::writeBinary (src/graph.cpp:261-285).
+extern "C" int dc_graph_write_binary(dc_graph* h, const char* path, uint32_t gap) {
+    if (!h || !path) return set_error(DC_ERR_INVALID, "null argument");
+    uint64_t E = 0;
+    if (int rc = dc_graph_get_edges(h, nullptr, nullptr, 0, &E)) return rc;
+    std::vector<uint32_t> s(E ? E : 1), d(E ? E : 1);
+    if (int rc = dc_graph_get_edges(h, s.data(), d.data(), E, &E)) return rc;
+    return write_binary_graph(path, h->g.V, E, s.data(), d.data(), gap);
+}
+
+// dcore(Graph&) (main.cu:197-262) / checkDCore (main.cu:276-293).
+extern "C" int dc_decompose(dc_graph* h, int method, int32_t* kmax, int32_t* lmax) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    if (method != DC_METHOD_INCREMENTAL && method != DC_METHOD_PEEL)
+        return set_error(DC_ERR_INVALID, "unknown decomposition method %d", method);
+    API_CUDA(cudaSetDevice(h->device));
+    if (int rc = decompose(h, method, 0)) return rc;
+    if (kmax) *kmax = h->d.kmax;
+    if (lmax) *lmax = h->d.lmax;
+    return DC_OK;
+}
+
+extern "C" int dc_decomp_info_get(dc_graph* h, dc_decomp_info* info) {
+    if (!h || !info) return set_error(DC_ERR_INVALID, "null argument");
+    if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    memset(info, 0, sizeof(*info));
+    info->kmax = h->d.kmax;
+    info->lmax = h->d.lmax;
+    info->n_corners = h->d.n_corners;
+    info->kmax_ms = h->times.kmax_ms;
+    info->row0_ms = h->times.row0_ms;
+    info->rows_ms = h->times.trans_ms;
+    info->skyline_ms = h->times.sky_ms;
+    info->expand_ms = h->times.expand_ms;
+    info->evals = h->stat_evals;
+    info->drops = h->stat_drops;
+    return DC_OK;
+}
+
+extern "C" int dc_get_kmaxes(dc_graph* h, int32_t* out) {
+    if (!h || !out) return set_error(DC_ERR_INVALID, "null argument");
+    if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    if (h->g.V) API_CUDA(cudaMemcpyAsync(out, h->d.kmax_v, 4ull * h->g.V, cudaMemcpyDeviceToHost, h->stream));
+    API_CUDA(cudaStreamSynchronize(h->stream));
+    return DC_OK;
+}
+
+extern "C" int dc_get_lmax_rows_device(dc_graph* h, uint32_t k0, uint32_t n, int32_t* d_out) {
+    if (!h || (n && !d_out)) return set_error(DC_ERR_INVALID, "null argument");
+    if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    if ((uint64_t)k0 + n > (uint64_t)h->d.kmax + 1)
+        return set_error(DC_ERR_INVALID, "rows [%u, %llu) outside 0..kmax=%d", k0, (unsigned long long)k0 + n, h->d.kmax);
+    if (h->d.rows_valid) {
+        if (n)
+            API_CUDA(cudaMemcpyAsync(d_out, h->d.rows + (uint64_t)k0 * h->g.V, 4ull * n * h->g.V,
+                                     cudaMemcpyDeviceToDevice, h->stream));
+        return DC_OK;
+    }
+    return expand_rows(h, k0, n, d_out);
+}
+
+// The rows of g.lmaxes (main.cu:226-247) copied to host memory.
+extern "C" int dc_get_lmax_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* out) {
+    if (!h || (n && !out)) return set_error(DC_ERR_INVALID, "null argument");
+    if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    if ((uint64_t)k0 + n > (uint64_t)h->d.kmax + 1)
+        return set_error(DC_ERR_INVALID, "rows [%u, %llu) outside 0..kmax=%d", k0, (unsigned long long)k0 + n, h->d.kmax);
+    const uint64_t V = h->g.V;
+    if (n == 0 || V == 0) return DC_OK;
+    if (h->d.rows_valid) {
+        API_CUDA(cudaMemcpyAsync(out, h->d.rows + (uint64_t)k0 * V, 4ull * n * V, cudaMemcpyDeviceToHost, h->stream));
+        API_CUDA(cudaStreamSynchronize(h->stream));
+        return DC_OK;
+    }
+    // expand in chunks of rows through two device staging buffers
+    uint64_t chunk_rows = std::max<uint64_t>(1, (256ull << 20) / (4 * V));
+    chunk_rows = std::min<uint64_t>(chunk_rows, n);
+    int32_t* stage[2] = {nullptr, nullptr};
+    for (int i = 0; i < 2; ++i)
+        if (cudaMalloc(&stage[i], 4 * chunk_rows * V) != cudaSuccess) {
+            cudaGetLastError();
+            if (stage[0]) cudaFree(stage[0]);
+            return set_error(DC_ERR_NOMEM, "row staging buffer allocation failed");
+        }
+    int rc = DC_OK;
+    int b = 0;
+    for (uint64_t r = 0; r < n && rc == DC_OK; r += chunk_rows, b ^= 1) {
+        uint64_t m = std::min<uint64_t>(chunk_rows, n - r);
+        rc = expand_rows(h, (uint32_t)(k0 + r), (uint32_t)m, stage[b]);
+        if (rc == DC_OK && cudaMemcpyAsync(out + r * V, stage[b], 4 * m * V, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+            rc = set_error(DC_ERR_CUDA, "row download failed");
+    }
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    cudaFree(stage[0]);
+    cudaFree(stage[1]);
+    if (rc == DC_OK && e != cudaSuccess) rc = set_error(DC_ERR_CUDA, "row download: %s", cudaGetErrorString(e));
+    return rc;
+}
+
+extern "C" int dc_materialize_rows(dc_graph* h) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    if (h->d.rows_valid) return DC_OK;
+    uint64_t elems = (uint64_t)(h->d.kmax + 1) * h->g.V;
+    if (h->d.rows_cap < elems) {
+        if (h->d.rows) cudaFree(h->d.rows);
+        h->d.rows = nullptr;
+        h->d.rows_cap = 0;
+        if (cudaMalloc(&h->d.rows, 4 * (elems ? elems : 1)) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(DC_ERR_NOMEM, "dense rows (%llu values) do not fit in device memory",
+                             (unsigned long long)elems);
+        }
+        h->d.rows_cap = elems;
+    }
+    if (int rc = expand_rows(h, 0, (uint32_t)h->d.kmax + 1, h->d.rows)) return rc;
+    API_CUDA(cudaStreamSynchronize(h->stream));
+    h->d.rows_valid = true;
+    return DC_OK;
+}
+
+extern "C" int dc_release_rows(dc_graph* h) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    if (h->d.rows) cudaFree(h->d.rows);
+    h->d.rows = nullptr;
+    h->d.rows_cap = 0;
+    h->d.rows_valid = false;
+    return DC_OK;
+}
+
+extern "C" int dc_get_skyline(dc_graph* h, uint32_t* off, int32_t* ks, int32_t* ls, uint64_t capacity,
+                              uint64_t* n_corners) {
+    if (!h || !n_corners) return set_error(DC_ERR_INVALID, "null argument");
+    if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    *n_corners = h->d.n_corners;
+    if (!off || !ks || !ls) return DC_OK;
+    if (capacity < h->d.n_corners) return set_error(DC_ERR_CAPACITY, "dc_get_skyline: capacity too small");
+    const uint64_t V = h->g.V;
+    API_CUDA(cudaMemcpyAsync(off, h->d.sky_off, 4 * (V + 1), cudaMemcpyDeviceToHost, h->stream));
+    if (h->d.n_corners) {
+        API_CUDA(cudaMemcpyAsync(ks, h->d.sky_k, 4 * h->d.n_corners, cudaMemcpyDeviceToHost, h->stream));
+        API_CUDA(cudaMemcpyAsync(ls, h->d.sky_l, 4 * h->d.n_corners, cudaMemcpyDeviceToHost, h->stream));
+    }
+    API_CUDA(cudaStreamSynchronize(h->stream));
+    return DC_OK;
+}
+
+// writeDecompFile (src/utils.h:98-109).
+extern "C" int dc_write_decomp(dc_graph* h, const char* path) {
+    if (!h || !path) return set_error(DC_ERR_INVALID, "null argument");
+    if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    const uint64_t V = h->g.V;
+    std::vector<int32_t> km(V ? V : 1), rows((uint64_t)(h->d.kmax + 1) * V + 1);
+    if (int rc = dc_get_kmaxes(h, km.data())) return rc;
+    if (int rc = dc_get_lmax_rows(h, 0, (uint32_t)h->d.kmax + 1, rows.data())) return rc;
+    return dc_decomp_file_write(path, (uint32_t)V, h->d.kmax, h->d.lmax, km.data(), rows.data());
+}
+
+// writeDecompFileCPU (src/utils.h:110-124).
+extern "C" int dc_write_decomp_cpu(dc_graph* h, const char* path) {
+    if (!h || !path) return set_error(DC_ERR_INVALID, "null argument");
+    if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    const uint64_t V = h->g.V;
+    std::vector<int32_t> km(V ? V : 1), rows((uint64_t)(h->d.kmax + 1) * V + 1);
+    if (int rc = dc_get_kmaxes(h, km.data())) return rc;
+    if (int rc = dc_get_lmax_rows(h, 0, (uint32_t)h->d.kmax + 1, rows.data())) return rc;
+    return dc_decomp_cpu_file_write(path, (uint32_t)V, km.data(), rows.data());
+}
+
+extern "C" int dc_host_alloc(uint64_t bytes, void** p) {
+    if (!p) return set_error(DC_ERR_INVALID, "null argument");
+    *p = nullptr;
+    cudaError_t e = cudaHostAlloc(p, bytes ? bytes : 1, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return set_error(DC_ERR_NOMEM, "pinned host allocation of %llu bytes failed: %s", (unsigned long long)bytes,
+                         cudaGetErrorString(e));
+    }
+    return DC_OK;
+}
+
+extern "C" int dc_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+    return DC_OK;
+}
+
+extern "C" int dc_synchronize(dc_graph* h) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    API_CUDA(cudaStreamSynchronize(h->stream));
+    return DC_OK;
+}
+
+extern "C" int dc_graph_stream(dc_graph* h, void** stream) {
+    if (!h || !stream) return set_error(DC_ERR_INVALID, "null argument");
+    *stream = (void*)h->stream;
+    return DC_OK;
+}

@@ -1,0 +1,61 @@
+// Host entry points of the device engine (implemented in dc_engine.cu).
+#pragma once
+#include <cstdint>
+
+#include "dc_graph.hpp"
+
+namespace dc {
+
+struct Scratch {
+    uint32_t cap_V = 0;
+    int32_t* key = nullptr;      // [V] peeling degree / cnt_in
+    int32_t* cdeg = nullptr;     // [V] constraint degree
+    int32_t* cur = nullptr;      // [V] current row values
+    int32_t* row0 = nullptr;     // [V] row 0 values
+    uint32_t* mark = nullptr;    // [V]
+    int32_t* stamp = nullptr;    // [V]
+    uint32_t* logidx = nullptr;  // [V]
+    uint32_t* rem0 = nullptr;    // [V]
+    uint32_t* rem1 = nullptr;    // [V]
+    uint32_t* order = nullptr;   // [V] vertices by kmax descending
+    uint32_t* ck = nullptr;      // [kmax+2] |C_k|
+    uint32_t ck_cap = 0;
+    uint32_t* ring = nullptr;    // ring queue slots
+    uint32_t ring_mask = 0;
+    uint32_t* log_v = nullptr;
+    int32_t* log_k = nullptr;
+    int32_t* log_l = nullptr;
+    uint64_t log_cap = 0;
+    uint64_t* tmp64 = nullptr;   // [V+1] scan scratch
+    uint64_t* partial = nullptr; // [blocks] scan scratch
+    uint32_t* cursor = nullptr;  // [V+1]
+    void* tmp_edges = nullptr;   // staging for uploaded edge arrays
+    uint64_t tmp_edges_bytes = 0;
+};
+
+// Allocation / release (all errors reported through set_error, return DC_*).
+int ensure_scratch(dc_graph* h, uint32_t V);
+void free_scratch(dc_graph* h);
+int init_handle(dc_graph* h);
+void free_graph_arrays(DevGraph& g);
+void free_decomp(Decomp& d);
+
+// Builds the slack CSR/CSC of h from device edge arrays (src, dst of length E).
+int build_from_device_edges(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_src, const uint32_t* d_dst);
+// Builds from host CSR/CSC arrays in the reference binary layout.
+int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_deg, const int32_t* out_deg,
+                        const uint32_t* in_off, const uint32_t* out_off, const uint32_t* in_nbr,
+                        const uint32_t* out_nbr, uint64_t nbr_len);
+
+// Full decomposition; method 0 = incremental rows, 1 = per-row peel.
+int decompose(dc_graph* h, int method, int materialize_rows);
+// Dense rows [k0, k0+n) into dst (device pointer, row-major, V per row).
+int expand_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* d_dst);
+
+// Peel of one pass into d_val (device); returns the largest value via *maxval.
+int run_peel(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* d_val, int32_t* maxval, int sync);
+
+// Cooperative launch helper.
+int coop_launch(dc_graph* h, const void* fn, void** args, int threads, const char* name);
+
+}  // namespace dc

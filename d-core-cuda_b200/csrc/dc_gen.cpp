@@ -1,0 +1,189 @@
+// Seeded synthetic directed graphs: Erdős–Rényi G(n, m) and R-MAT.
+//
+// The reference ships a non-seedable generator (src/graph_gen.cpp:9-34: unique
+// directed edges from std::set and rand() % V, srand(time)).  These generators
+// keep its contract -- u != v, no duplicate edges -- and add a seed so that
+// every run, test and benchmark sees the same graph.  Both emit the edge list
+// sorted by (src, dst), like iterating the reference's std::set.
+//
+// R-MAT follows Chakrabarti, Zhan & Faloutsos (SDM 2004): each edge picks one
+// quadrant per bit with probabilities (a, b, c, d); here the bits are drawn
+// MSB first, self-loops are dropped, duplicates are removed by sort-unique and
+// vertex labels are optionally permuted by a seeded Fisher-Yates shuffle
+// (Graph500 practice) so that degree does not correlate with label.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <omp.h>
+
+#include "dc_internal.h"
+#include "dc_rng.h"
+
+namespace dc {
+
+// Stable parallel LSD radix sort of 64-bit keys on their low `bits` bits.
+void radix_sort_u64(uint64_t* keys, uint64_t* tmp, size_t n, int bits) {
+    if (n < 2 || bits <= 0) return;
+    const int DIGIT = 16;
+    const size_t R = size_t(1) << DIGIT;
+    int passes = (bits + DIGIT - 1) / DIGIT;
+    int T = std::max(1, std::min(omp_get_max_threads(), int(n / 65536) + 1));
+    std::vector<size_t> hist(size_t(T) * R);
+    uint64_t* in = keys;
+    uint64_t* out = tmp;
+    for (int p = 0; p < passes; ++p) {
+        int shift = p * DIGIT;
+        std::fill(hist.begin(), hist.end(), 0);
+#pragma omp parallel num_threads(T)
+        {
+            int t = omp_get_thread_num();
+            size_t lo = n * t / T, hi = n * (t + 1) / T;
+            size_t* h = hist.data() + size_t(t) * R;
+            for (size_t i = lo; i < hi; ++i) h[(in[i] >> shift) & (R - 1)]++;
+#pragma omp barrier
+#pragma omp single
+            {
+                size_t run = 0;
+                for (size_t d = 0; d < R; ++d)
+                    for (int tt = 0; tt < T; ++tt) {
+                        size_t c = hist[size_t(tt) * R + d];
+                        hist[size_t(tt) * R + d] = run;
+                        run += c;
+                    }
+            }
+            for (size_t i = lo; i < hi; ++i) {
+                uint64_t k = in[i];
+                out[h[(k >> shift) & (R - 1)]++] = k;
+            }
+        }
+        std::swap(in, out);
+    }
+    if (in != keys) std::memcpy(keys, in, n * sizeof(uint64_t));
+}
+
+}  // namespace dc
+
+using namespace dc;
+
+extern "C" int dc_gen_er(uint32_t n, uint64_t m, uint64_t seed, uint32_t* src, uint32_t* dst) {
+    if (n < 2 && m > 0) return dc::set_error(DC_ERR_INVALID, "dc_gen_er: need n >= 2 for m > 0");
+    if (m > uint64_t(n) * (n - 1)) return dc::set_error(DC_ERR_INVALID, "dc_gen_er: m exceeds n*(n-1)");
+    if (m > 0 && (!src || !dst)) return dc::set_error(DC_ERR_INVALID, "dc_gen_er: null output");
+    // open-addressing set of accepted (u, v) keys; key+1 stored so 0 means empty
+    size_t cap = 16;
+    while (cap < 2 * m + 16) cap <<= 1;
+    std::vector<uint64_t> table(cap, 0);
+    std::vector<uint64_t> keys;
+    keys.reserve(m);
+    Xoshiro256ss rng(derive_seed(seed, 0x4552ull));
+    while (keys.size() < m) {
+        uint32_t u = rng.bounded(n), v = rng.bounded(n);
+        if (u == v) continue;
+        uint64_t key = (uint64_t(u) << 32) | v;
+        uint64_t h = (key * 0x9E3779B97F4A7C15ull) >> 7;
+        size_t i = h & (cap - 1);
+        bool dup = false;
+        while (table[i]) {
+            if (table[i] == key + 1) { dup = true; break; }
+            i = (i + 1) & (cap - 1);
+        }
+        if (dup) continue;
+        table[i] = key + 1;
+        keys.push_back(key);
+    }
+    std::sort(keys.begin(), keys.end());
+    for (uint64_t i = 0; i < m; ++i) {
+        src[i] = uint32_t(keys[i] >> 32);
+        dst[i] = uint32_t(keys[i]);
+    }
+    return DC_OK;
+}
+
+extern "C" int dc_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                           uint64_t seed, int permute, uint64_t capacity,
+                           uint32_t* src, uint32_t* dst, uint64_t* n_edges) {
+    if (scale < 1 || scale > 31) return dc::set_error(DC_ERR_INVALID, "dc_gen_rmat: scale must be in [1, 31]");
+    if (!(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0))
+        return dc::set_error(DC_ERR_INVALID, "dc_gen_rmat: probabilities must be >= 0 with a+b+c <= 1");
+    if (!n_edges) return dc::set_error(DC_ERR_INVALID, "dc_gen_rmat: null n_edges");
+    const uint64_t V = uint64_t(1) << scale;
+    const uint64_t draws = uint64_t(edge_factor) << scale;
+    const double two32 = 4294967296.0;
+    auto thr = [&](double p) -> uint64_t {
+        double t = p * two32;
+        if (t >= two32) return uint64_t(1) << 32;
+        return uint64_t(t);
+    };
+    const uint64_t ta = thr(a), tab = thr(a + b), tabc = thr(a + b + c);
+
+    std::vector<uint32_t> perm;
+    if (permute) {
+        perm.resize(V);
+        for (uint64_t i = 0; i < V; ++i) perm[i] = uint32_t(i);
+        Xoshiro256ss prng(derive_seed(seed, 0x5045524Dull));
+        for (uint64_t i = V - 1; i > 0; --i) {
+            uint64_t j = prng.bounded64(i + 1);
+            std::swap(perm[i], perm[j]);
+        }
+    }
+
+    std::vector<uint64_t> keys(draws);
+    const uint64_t CHUNK = 1 << 16;
+    const uint64_t nchunks = (draws + CHUNK - 1) / CHUNK;
+    std::vector<uint64_t> chunk_count(nchunks);
+    const uint64_t mask = V - 1;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t ch = 0; ch < int64_t(nchunks); ++ch) {
+        Xoshiro256ss rng(derive_seed(seed, uint64_t(ch)));
+        uint64_t lo = uint64_t(ch) * CHUNK, hi = std::min(draws, lo + CHUNK);
+        uint64_t w = lo;
+        for (uint64_t e = lo; e < hi; ++e) {
+            uint64_t u = 0, v = 0;
+            uint64_t r64 = 0;
+            for (uint32_t lvl = 0; lvl < scale; ++lvl) {
+                uint64_t r;
+                if ((lvl & 1) == 0) { r64 = rng.next(); r = r64 >> 32; }
+                else r = r64 & 0xFFFFFFFFull;
+                uint32_t bit = scale - 1 - lvl;
+                if (r < ta) {
+                } else if (r < tab) {
+                    v |= uint64_t(1) << bit;
+                } else if (r < tabc) {
+                    u |= uint64_t(1) << bit;
+                } else {
+                    u |= uint64_t(1) << bit;
+                    v |= uint64_t(1) << bit;
+                }
+            }
+            if (u == v) continue;
+            if (permute) { u = perm[u]; v = perm[v]; }
+            keys[w++] = (u << scale) | (v & mask);
+        }
+        chunk_count[ch] = w - lo;
+    }
+    // compact chunks (each chunk wrote a prefix of its slot range)
+    uint64_t total = 0;
+    for (uint64_t ch = 0; ch < nchunks; ++ch) {
+        uint64_t lo = ch * CHUNK;
+        if (total != lo) std::memmove(keys.data() + total, keys.data() + lo, chunk_count[ch] * sizeof(uint64_t));
+        total += chunk_count[ch];
+    }
+    keys.resize(total);
+    {
+        std::vector<uint64_t> tmp(total);
+        radix_sort_u64(keys.data(), tmp.data(), total, int(2 * scale));
+    }
+    uint64_t uniq = 0;
+    for (uint64_t i = 0; i < total; ++i)
+        if (i == 0 || keys[i] != keys[i - 1]) keys[uniq++] = keys[i];
+    *n_edges = uniq;
+    if (!src || !dst) return DC_OK;  // size query
+    if (capacity < uniq) return dc::set_error(DC_ERR_CAPACITY, "dc_gen_rmat: output capacity too small");
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < int64_t(uniq); ++i) {
+        src[i] = uint32_t(keys[i] >> scale);
+        dst[i] = uint32_t(keys[i] & mask);
+    }
+    return DC_OK;
+}

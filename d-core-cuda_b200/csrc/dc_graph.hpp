@@ -1,0 +1,82 @@
+// Host-side handle of one device-resident graph and its decomposition.
+//
+// HBM layout (all arrays owned by the handle, one CUDA stream per handle):
+//   out_off[V+1]  u32   start of v's out-list slot range (capacity = off[v+1]-off[v])
+//   out_len[V]    i32   live out-degree of v (first out_len[v] slots are edges)
+//   out_nbr[cap]  u32   out-neighbour ids, slack slots after the live prefix
+//   in_off / in_len / in_nbr   the same for in-neighbours (CSC)
+// This is the reference's device_graph_pointers (src/common.h:81-91) with
+// per-list slack generalised from OFFSET_GAP = 1 (src/common.h:36).
+//
+// Decomposition state:
+//   kmax[V]                  in-degree core numbers (g.kmaxes in the reference)
+//   sky_off[V+1], sky_k[], sky_l[]
+//                            compact skyline: v's value in row k is sky_l of
+//                            the last corner with sky_k <= k, for k <= kmax[v];
+//                            0 above kmax[v]
+//   rows[(kmax+1) * V]       optional dense rows, row-major (g.lmaxes)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dc_device.cuh"
+
+namespace dc {
+
+struct DevGraph {
+    uint32_t V = 0;
+    uint64_t E = 0;  // live edges
+    uint32_t* out_off = nullptr;
+    int32_t* out_len = nullptr;
+    uint32_t* out_nbr = nullptr;
+    uint32_t* in_off = nullptr;
+    int32_t* in_len = nullptr;
+    uint32_t* in_nbr = nullptr;
+    uint64_t out_cap = 0, in_cap = 0;
+};
+
+// Persistent-kernel launch geometry for the current device.
+struct LaunchGeom {
+    int sms = 0;
+    int blocks = 0;   // cooperative grid size
+    int threads = 0;  // per block
+};
+
+struct Scratch;  // engine scratch buffers (dc_engine.cu)
+
+struct Decomp {
+    bool valid = false;
+    int32_t kmax = 0;
+    int32_t lmax = 0;
+    int32_t* kmax_v = nullptr;  // [V]
+    uint32_t* sky_off = nullptr;
+    int32_t* sky_k = nullptr;
+    int32_t* sky_l = nullptr;
+    uint64_t n_corners = 0;
+    uint64_t corner_cap = 0;
+    int32_t* rows = nullptr;  // dense rows when materialised
+    uint64_t rows_cap = 0;    // elements allocated
+    bool rows_valid = false;
+};
+
+struct PhaseTimes {
+    float build_ms = 0, kmax_ms = 0, row0_ms = 0, trans_ms = 0, sky_ms = 0, expand_ms = 0;
+};
+
+}  // namespace dc
+
+struct dc_graph {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    dc::DevGraph g;
+    dc::Decomp d;
+    dc::LaunchGeom geom;
+    dc::EngineCtl* ctl = nullptr;  // device
+    dc::Scratch* scratch = nullptr;
+    dc::PhaseTimes times;
+    cudaEvent_t ev[8] = {};
+    uint32_t gap_min = 1;      // minimum free slots per list
+    uint32_t gap_div = 0;      // extra slack = len / gap_div (0 = none)
+    int method = 0;            // 0 = incremental rows, 1 = per-row peel
+    uint64_t stat_evals = 0, stat_drops = 0;
+};

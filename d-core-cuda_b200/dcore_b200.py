@@ -1,0 +1,358 @@
+"""Python binding of the d-core-b200 C ABI (include/dcore_b200.h).
+
+A thin ctypes layer over libdcore_b200.so: numpy arrays in, numpy arrays out.
+It mirrors the reference's host interface for the load -> decompose ->
+maintain path (Graph, dcore, maintenanceFast in llysdal/d-core-cuda) so that
+tests and the benchmark read like the reference's own driver.  There is no
+CPU fallback: compute calls fail with DCoreError when the library or a CUDA
+device is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdcore_b200.so")
+
+DC_OK = 0
+ERR_NAMES = {
+    -1: "DC_ERR_INVALID", -2: "DC_ERR_CUDA", -3: "DC_ERR_NOMEM", -4: "DC_ERR_IO", -5: "DC_ERR_CAPACITY",
+    -6: "DC_ERR_TIMEOUT", -7: "DC_ERR_NOT_FOUND", -8: "DC_ERR_STATE", -9: "DC_ERR_NO_DEVICE",
+}
+METHOD_INCREMENTAL = 0
+METHOD_PEEL = 1
+
+
+class DCoreError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+u32p = ctypes.POINTER(ctypes.c_uint32)
+i32p = ctypes.POINTER(ctypes.c_int32)
+u64p = ctypes.POINTER(ctypes.c_uint64)
+i64p = ctypes.POINTER(ctypes.c_int64)
+u8p = ctypes.POINTER(ctypes.c_uint8)
+vp = ctypes.c_void_p
+
+
+class GraphOpts(ctypes.Structure):
+    _fields_ = [("gap_min", ctypes.c_uint32), ("gap_div", ctypes.c_uint32), ("device", ctypes.c_int32)]
+
+
+class DecompInfo(ctypes.Structure):
+    _fields_ = [("kmax", ctypes.c_int32), ("lmax", ctypes.c_int32), ("n_corners", ctypes.c_uint64),
+                ("kmax_ms", ctypes.c_float), ("row0_ms", ctypes.c_float), ("rows_ms", ctypes.c_float),
+                ("skyline_ms", ctypes.c_float), ("expand_ms", ctypes.c_float),
+                ("evals", ctypes.c_uint64), ("drops", ctypes.c_uint64)]
+
+
+# name -> argtypes; every function returns int status unless listed in _VOID / _STR
+SIGNATURES = {
+    "dc_gen_er": [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p, u32p],
+    "dc_gen_rmat": [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                    ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, u32p, u32p, u64p],
+    "dc_text_read_edges": [ctypes.c_char_p, ctypes.c_int, u32p, u64p, u32p, u32p, ctypes.c_uint64],
+    "dc_binary_read_edges": [ctypes.c_char_p, u32p, u64p, u32p, u32p, ctypes.c_uint64],
+    "dc_binary_write_edges": [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_uint32],
+    "dc_decomp_file_write": [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, i32p, i32p],
+    "dc_decomp_file_read": [ctypes.c_char_p, ctypes.c_uint32, i32p, i32p, i32p, i32p, ctypes.c_uint64],
+    "dc_decomp_cpu_file_write": [ctypes.c_char_p, ctypes.c_uint32, i32p, i32p],
+    "dc_graph_opts_default": [ctypes.POINTER(GraphOpts)],
+    "dc_device_count": [ctypes.POINTER(ctypes.c_int)],
+    "dc_graph_create": [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.POINTER(GraphOpts), ctypes.POINTER(vp)],
+    "dc_graph_create_device": [ctypes.c_uint32, ctypes.c_uint64, vp, vp, ctypes.POINTER(GraphOpts),
+                               ctypes.POINTER(vp)],
+    "dc_graph_load": [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(GraphOpts), ctypes.POINTER(vp)],
+    "dc_graph_free": [vp],
+    "dc_graph_info": [vp, u32p, u64p],
+    "dc_graph_degrees": [vp, i32p, i32p],
+    "dc_graph_get_edges": [vp, u32p, u32p, ctypes.c_uint64, u64p],
+    "dc_graph_write_binary": [vp, ctypes.c_char_p, ctypes.c_uint32],
+    "dc_decompose": [vp, ctypes.c_int, i32p, i32p],
+    "dc_decomp_info_get": [vp, ctypes.POINTER(DecompInfo)],
+    "dc_get_kmaxes": [vp, i32p],
+    "dc_get_lmax_rows": [vp, ctypes.c_uint32, ctypes.c_uint32, i32p],
+    "dc_get_lmax_rows_device": [vp, ctypes.c_uint32, ctypes.c_uint32, vp],
+    "dc_materialize_rows": [vp],
+    "dc_release_rows": [vp],
+    "dc_get_skyline": [vp, u32p, i32p, i32p, ctypes.c_uint64, u64p],
+    "dc_write_decomp": [vp, ctypes.c_char_p],
+    "dc_write_decomp_cpu": [vp, ctypes.c_char_p],
+    "dc_host_alloc": [ctypes.c_uint64, ctypes.POINTER(vp)],
+    "dc_host_free": [vp],
+    "dc_synchronize": [vp],
+    "dc_graph_stream": [vp, ctypes.POINTER(vp)],
+    "dc_last_error": [],
+    "dc_version": [],
+}
+_VOID = {"dc_graph_opts_default"}
+_STR = {"dc_last_error", "dc_version"}
+
+
+def lib():
+    """Loads libdcore_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise DCoreError(-9, f"{LIB_PATH} is not built; run d-core-cuda_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        if not hasattr(L, name):
+            continue
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = None if name in _VOID else (ctypes.c_char_p if name in _STR else ctypes.c_int)
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != DC_OK:
+        raise DCoreError(rc, lib().dc_last_error().decode())
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def last_error():
+    return lib().dc_last_error().decode()
+
+
+def device_count():
+    n = ctypes.c_int(0)
+    _check(lib().dc_device_count(ctypes.byref(n)))
+    return n.value
+
+
+# ---------------------------------------------------------------- generators
+def gen_er(n, m, seed):
+    """Seeded directed G(n, m), sorted by (src, dst)."""
+    src = np.empty(max(m, 1), np.uint32)
+    dst = np.empty(max(m, 1), np.uint32)
+    _check(lib().dc_gen_er(n, m, seed, _p(src, u32p), _p(dst, u32p)))
+    return src[:m], dst[:m]
+
+
+def gen_rmat(scale, edge_factor, seed, a=0.57, b=0.19, c=0.19, permute=True):
+    """Seeded R-MAT graph, self-loops and duplicates removed, sorted by (src, dst)."""
+    cap = edge_factor << scale
+    src = np.empty(max(cap, 1), np.uint32)
+    dst = np.empty(max(cap, 1), np.uint32)
+    n = ctypes.c_uint64(0)
+    _check(lib().dc_gen_rmat(scale, edge_factor, a, b, c, seed, int(permute), cap, _p(src, u32p), _p(dst, u32p),
+                             ctypes.byref(n)))
+    return 1 << scale, src[:n.value], dst[:n.value]
+
+
+# ---------------------------------------------------------------- file formats
+def read_text_edges(path, prune=True):
+    V = ctypes.c_uint32(0)
+    E = ctypes.c_uint64(0)
+    _check(lib().dc_text_read_edges(path.encode(), int(prune), ctypes.byref(V), ctypes.byref(E), None, None, 0))
+    src = np.empty(max(E.value, 1), np.uint32)
+    dst = np.empty(max(E.value, 1), np.uint32)
+    _check(lib().dc_text_read_edges(path.encode(), int(prune), ctypes.byref(V), ctypes.byref(E), _p(src, u32p),
+                                    _p(dst, u32p), E.value))
+    return V.value, src[:E.value], dst[:E.value]
+
+
+def read_binary_edges(path):
+    V = ctypes.c_uint32(0)
+    E = ctypes.c_uint64(0)
+    _check(lib().dc_binary_read_edges(path.encode(), ctypes.byref(V), ctypes.byref(E), None, None, 0))
+    src = np.empty(max(E.value, 1), np.uint32)
+    dst = np.empty(max(E.value, 1), np.uint32)
+    _check(lib().dc_binary_read_edges(path.encode(), ctypes.byref(V), ctypes.byref(E), _p(src, u32p),
+                                      _p(dst, u32p), E.value))
+    return V.value, src[:E.value], dst[:E.value]
+
+
+def write_binary_edges(path, V, src, dst, gap=1):
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    _check(lib().dc_binary_write_edges(path.encode(), V, len(src), _p(src, u32p), _p(dst, u32p), gap))
+
+
+def write_decomp_file(path, kmax, lmax, kmaxes, rows):
+    kmaxes = np.ascontiguousarray(kmaxes, np.int32)
+    rows = np.ascontiguousarray(rows, np.int32)
+    _check(lib().dc_decomp_file_write(path.encode(), len(kmaxes), kmax, lmax, _p(kmaxes, i32p), _p(rows, i32p)))
+
+
+def read_decomp_file(path, V):
+    km = ctypes.c_int32(0)
+    lm = ctypes.c_int32(0)
+    _check(lib().dc_decomp_file_read(path.encode(), V, ctypes.byref(km), ctypes.byref(lm), None, None, 0))
+    kmaxes = np.empty(max(V, 1), np.int32)
+    rows = np.empty(max((km.value + 1) * V, 1), np.int32)
+    _check(lib().dc_decomp_file_read(path.encode(), V, ctypes.byref(km), ctypes.byref(lm), _p(kmaxes, i32p),
+                                     _p(rows, i32p), rows.size))
+    return km.value, lm.value, kmaxes[:V], rows[:(km.value + 1) * V].reshape(km.value + 1, V)
+
+
+def write_decomp_cpu_file(path, kmaxes, rows):
+    kmaxes = np.ascontiguousarray(kmaxes, np.int32)
+    rows = np.ascontiguousarray(rows, np.int32)
+    _check(lib().dc_decomp_cpu_file_write(path.encode(), len(kmaxes), _p(kmaxes, i32p), _p(rows, i32p)))
+
+
+# ---------------------------------------------------------------- graphs
+class Graph:
+    """A device-resident graph handle (Graph / GraphGPU in the reference)."""
+
+    def __init__(self, handle):
+        self._h = vp(handle)
+
+    @staticmethod
+    def _opts(gap_min=1, gap_div=0, device=-1):
+        o = GraphOpts()
+        lib().dc_graph_opts_default(ctypes.byref(o))
+        o.gap_min, o.gap_div, o.device = gap_min, gap_div, device
+        return o
+
+    @classmethod
+    def from_edges(cls, V, src, dst, gap_min=1, gap_div=0, device=-1):
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        h = vp()
+        o = cls._opts(gap_min, gap_div, device)
+        _check(lib().dc_graph_create(V, len(src), _p(src, u32p), _p(dst, u32p), ctypes.byref(o), ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_device_edges(cls, V, E, d_src_ptr, d_dst_ptr, gap_min=1, gap_div=0, device=-1):
+        h = vp()
+        o = cls._opts(gap_min, gap_div, device)
+        _check(lib().dc_graph_create_device(V, E, vp(d_src_ptr), vp(d_dst_ptr), ctypes.byref(o), ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def load(cls, path, prune=True, gap_min=1, gap_div=0, device=-1):
+        h = vp()
+        o = cls._opts(gap_min, gap_div, device)
+        _check(lib().dc_graph_load(path.encode(), int(prune), ctypes.byref(o), ctypes.byref(h)))
+        return cls(h.value)
+
+    def free(self):
+        if self._h and self._h.value:
+            lib().dc_graph_free(self._h)
+            self._h = vp()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        V = ctypes.c_uint32(0)
+        E = ctypes.c_uint64(0)
+        _check(lib().dc_graph_info(self._h, ctypes.byref(V), ctypes.byref(E)))
+        return V.value, E.value
+
+    @property
+    def V(self):
+        return self.info()[0]
+
+    def degrees(self):
+        V = self.V
+        i = np.empty(max(V, 1), np.int32)
+        o = np.empty(max(V, 1), np.int32)
+        _check(lib().dc_graph_degrees(self._h, _p(i, i32p), _p(o, i32p)))
+        return i[:V], o[:V]
+
+    def edges(self):
+        n = ctypes.c_uint64(0)
+        _check(lib().dc_graph_get_edges(self._h, None, None, 0, ctypes.byref(n)))
+        s = np.empty(max(n.value, 1), np.uint32)
+        d = np.empty(max(n.value, 1), np.uint32)
+        _check(lib().dc_graph_get_edges(self._h, _p(s, u32p), _p(d, u32p), n.value, ctypes.byref(n)))
+        return s[:n.value], d[:n.value]
+
+    def write_binary(self, path, gap=1):
+        _check(lib().dc_graph_write_binary(self._h, path.encode(), gap))
+
+    # ---- decomposition
+    def decompose(self, method=METHOD_INCREMENTAL):
+        km = ctypes.c_int32(0)
+        lm = ctypes.c_int32(0)
+        _check(lib().dc_decompose(self._h, method, ctypes.byref(km), ctypes.byref(lm)))
+        return km.value, lm.value
+
+    def decomp_info(self):
+        info = DecompInfo()
+        _check(lib().dc_decomp_info_get(self._h, ctypes.byref(info)))
+        return {f: getattr(info, f) for f, _ in DecompInfo._fields_}
+
+    def kmaxes(self):
+        V = self.V
+        out = np.empty(max(V, 1), np.int32)
+        _check(lib().dc_get_kmaxes(self._h, _p(out, i32p)))
+        return out[:V]
+
+    def rows(self, k0=0, n=None, out=None):
+        """Dense rows k0..k0+n-1 of lmaxes as an (n, V) int32 array."""
+        V = self.V
+        if n is None:
+            n = self.decomp_info()["kmax"] + 1 - k0
+        if out is None:
+            out = np.empty((n, V), np.int32)
+        if n and V:
+            _check(lib().dc_get_lmax_rows(self._h, k0, n, _p(out, i32p)))
+        return out
+
+    def rows_to_device(self, k0, n, d_ptr):
+        _check(lib().dc_get_lmax_rows_device(self._h, k0, n, vp(d_ptr)))
+
+    def materialize_rows(self):
+        _check(lib().dc_materialize_rows(self._h))
+
+    def release_rows(self):
+        _check(lib().dc_release_rows(self._h))
+
+    def skyline(self):
+        n = ctypes.c_uint64(0)
+        _check(lib().dc_get_skyline(self._h, None, None, None, 0, ctypes.byref(n)))
+        V = self.V
+        off = np.empty(V + 1, np.uint32)
+        ks = np.empty(max(n.value, 1), np.int32)
+        ls = np.empty(max(n.value, 1), np.int32)
+        _check(lib().dc_get_skyline(self._h, _p(off, u32p), _p(ks, i32p), _p(ls, i32p), n.value, ctypes.byref(n)))
+        return off, ks[:n.value], ls[:n.value]
+
+    def write_decomp(self, path):
+        _check(lib().dc_write_decomp(self._h, path.encode()))
+
+    def write_decomp_cpu(self, path):
+        _check(lib().dc_write_decomp_cpu(self._h, path.encode()))
+
+    def synchronize(self):
+        _check(lib().dc_synchronize(self._h))
+
+    def stream(self):
+        s = vp()
+        _check(lib().dc_graph_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+
+def exported_symbols():
+    """Names the header declares that the loaded library exports."""
+    L = lib()
+    return sorted(n for n in SIGNATURES if hasattr(L, n))

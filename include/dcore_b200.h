@@ -1,0 +1,180 @@
+/*
+ * d-core-b200 -- C ABI of the B200 (sm_100a) D-core engine.
+ *
+ * Drop-in boundary for the load -> decompose -> maintain path of
+ * llysdal/d-core-cuda.  The reference exposes that path as C++ free functions
+ * and classes compiled into one binary with main(); each entry point below
+ * names the reference interface it replaces (file:line in the reference tree).
+ *
+ * Conventions
+ *   - Every function returns DC_OK (0) or a negative DC_ERR_* code;
+ *     dc_last_error() gives the message of the calling thread's last failure.
+ *   - Plain pointers and sizes only.  Host buffers belong to the caller; the
+ *     engine owns all device memory of a graph handle.
+ *   - Values are the reference's types: `degree` = int32_t
+ *     (src/common.h:59), vertex ids and offsets = uint32_t (src/common.h:60-62).
+ *   - A graph handle is used by one host thread at a time; distinct handles
+ *     may be used from different threads concurrently (each has its own
+ *     CUDA stream).
+ */
+#ifndef DCORE_B200_H
+#define DCORE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define DC_OK 0
+#define DC_ERR_INVALID (-1)   /* bad argument, malformed input            */
+#define DC_ERR_CUDA (-2)      /* CUDA runtime error (message has details) */
+#define DC_ERR_NOMEM (-3)     /* device or host allocation failed         */
+#define DC_ERR_IO (-4)        /* file could not be read or written        */
+#define DC_ERR_CAPACITY (-5)  /* output buffer too small / bound exceeded */
+#define DC_ERR_TIMEOUT (-6)   /* a bounded device-side wait ran out       */
+#define DC_ERR_NOT_FOUND (-7) /* delete of an edge that is not present    */
+#define DC_ERR_STATE (-8)     /* call order (e.g. no decomposition yet)   */
+#define DC_ERR_NO_DEVICE (-9) /* no CUDA device / extension unusable      */
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* dc_last_error(void);
+/* Library version string. */
+const char* dc_version(void);
+
+/* ---- seeded generators (host only, no GPU needed) ----------------------- */
+
+/* Directed Erdos-Renyi G(n, m): m distinct edges (u, v), u != v, uniform,
+ * written sorted by (src, dst).  Replaces generateGraph
+ * (src/graph_gen.cpp:9-34), which is seeded by time and so not reproducible. */
+int dc_gen_er(uint32_t n, uint64_t m, uint64_t seed, uint32_t* src, uint32_t* dst);
+
+/* R-MAT graph with 2^scale vertices and edge_factor * 2^scale draws,
+ * quadrant probabilities (a, b, c, 1-a-b-c); self-loops dropped, duplicates
+ * removed, labels permuted by a seeded shuffle when permute != 0.  Writes the
+ * final edge count to *n_edges; with src or dst NULL it only reports the
+ * count.  capacity = length of src/dst.  No reference counterpart (the
+ * reference has only the ER generator). */
+int dc_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                uint64_t seed, int permute, uint64_t capacity,
+                uint32_t* src, uint32_t* dst, uint64_t* n_edges);
+
+
+/* ---- file formats (host only, no GPU needed) ---------------------------- */
+
+/* Text graph: "# V" header, then "s t" lines.  Self-loops dropped, duplicate
+ * edges kept; prune != 0 removes vertices without edges and renumbers the
+ * rest in increasing id order.  Replaces Graph::readFile and
+ * pruneEmptyVertices (src/graph.cpp:146-250, 110-144).  With src or dst NULL
+ * only *V and *E are reported. */
+int dc_text_read_edges(const char* path, int prune, uint32_t* V, uint64_t* E,
+                       uint32_t* src, uint32_t* dst, uint64_t capacity);
+
+/* Binary graph "<file>-binary-g=<GAP>" (Graph::readBinary,
+ * src/graph.cpp:287-325): the out-lists as an edge list, src ascending. */
+int dc_binary_read_edges(const char* path, uint32_t* V, uint64_t* E,
+                         uint32_t* src, uint32_t* dst, uint64_t capacity);
+/* Graph::writeBinary (src/graph.cpp:261-285) of an edge list, lists in
+ * ascending neighbour order, `gap` free slots per list (filled 0xCDCDCDCD). */
+int dc_binary_write_edges(const char* path, uint32_t V, uint64_t E,
+                          const uint32_t* src, const uint32_t* dst, uint32_t gap);
+
+/* .decomp file (writeDecompFile / readDecompFile, src/utils.h:76-109):
+ * kmax, lmax, kmaxes[V], rows[(kmax+1) * V], all int32. */
+int dc_decomp_file_write(const char* path, uint32_t V, int32_t kmax, int32_t lmax,
+                         const int32_t* kmaxes, const int32_t* rows);
+/* Reads the header (and, when kmaxes/rows are given and rows_cap is large
+ * enough, the arrays).  V must be the graph's vertex count. */
+int dc_decomp_file_read(const char* path, uint32_t V, int32_t* kmax, int32_t* lmax,
+                        int32_t* kmaxes, int32_t* rows, uint64_t rows_cap);
+/* .decompCPU text file (writeDecompFileCPU, src/utils.h:110-124). */
+int dc_decomp_cpu_file_write(const char* path, uint32_t V, const int32_t* kmaxes,
+                             const int32_t* rows);
+
+/* ---- device-resident graphs ---------------------------------------------- */
+
+typedef struct dc_graph dc_graph;
+
+typedef struct dc_graph_opts {
+    uint32_t gap_min; /* free slots per adjacency list (reference OFFSET_GAP = 1) */
+    uint32_t gap_div; /* extra free slots = degree / gap_div (0: none)             */
+    int32_t device;   /* CUDA device ordinal, -1 = current device                  */
+} dc_graph_opts;
+
+void dc_graph_opts_default(dc_graph_opts* opts);
+/* Number of visible CUDA devices (0 when none; never fails). */
+int dc_device_count(int* n);
+
+/* Builds the device CSR (out) + CSC (in) from host edge arrays; the copy to
+ * the device is part of the call.  Replaces Graph construction plus
+ * allocateDeviceGraphMemory / moveGraphToDevice (src/cuda_memory.h:5-41). */
+int dc_graph_create(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst,
+                    const dc_graph_opts* opts, dc_graph** out);
+/* Same from device-resident edge arrays (no host copy). */
+int dc_graph_create_device(uint32_t V, uint64_t E, const uint32_t* d_src, const uint32_t* d_dst,
+                           const dc_graph_opts* opts, dc_graph** out);
+/* Graph(const string&) (src/graph.cpp:381-395): reads "<path>-binary-g=<gap>"
+ * when present (or `path` itself when it names such a file), else parses the
+ * text file (prune as in dc_text_read_edges). */
+int dc_graph_load(const char* path, int prune, const dc_graph_opts* opts, dc_graph** out);
+int dc_graph_free(dc_graph* g);
+int dc_graph_info(const dc_graph* g, uint32_t* V, uint64_t* E);
+/* Live in/out degrees (host arrays of V). */
+int dc_graph_degrees(dc_graph* g, int32_t* in_deg, int32_t* out_deg);
+/* Live edges, src ascending, dst ascending within a source.  With src/dst
+ * NULL only *n_edges is reported. */
+int dc_graph_get_edges(dc_graph* g, uint32_t* src, uint32_t* dst, uint64_t capacity, uint64_t* n_edges);
+/* Graph::writeBinary of the current device graph. */
+int dc_graph_write_binary(dc_graph* g, const char* path, uint32_t gap);
+
+/* ---- decomposition ------------------------------------------------------- */
+
+#define DC_METHOD_INCREMENTAL 0 /* kmax + row 0 by peeling, rows 1..kmax derived row to row */
+#define DC_METHOD_PEEL 1        /* one fresh peel per row, the reference's schedule          */
+
+/* dcore(Graph&) (main.cu:197-262), also checkDCore (main.cu:276-293): kmax of
+ * every vertex and all rows lmax[k][v], k = 0..kmax, kept on the device.
+ * Reports the global kmax and lmax.  Both methods give identical results. */
+int dc_decompose(dc_graph* g, int method, int32_t* kmax, int32_t* lmax);
+
+typedef struct dc_decomp_info {
+    int32_t kmax, lmax;
+    uint64_t n_corners; /* skyline corners stored on the device */
+    float kmax_ms, row0_ms, rows_ms, skyline_ms, expand_ms;
+    uint64_t evals, drops; /* row-to-row evaluations and value drops */
+} dc_decomp_info;
+int dc_decomp_info_get(dc_graph* g, dc_decomp_info* info);
+
+/* g.kmaxes (host array of V). */
+int dc_get_kmaxes(dc_graph* g, int32_t* out);
+/* Rows k0..k0+n-1 of g.lmaxes, row-major, V values per row, into host memory
+ * (pinned memory from dc_host_alloc gives full copy bandwidth). */
+int dc_get_lmax_rows(dc_graph* g, uint32_t k0, uint32_t n, int32_t* out);
+/* Same into device memory. */
+int dc_get_lmax_rows_device(dc_graph* g, uint32_t k0, uint32_t n, int32_t* d_out);
+/* Keeps all (kmax+1) * V rows dense on the device (later row reads are copies). */
+int dc_materialize_rows(dc_graph* g);
+int dc_release_rows(dc_graph* g);
+/* Compact skyline: off[V+1]; corners off[v]..off[v+1]-1 of v as (k, l) pairs
+ * with k ascending; lmax[k][v] = l of the last corner with k_i <= k for
+ * k <= kmax[v], 0 above.  With off/ks/ls NULL only *n_corners is reported. */
+int dc_get_skyline(dc_graph* g, uint32_t* off, int32_t* ks, int32_t* ls, uint64_t capacity,
+                   uint64_t* n_corners);
+/* writeDecompFile / writeDecompFileCPU of the current decomposition. */
+int dc_write_decomp(dc_graph* g, const char* path);
+int dc_write_decomp_cpu(dc_graph* g, const char* path);
+
+/* ---- utilities ----------------------------------------------------------- */
+int dc_host_alloc(uint64_t bytes, void** p); /* pinned host memory */
+int dc_host_free(void* p);
+int dc_synchronize(dc_graph* g);
+/* The graph's CUDA stream (cudaStream_t) for interop. */
+int dc_graph_stream(dc_graph* g, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DCORE_B200_H */

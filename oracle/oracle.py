@@ -1,0 +1,108 @@
+"""ctypes wrapper of the CPU oracle (dcore_oracle.c) -- TEST INFRASTRUCTURE.
+
+Used only by the tests, the smoke check and the benchmark's CPU-baseline leg
+to check or time the engine; never by the engine itself.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+u32p = ctypes.POINTER(ctypes.c_uint32)
+i32p = ctypes.POINTER(ctypes.c_int32)
+i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build as _b  # noqa: F401  (package import when available)
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.or_peel_levels.argtypes = [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_int, ctypes.c_int32, i32p]
+        _lib.or_peel_levels.restype = ctypes.c_int32
+        _lib.or_kmax.argtypes = [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, i32p]
+        _lib.or_kmax.restype = ctypes.c_int32
+        _lib.or_bz_row.argtypes = [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, i32p, ctypes.c_int32, i32p]
+        _lib.or_bz_row.restype = ctypes.c_int32
+        _lib.or_dcore.argtypes = [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_int, i32p, i32p,
+                                  ctypes.c_uint64, i32p, i32p]
+        _lib.or_dcore.restype = ctypes.c_int
+        _lib.or_kedge_batches.argtypes = [ctypes.c_uint32, i32p, ctypes.c_uint64, u32p, u32p, i64p]
+        _lib.or_kedge_batches.restype = ctypes.c_int64
+    return _lib
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, np.uint32)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+def peel_levels(V, src, dst, swap, k):
+    """Literal restatement of one reference pass; returns (last level, core[V])."""
+    src, dst = _u32(src), _u32(dst)
+    core = np.empty(max(V, 1), np.int32)
+    lvl = lib().or_peel_levels(V, len(src), _ptr(src, u32p), _ptr(dst, u32p), int(swap), k, _ptr(core, i32p))
+    return lvl, core[:V]
+
+
+def dcore_levels(V, src, dst):
+    """dcore() with the literal level-loop pass for every row (small graphs)."""
+    kmax, kmaxes = peel_levels(V, dst, src, 0, 0)  # swapped k = 0 pass
+    kmax = max(kmax, 0)
+    rows = []
+    lmax = 0
+    for k in range(kmax + 1):
+        l, row = peel_levels(V, src, dst, 0, k)
+        lmax = max(lmax, l)
+        rows.append(row)
+    return kmax, lmax, kmaxes, np.stack(rows) if rows else np.zeros((1, V), np.int32)
+
+
+def dcore(V, src, dst, threads=0):
+    """Bucket-queue decomposition: (kmax, lmax, kmaxes[V], rows[kmax+1, V])."""
+    src, dst = _u32(src), _u32(dst)
+    kmaxes = np.empty(max(V, 1), np.int32)
+    km = ctypes.c_int32(0)
+    lm = ctypes.c_int32(0)
+    rc = lib().or_dcore(V, len(src), _ptr(src, u32p), _ptr(dst, u32p), threads, _ptr(kmaxes, i32p), None, 0,
+                        ctypes.byref(km), ctypes.byref(lm))
+    if rc not in (0, -5):
+        raise RuntimeError(f"oracle or_dcore failed: {rc}")
+    rows = np.empty((km.value + 1, max(V, 1)), np.int32)
+    rc = lib().or_dcore(V, len(src), _ptr(src, u32p), _ptr(dst, u32p), threads, _ptr(kmaxes, i32p),
+                        _ptr(rows, i32p), km.value + 1, ctypes.byref(km), ctypes.byref(lm))
+    if rc != 0:
+        raise RuntimeError(f"oracle or_dcore failed: {rc}")
+    return km.value, lm.value, kmaxes[:V], rows[:, :V]
+
+
+def kmax(V, src, dst):
+    src, dst = _u32(src), _u32(dst)
+    out = np.empty(max(V, 1), np.int32)
+    km = lib().or_kmax(V, len(src), _ptr(src, u32p), _ptr(dst, u32p), _ptr(out, i32p))
+    return km, out[:V]
+
+
+def row(V, src, dst, kmaxes, k):
+    src, dst = _u32(src), _u32(dst)
+    kmaxes = np.ascontiguousarray(kmaxes, np.int32)
+    out = np.empty(max(V, 1), np.int32)
+    l = lib().or_bz_row(V, len(src), _ptr(src, u32p), _ptr(dst, u32p), _ptr(kmaxes, i32p), k, _ptr(out, i32p))
+    return l, out[:V]
+
+
+def kedge_batches(V, kmaxes, frm, to):
+    """getKmaxEdgeBatches (KEDGE_BATCHING): sub-batch index of every edge."""
+    frm, to = _u32(frm), _u32(to)
+    kmaxes = np.ascontiguousarray(kmaxes, np.int32)
+    out = np.empty(max(len(frm), 1), np.int64)
+    nb = lib().or_kedge_batches(V, _ptr(kmaxes, i32p), len(frm), _ptr(frm, u32p), _ptr(to, u32p), _ptr(out, i64p))
+    return nb, out[:len(frm)]
