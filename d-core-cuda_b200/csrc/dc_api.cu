@@ -163,9 +163,30 @@ extern "C" int dc_graph_load(const char* path, int prune, const dc_graph_opts* o
     return dc_graph_create(V, s.size(), s.data(), d.data(), o, out);
 }
 
+extern "C" int dc_set_trace(dc_graph* h, uint32_t max_steps, dc_trace_fn fn, void* user) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    if (h->trace_dev) cudaFree(h->trace_dev);
+    if (h->trace_host) cudaFreeHost(h->trace_host);
+    h->trace_dev = nullptr;
+    h->trace_host = nullptr;
+    h->trace_cap = 0;
+    h->trace_cb = nullptr;
+    if (max_steps == 0 || !fn) return DC_OK;
+    if (cudaMalloc(&h->trace_dev, 64ull * max_steps) != cudaSuccess ||
+        cudaHostAlloc(&h->trace_host, 64ull * max_steps, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(DC_ERR_NOMEM, "trace buffers");
+    }
+    h->trace_cap = max_steps;
+    h->trace_cb = fn;
+    h->trace_user = user;
+    return DC_OK;
+}
+
 extern "C" int dc_graph_free(dc_graph* h) {
     if (!h) return DC_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    dc_set_trace(h, 0, nullptr, nullptr);
     free_graph_arrays(h->g);
     free_decomp(h->d);
     free_scratch(h);
@@ -260,6 +281,7 @@ extern "C" int dc_decomp_info_get(dc_graph* h, dc_decomp_info* info) {
     info->expand_ms = h->times.expand_ms;
     info->evals = h->stat_evals;
     info->drops = h->stat_drops;
+    info->entries = h->stat_entries;
     return DC_OK;
 }
 
@@ -393,6 +415,14 @@ extern "C" int dc_write_decomp_cpu(dc_graph* h, const char* path) {
     return dc_decomp_cpu_file_write(path, (uint32_t)V, km.data(), rows.data());
 }
 
+// Launch-shape knobs of the persistent kernels (tuning).
+extern "C" int dc_set_launch(dc_graph* h, int blocks_per_sm) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    if (blocks_per_sm < 0 || blocks_per_sm > 8) return set_error(DC_ERR_INVALID, "blocks_per_sm must be 0..8");
+    h->blocks_per_sm = blocks_per_sm;
+    return DC_OK;
+}
+
 extern "C" int dc_host_alloc(uint64_t bytes, void** p) {
     if (!p) return set_error(DC_ERR_INVALID, "null argument");
     *p = nullptr;
@@ -408,6 +438,16 @@ extern "C" int dc_host_alloc(uint64_t bytes, void** p) {
 
 extern "C" int dc_host_free(void* p) {
     if (p) cudaFreeHost(p);
+    return DC_OK;
+}
+
+namespace dc {
+extern unsigned long long g_launches;
+}
+
+extern "C" int dc_launch_count(unsigned long long* n) {
+    if (!n) return set_error(DC_ERR_INVALID, "null argument");
+    *n = dc::g_launches;
     return DC_OK;
 }
 

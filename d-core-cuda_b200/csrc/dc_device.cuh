@@ -45,6 +45,24 @@ struct EngineCtl {
     unsigned long long drops;
     unsigned long long pushes;
     unsigned long long edges_scanned;
+    // ticket queue (see TicketQueue)
+    unsigned t_head;        // next ticket
+    unsigned t_tail;        // next slot to reserve
+    int outstanding;        // unfinished producers + pushed, unfinished items
+    unsigned phase_done;    // set by whoever brings outstanding to 0
+    unsigned rc_cur[2];     // remaining-list sizes per peel instance
+    unsigned rc_next[2];
+    int maxv[2];            // largest value per peel instance
+    int step;               // level / transition index
+    unsigned nworkers;      // producers per phase (warps in the grid)
+    // optional per-step timing trace: 8 words per step
+    //   [0] %globaltimer at step start, [1] when its work ran out,
+    //   [2] queue items of the step, [3] %globaltimer at the closing barrier,
+    //   [4] latest block wake-up after the opening barrier,
+    //   [5] latest block seeding done, [6] earliest block wake-up
+    unsigned long long* trace;
+    unsigned trace_cap;
+    unsigned trace_tail0;
 };
 
 __device__ __forceinline__ unsigned ld_vol(const unsigned* p) {
@@ -96,6 +114,48 @@ __device__ __forceinline__ bool grid_sync(EngineCtl* c) {
     }
     __syncthreads();
     return s_ok != 0u;
+}
+
+// Grid barrier whose last arriving block runs hook(c) before releasing the
+// others, so per-phase counters can be reset with no other block running.
+template <typename Hook>
+__device__ __forceinline__ bool grid_sync_hook(EngineCtl* c, Hook hook) {
+    __shared__ unsigned s_ok2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned nb = gridDim.x;
+        unsigned gen = ld_vol(&c->bar_gen);
+        __threadfence();
+        unsigned arrived = atomicAdd(&c->bar_count, 1u);
+        if (arrived == nb - 1) {
+            hook(c);
+            atomicExch(&c->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&c->bar_gen, 1u);
+        } else {
+            unsigned long long t0 = gtimer();
+            while (ld_vol(&c->bar_gen) == gen) {
+                if (ld_vol(&c->error)) break;
+                if (gtimer() - t0 > kWaitNs) {
+                    set_dev_error(c, DC_DEV_ERR_TIMEOUT, 4);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok2 = (ld_vol(&c->error) == 0u);
+        if (c->trace) {
+            int st = ld_vol(&c->step);
+            if (st >= 0 && (unsigned)st < c->trace_cap) {
+                unsigned long long now = gtimer();
+                atomicMax(&c->trace[8 * st + 4], now);
+                atomicMin(&c->trace[8 * st + 6], now);
+            }
+        }
+    }
+    __syncthreads();
+    return s_ok2 != 0u;
 }
 
 // Warp-aggregated append: every lane of a converged warp calls this; lanes
@@ -190,6 +250,137 @@ __device__ __forceinline__ void q_done_warp(EngineCtl* c, unsigned n) {
     __threadfence();
     __syncwarp();
     if ((threadIdx.x & 31u) == 0 && n) atomicAdd(&c->q_done, n);
+}
+
+// ---------------------------------------------------------------------------
+// Ticket queue.  Items are 64-bit words in a ring of slots (kEmptyItem =
+// free).  A consumer warp takes a ticket with one atomicAdd on t_head and
+// polls only its own slot, so idle warps do not contend on shared counters.
+// Termination uses one counter: `outstanding` starts at the number of
+// producer warps; each producer subtracts 1 when its seeding share is done,
+// each push adds the number of pushed items before they become visible, and
+// each finished item subtracts 1 after its own pushes.  Whoever brings it to
+// 0 sets phase_done; a consumer whose slot is still empty then leaves.  At
+// the barrier that ends the phase the abandoned tickets are skipped by
+// setting t_tail = t_head (grid_sync_hook).
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kEmptyItem = ~0ull;
+
+struct TicketQueue {
+    unsigned long long* slots;
+    unsigned mask;
+};
+
+__device__ __forceinline__ void tq_finish(EngineCtl* c, int n) {
+    __threadfence();
+    if (atomicSub(&c->outstanding, n) == n) {
+        atomicExch(&c->phase_done, 1u);
+        if (c->trace && (unsigned)c->step < c->trace_cap) c->trace[8 * c->step + 1] = gtimer();
+    }
+}
+
+// Called by the last block of a phase-ending barrier: closes the step's
+// trace record and opens the next one.
+__device__ __forceinline__ void trace_step_end(EngineCtl* c) {
+    unsigned long long now = gtimer();
+    if (c->trace && c->step >= 0 && (unsigned)c->step < c->trace_cap) {
+        c->trace[8 * c->step + 2] = c->t_tail - c->trace_tail0;
+        c->trace[8 * c->step + 3] = now;
+    }
+    c->step++;
+    if (c->trace && (unsigned)c->step < c->trace_cap) {
+        c->trace[8 * c->step] = now;
+        c->trace[8 * c->step + 6] = ~0ull;
+    }
+    c->trace_tail0 = c->t_tail;
+}
+
+// Converged warp: lanes with pred push `cnt` consecutive items item0,
+// item0 + inc, ... (cnt may be 0).
+__device__ __forceinline__ void tq_push_warp_multi(EngineCtl* c, TicketQueue q, unsigned cnt,
+                                                   unsigned long long item0, unsigned long long inc) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (unsigned)o) x += y;
+    }
+    unsigned total = __shfl_sync(0xFFFFFFFFu, x, 31);
+    if (total == 0) return;
+    unsigned base = 0;
+    if (lane == 0) {
+        atomicAdd(&c->outstanding, (int)total);
+        base = atomicAdd(&c->t_tail, total);
+    }
+    base = __shfl_sync(0xFFFFFFFFu, base, 0) + (x - cnt);
+    if (cnt) __threadfence();
+    for (unsigned i = 0; i < cnt; ++i) {
+        volatile unsigned long long* s = &q.slots[(base + i) & q.mask];
+        *s = item0 + inc * i;
+    }
+}
+
+__device__ __forceinline__ void tq_push_warp(EngineCtl* c, TicketQueue q, bool pred, unsigned long long item) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned m = __ballot_sync(0xFFFFFFFFu, pred);
+    if (!m) return;
+    unsigned base = 0;
+    if (lane == 0) {
+        atomicAdd(&c->outstanding, (int)__popc(m));
+        base = atomicAdd(&c->t_tail, (unsigned)__popc(m));
+    }
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (pred) {
+        __threadfence();
+        volatile unsigned long long* s = &q.slots[(base + __popc(m & ((1u << lane) - 1u))) & q.mask];
+        *s = item;
+    }
+}
+
+// Converged warp: returns true with *item set, or false when the phase is
+// over (or an error / timeout occurred).  *ticket holds the warp's current
+// ticket between calls (kNoTicket initially).
+constexpr unsigned kNoTicket = 0xFFFFFFFFu;
+__device__ __forceinline__ bool tq_take_warp(EngineCtl* c, TicketQueue q, unsigned* ticket,
+                                             unsigned long long* item) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned long long it = kEmptyItem;
+    int state = 0;  // 1 = got item, 2 = phase over
+    if (lane == 0) {
+        if (*ticket == kNoTicket) *ticket = atomicAdd(&c->t_head, 1u);
+        volatile unsigned long long* s = &q.slots[*ticket & q.mask];
+        unsigned long long t0 = 0;
+        unsigned spins = 0;
+        for (;;) {
+            it = *s;
+            if (it != kEmptyItem) {
+                *s = kEmptyItem;
+                *ticket = kNoTicket;
+                state = 1;
+                break;
+            }
+            if (ld_vol(&c->phase_done) || ld_vol(&c->error)) {
+                // abandon the ticket: the phase-ending barrier skips it
+                *ticket = kNoTicket;
+                state = 2;
+                break;
+            }
+            if (++spins == 64) t0 = gtimer();
+            if (spins > 64 && (spins & 63) == 0 && gtimer() - t0 > kWaitNs) {
+                set_dev_error(c, DC_DEV_ERR_TIMEOUT, 5);
+                *ticket = kNoTicket;
+                state = 2;
+                break;
+            }
+            if (spins > 16) __nanosleep(spins > 256 ? 256 : 32);
+        }
+    }
+    state = __shfl_sync(0xFFFFFFFFu, state, 0);
+    it = __shfl_sync(0xFFFFFFFFu, it, 0);
+    __threadfence();
+    *item = it;
+    return state == 1;
 }
 
 // Idle-wait helper for the drain loops: returns false once the phase has made

@@ -22,6 +22,9 @@
 
 namespace dc {
 
+// Kernel launches issued by the engine since load (host counter).
+unsigned long long g_launches = 0;
+
 #define DC_CUDA(call)                                                                        \
     do {                                                                                     \
         cudaError_t _e = (call);                                                             \
@@ -183,206 +186,29 @@ __global__ void k_scatter_edges(uint64_t E, const uint32_t* src, const uint32_t*
 }
 
 // ---------------------------------------------------------------------------
-// persistent peel
+// incremental rows: shared helpers
 // ---------------------------------------------------------------------------
-struct PeelParams {
-    uint32_t V;
-    const uint32_t* a_off;
-    const int32_t* a_len;
-    const uint32_t* a_nbr;
-    const uint32_t* b_off;
-    const int32_t* b_len;
-    const uint32_t* b_nbr;
-    const int32_t* member;  // nullptr: every vertex is in the set
-    int32_t k;              // constraint threshold (0: none)
-    int32_t* key;
-    int32_t* cdeg;
-    int32_t* val;
-    uint32_t* rem0;
-    uint32_t* rem1;
-    RingQueue q;
-    EngineCtl* ctl;
-};
-
-// One pass of the reference's level loop (KListInplace, main.cu:171-195):
-// level L removes every remaining vertex whose peeling degree is L (scan,
-// main.cu:37-56) and then the cascade of vertices whose peeling degree falls
-// to L or whose constraint degree falls below k (process, main.cu:100-135),
-// all with value L.  Here the cascade runs through the device work queue and
-// one software grid barrier separates levels.
-__global__ void __launch_bounds__(kThreads) k_peel(PeelParams p) {
-    const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
-    const unsigned gwarp = blockIdx.x * kWarpsPerBlock + wib;
-    const unsigned nwarps = gridDim.x * kWarpsPerBlock;
-    EngineCtl* c = p.ctl;
-    __shared__ uint32_t s_x[kWarpsPerBlock][32];
-    __shared__ uint32_t s_start[kWarpsPerBlock][32];
-    __shared__ int32_t s_la[kWarpsPerBlock][32];
-
-    // ---- init: degrees restricted to the member set, remaining list
-    for (uint64_t base = (uint64_t)gwarp * 32; base < p.V; base += (uint64_t)nwarps * 32) {
-        uint64_t vi = base + lane;
-        bool ok = vi < p.V, in = false;
-        uint32_t v = (uint32_t)vi;
-        if (ok) {
-            in = !p.member || p.member[v] >= p.k;
-            if (!in) {
-                p.val[v] = 0;
-            } else {
-                p.val[v] = -1;
-                int kd = 0, cd = 0;
-                if (!p.member) {
-                    kd = p.a_len[v];
-                } else {
-                    uint32_t o = p.a_off[v], e = o + (uint32_t)p.a_len[v];
-                    for (; o < e; ++o) kd += (p.member[p.a_nbr[o]] >= p.k);
-                    o = p.b_off[v];
-                    e = o + (uint32_t)p.b_len[v];
-                    for (; o < e; ++o) cd += (p.member[p.b_nbr[o]] >= p.k);
-                }
-                p.key[v] = kd;
-                p.cdeg[v] = cd;
-            }
-        }
-        unsigned pos = warp_append(&c->rcount[0], ok && in);
-        if (ok && in) p.rem0[pos] = v;
-    }
-    if (!grid_sync(c)) return;
-
-    uint32_t* rc = p.rem0;
-    uint32_t* rn = p.rem1;
-    int L = 0;
-    for (;; ++L) {
-        const unsigned cs = L % 3, ns = (L + 1) % 3, zs = (L + 2) % 3;
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            c->rcount[zs] = 0;
-            c->producers[ns] = 0;
-        }
-        const unsigned n_rem = ld_vol(&c->rcount[cs]);
-        if (n_rem == 0) break;
-        bool pushed_any = false;
-        // ---- scan the remaining list
-        for (unsigned base = gwarp * 32; base < n_rem; base += nwarps * 32) {
-            unsigned i = base + lane;
-            bool ok = i < n_rem;
-            uint32_t v = ok ? rc[i] : 0;
-            bool keep = false, push = false;
-            if (ok && ld_vol(&p.val[v]) == -1) {
-                if (ld_vol(&p.key[v]) <= L)
-                    push = atomicCAS(&p.val[v], -1, L) == -1;
-                else
-                    keep = true;
-            }
-            unsigned pos = warp_append(&c->rcount[ns], keep);
-            if (keep) rn[pos] = v;
-            q_push_warp(c, p.q, push, v);
-            pushed_any |= push;
-        }
-        __threadfence();
-        __syncwarp();
-        if (lane == 0) atomicAdd(&c->producers[cs], 1u);
-
-        // ---- drain the cascade
-        IdleClock clk;
-        clk.start(c);
-        for (;;) {
-            unsigned first;
-            bool fin;
-            unsigned n = q_claim_warp(c, 32, nwarps, &c->producers[cs], &first, &fin);
-            if (n == 0) {
-                if (fin || ld_vol(&c->error)) break;
-                if (!clk.tick(c)) break;
-                continue;
-            }
-            uint32_t x = 0;
-            int la = 0, lb = 0;
-            if (lane < n) {
-                x = q_take(c, p.q, first + lane);
-                if (x != kEmptySlot) {
-                    la = p.k > 0 ? p.a_len[x] : 0;
-                    lb = p.b_len[x];
-                }
-            }
-            unsigned tot = (unsigned)(la + lb);
-            unsigned inc = warp_incl_scan(tot);
-            unsigned T = __shfl_sync(0xFFFFFFFFu, inc, 31);
-            s_x[wib][lane] = x;
-            s_start[wib][lane] = inc - tot;
-            s_la[wib][lane] = la;
-            __syncwarp();
-            for (unsigned base = 0; base < T; base += 32) {
-                unsigned e = base + lane;
-                bool push = false;
-                uint32_t pv = 0;
-                if (e < T) {
-                    int lo = 0, hi = (int)n - 1;
-                    while (lo < hi) {
-                        int mid = (lo + hi + 1) >> 1;
-                        if (s_start[wib][mid] <= e) lo = mid;
-                        else hi = mid - 1;
-                    }
-                    uint32_t xj = s_x[wib][lo];
-                    unsigned local = e - s_start[wib][lo];
-                    int laj = s_la[wib][lo];
-                    if ((int)local < laj) {
-                        uint32_t u = p.a_nbr[p.a_off[xj] + local];
-                        int old = atomicSub(&p.cdeg[u], 1);
-                        if (old == p.k && ld_vol(&p.val[u]) == -1 && atomicCAS(&p.val[u], -1, L) == -1) {
-                            push = true;
-                            pv = u;
-                        }
-                    } else {
-                        uint32_t w = p.b_nbr[p.b_off[xj] + (local - (unsigned)laj)];
-                        int old = atomicSub(&p.key[w], 1);
-                        if (old == L + 1 && ld_vol(&p.val[w]) == -1 && atomicCAS(&p.val[w], -1, L) == -1) {
-                            push = true;
-                            pv = w;
-                        }
-                    }
-                }
-                q_push_warp(c, p.q, push, pv);
-                pushed_any |= push;
-            }
-            q_done_warp(c, n);
-        }
-        if (__any_sync(0xFFFFFFFFu, pushed_any) && lane == 0) atomicMax(&c->maxval, L);
-        if (!grid_sync(c)) return;
-        uint32_t* t = rc;
-        rc = rn;
-        rn = t;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) c->steps = L;
-}
-
-// ---------------------------------------------------------------------------
-// incremental rows
-// ---------------------------------------------------------------------------
-struct TransParams {
-    uint32_t V;
-    const uint32_t* out_off;
-    const int32_t* out_len;
-    const uint32_t* out_nbr;
-    const uint32_t* in_off;
-    const int32_t* in_len;
-    const uint32_t* in_nbr;
-    const int32_t* kmax;
-    int32_t K;
-    const uint32_t* order;  // vertices by kmax descending
-    const uint32_t* ck;     // ck[k] = |C_k|, k = 0..K+1
-    int32_t* cur;           // row values, -1 outside C
-    int32_t* cnt_in;        // #in-neighbours with cur >= cur[v]
-    uint32_t* mark;
-    int32_t* stamp;
-    uint32_t* logidx;
-    uint32_t* log_v;
-    int32_t* log_k;
-    int32_t* log_l;
-    unsigned long long log_cap;
-    RingQueue q;
-    EngineCtl* ctl;
-};
-
 static constexpr int kWin = 64;
+
+// The last warp of a block to finish its seeding share reports the block as
+// one producer (outstanding counts blocks, not warps: far fewer atomics on
+// the shared counter per step).
+__device__ __forceinline__ void block_producer_done(EngineCtl* c, unsigned* s_cnt) {
+    __syncwarp();
+    if ((threadIdx.x & 31u) == 0) {
+        __threadfence();
+        unsigned o = atomicAdd(s_cnt, 1u);
+        if (o == (blockDim.x >> 5) - 1) {
+            *s_cnt = 0;
+            if (c->trace) {
+                int st = ld_vol(&c->step);
+                if (st >= 0 && (unsigned)st < c->trace_cap) atomicMax(&c->trace[8 * st + 5], gtimer());
+            }
+            tq_finish(c, 1);
+        }
+    }
+    __syncwarp();
+}
 
 // Per-vertex queue state for the transition drain:
 //   0 idle, 1 queued, 2 being evaluated, 3 being evaluated and re-run
@@ -408,222 +234,467 @@ __device__ __forceinline__ bool mark_request(uint32_t* m, EngineCtl* c) {
     return false;
 }
 
-// cnt_in[v] = #{w in N_in(v) : cur[w] >= cur[v]}  (warp per vertex)
-__global__ void k_cnt_in_init(uint32_t V, const uint32_t* in_off, const int32_t* in_len, const uint32_t* in_nbr,
-                              const int32_t* cur, int32_t* cnt_in) {
+// ---------------------------------------------------------------------------
+// fused peel, ticket queue, chunked items
+// ---------------------------------------------------------------------------
+struct PeelInst {
+    const uint32_t* a_off;
+    const int32_t* a_len;
+    const uint32_t* a_nbr;
+    const uint32_t* b_off;
+    const int32_t* b_len;
+    const uint32_t* b_nbr;
+    const int32_t* member;  // nullptr: all vertices
+    int32_t k;              // constraint threshold (0: none)
+    int32_t* key;
+    int32_t* cdeg;
+    int32_t* val;
+    uint32_t* rem0;
+    uint32_t* rem1;
+};
+
+struct Peel2Params {
+    uint32_t V;
+    int ninst;
+    unsigned chunk;  // adjacency entries per queue item
+    PeelInst in[2];
+    TicketQueue q;
+    EngineCtl* ctl;
+};
+
+__device__ __forceinline__ unsigned long long peel_item(uint32_t v, unsigned ch, int inst) {
+    return (unsigned long long)v | ((unsigned long long)ch << 32) | ((unsigned long long)inst << 63);
+}
+
+__device__ __forceinline__ unsigned peel_nitems(const PeelInst& I, uint32_t x, unsigned CH) {
+    unsigned len = (unsigned)(I.k > 0 ? I.a_len[x] : 0) + (unsigned)I.b_len[x];
+    return (len + CH - 1) / CH;
+}
+
+struct PeelHook {
+    int ninst;
+    unsigned nworkers;
+    __device__ void operator()(EngineCtl* c) const {
+        for (int i = 0; i < ninst; ++i) {
+            c->rc_cur[i] = c->rc_next[i];
+            c->rc_next[i] = 0;
+        }
+        trace_step_end(c);
+        c->t_tail = c->t_head;
+        c->trace_tail0 = c->t_tail;
+        c->outstanding = (int)nworkers;
+        c->phase_done = 0;
+        __threadfence();
+    }
+};
+
+// Up to two independent peels advance level by level in one grid: the kmax
+// pass (peeling in-degree, swapInOut + KListInplace(k = 0), main.cu:218-220)
+// and row 0 (peeling out-degree), or two rows of the per-row method.  Level
+// L of each peel removes every remaining vertex whose peeling degree is at
+// most L (scan, main.cu:37-56) and the cascade that follows (process,
+// main.cu:100-135) with value L.  Work items are (vertex, chunk of its
+// adjacency), so hub lists spread over many warps.
+__global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
+    const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const unsigned gwarp = blockIdx.x * kWarpsPerBlock + wib;
+    const unsigned nwarps = gridDim.x * kWarpsPerBlock;
+    EngineCtl* c = p.ctl;
+    const unsigned CH = p.chunk;
+    PeelHook hook{p.ninst, gridDim.x};
+    __shared__ unsigned s_prod;
+    if (threadIdx.x == 0) s_prod = 0;
+    __syncthreads();
+
+    // ---- init
+    for (int i = 0; i < p.ninst; ++i) {
+        const PeelInst& I = p.in[i];
+        for (uint64_t base = (uint64_t)gwarp * 32; base < p.V; base += (uint64_t)nwarps * 32) {
+            uint64_t vi = base + lane;
+            bool ok = vi < p.V, in = false;
+            uint32_t v = (uint32_t)vi;
+            if (ok) {
+                in = !I.member || I.member[v] >= I.k;
+                if (!in) {
+                    I.val[v] = 0;
+                } else {
+                    I.val[v] = -1;
+                    int kd = 0, cd = 0;
+                    if (!I.member) {
+                        kd = I.a_len[v];
+                    } else {
+                        uint32_t o = I.a_off[v], e = o + (uint32_t)I.a_len[v];
+                        for (; o < e; ++o) kd += (I.member[I.a_nbr[o]] >= I.k);
+                        o = I.b_off[v];
+                        e = o + (uint32_t)I.b_len[v];
+                        for (; o < e; ++o) cd += (I.member[I.b_nbr[o]] >= I.k);
+                    }
+                    I.key[v] = kd;
+                    I.cdeg[v] = cd;
+                }
+            }
+            unsigned pos = warp_append(&c->rc_next[i], ok && in);
+            if (ok && in) I.rem0[pos] = v;
+        }
+    }
+    if (!grid_sync_hook(c, hook)) return;
+
+    unsigned ticket = kNoTicket;
+    for (int L = 0;; ++L) {
+        bool any_left = false;
+        for (int i = 0; i < p.ninst; ++i) any_left |= ld_vol(&c->rc_cur[i]) != 0u;
+        if (!any_left) break;
+        unsigned pushed_mask = 0;
+        // ---- scan remaining lists
+        for (int i = 0; i < p.ninst; ++i) {
+            const PeelInst& I = p.in[i];
+            const unsigned n_rem = ld_vol(&c->rc_cur[i]);
+            const uint32_t* rc = (L & 1) ? I.rem1 : I.rem0;
+            uint32_t* rn = (L & 1) ? I.rem0 : I.rem1;
+            for (unsigned base = gwarp * 32; base < n_rem; base += nwarps * 32) {
+                unsigned idx = base + lane;
+                bool ok = idx < n_rem;
+                uint32_t v = ok ? rc[idx] : 0;
+                bool keep = false, push = false;
+                if (ok && ld_vol(&I.val[v]) == -1) {
+                    if (ld_vol(&I.key[v]) <= L)
+                        push = atomicCAS(&I.val[v], -1, L) == -1;
+                    else
+                        keep = true;
+                }
+                unsigned pos = warp_append(&c->rc_next[i], keep);
+                if (keep) rn[pos] = v;
+                unsigned cnt = push ? peel_nitems(I, v, CH) : 0u;
+                tq_push_warp_multi(c, p.q, cnt, peel_item(v, 0, i), 1ull << 32);
+                if (__any_sync(0xFFFFFFFFu, push)) pushed_mask |= 1u << i;
+            }
+        }
+        block_producer_done(c, &s_prod);
+        // ---- drain the cascade
+        unsigned long long item;
+        while (tq_take_warp(c, p.q, &ticket, &item)) {
+            const int i = (int)(item >> 63);
+            const uint32_t x = (uint32_t)item;
+            const unsigned ch = (unsigned)((item >> 32) & 0x7FFFFFFFull);
+            const PeelInst& I = p.in[i];
+            const unsigned la = (unsigned)(I.k > 0 ? I.a_len[x] : 0);
+            const unsigned len = la + (unsigned)I.b_len[x];
+            const unsigned e0 = ch * CH, e1 = min(len, e0 + CH);
+            const uint32_t ao = I.a_off[x], bo = I.b_off[x];
+            bool pushed = false;
+            for (unsigned base = e0; base < e1; base += 64) {
+                // two entries per lane, both atomics issued before either result is used
+                unsigned ea = base + lane, eb = base + 32 + lane;
+                int olda = 0, oldb = 0;
+                uint32_t ua = 0, ub = 0;
+                bool isa_a = false, isa_b = false;
+                if (ea < e1) {
+                    isa_a = ea < la;
+                    ua = isa_a ? I.a_nbr[ao + ea] : I.b_nbr[bo + (ea - la)];
+                }
+                if (eb < e1) {
+                    isa_b = eb < la;
+                    ub = isa_b ? I.a_nbr[ao + eb] : I.b_nbr[bo + (eb - la)];
+                }
+                if (ea < e1) olda = atomicSub(isa_a ? &I.cdeg[ua] : &I.key[ua], 1);
+                if (eb < e1) oldb = atomicSub(isa_b ? &I.cdeg[ub] : &I.key[ub], 1);
+                bool pa = ea < e1 && (isa_a ? olda == I.k : olda == L + 1) && ld_vol(&I.val[ua]) == -1 &&
+                          atomicCAS(&I.val[ua], -1, L) == -1;
+                bool pb = eb < e1 && (isa_b ? oldb == I.k : oldb == L + 1) && ld_vol(&I.val[ub]) == -1 &&
+                          atomicCAS(&I.val[ub], -1, L) == -1;
+                unsigned cnta = pa ? peel_nitems(I, ua, CH) : 0u;
+                tq_push_warp_multi(c, p.q, cnta, peel_item(ua, 0, i), 1ull << 32);
+                unsigned cntb = pb ? peel_nitems(I, ub, CH) : 0u;
+                tq_push_warp_multi(c, p.q, cntb, peel_item(ub, 0, i), 1ull << 32);
+                pushed |= __any_sync(0xFFFFFFFFu, pa || pb);
+            }
+            if (pushed) pushed_mask |= 1u << i;
+            __syncwarp();
+            if (lane == 0) tq_finish(c, 1);
+        }
+        if (lane == 0) {
+            for (int i = 0; i < p.ninst; ++i)
+                if (pushed_mask & (1u << i)) atomicMax(&c->maxv[i], L);
+        }
+        if (!grid_sync_hook(c, hook)) return;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// incremental rows with exact support counters
+// ---------------------------------------------------------------------------
+struct Trans2Params {
+    uint32_t V;
+    const uint32_t* out_off;
+    int32_t* out_len;  // working copies, pruned in place
+    uint32_t* out_nbr;
+    const uint32_t* in_off;
+    int32_t* in_len;
+    uint32_t* in_nbr;
+    const int32_t* kmax;
+    int32_t K;
+    int sorted;  // lists ordered by neighbour kmax, descending
+    const uint32_t* order;
+    const uint32_t* ck;
+    int32_t* cur;
+    int32_t* cnt_out;  // #{u in N_out(v) : cur[u] >= cur[v]}  (never above the truth)
+    int32_t* cnt_in;   // #{w in N_in(v)  : cur[w] >= cur[v]}
+    uint32_t* mark;
+    int32_t* stamp;
+    uint32_t* logidx;
+    uint32_t* log_v;
+    int32_t* log_k;
+    int32_t* log_l;
+    unsigned long long log_cap;
+    TicketQueue q;
+    EngineCtl* ctl;
+};
+
+struct TransHook {
+    unsigned nworkers;
+    __device__ void operator()(EngineCtl* c) const {
+        trace_step_end(c);
+        c->t_tail = c->t_head;
+        c->trace_tail0 = c->t_tail;
+        c->outstanding = (int)nworkers;
+        c->phase_done = 0;
+        __threadfence();
+    }
+};
+
+// Counters of v against every neighbour, at v's row-0 value.
+__global__ void k_counters_init(uint32_t V, const uint32_t* out_off, const int32_t* out_len, const uint32_t* out_nbr,
+                                const uint32_t* in_off, const int32_t* in_len, const uint32_t* in_nbr,
+                                const int32_t* cur, int32_t* cnt_out, int32_t* cnt_in) {
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t v = gw; v < V; v += nw) {
         int cv = cur[v];
-        uint32_t o = in_off[v];
-        int n = in_len[v];
-        int cnt = 0;
-        for (int i = lane; i < n; i += 32) cnt += (cur[in_nbr[o + i]] >= cv);
+        int co = 0, ci = 0;
+        uint32_t o = out_off[v];
+        int n = out_len[v];
+        for (int i = lane; i < n; i += 32) co += (cur[out_nbr[o + i]] >= cv);
+        o = in_off[v];
+        n = in_len[v];
+        for (int i = lane; i < n; i += 32) ci += (cur[in_nbr[o + i]] >= cv);
 #pragma unroll
-        for (int s = 16; s; s >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, s);
-        if (lane == 0) cnt_in[v] = cnt;
+        for (int s = 16; s; s >>= 1) {
+            co += __shfl_xor_sync(0xFFFFFFFFu, co, s);
+            ci += __shfl_xor_sync(0xFFFFFFFFu, ci, s);
+        }
+        if (lane == 0) {
+            cnt_out[v] = co;
+            cnt_in[v] = ci;
+        }
     }
 }
 
-// Warp evaluation of vertex x against in-count requirement kreq.
-// New value = max L <= cap with #{out-nbrs u: cur[u] >= L} >= L and
-// #{in-nbrs w: cur[w] >= L} >= kreq; found by windowed histograms of
-// neighbour values, 64 levels per pass from the top.
-// Returns new value; *cnt = #{in-nbrs w : cur[w] >= new value}.
-__device__ int eval_vertex(const TransParams& p, uint32_t x, int cap, int kreq, int* s_ho, int* s_hi, int* cnt_out_in) {
+// One histogram pass over the C_j prefix of a kmax-sorted neighbour list for
+// the window [lo, hi]; values above hi land in bin hi only on the first
+// window (hi == cap).  Four entries per lane per step; the pass stops after
+// a step whose last entry has left C_j (value -1), since every later entry
+// has a kmax no larger.
+__device__ __forceinline__ int hist_pass(const int32_t* cur, const uint32_t* a, int n, int lo, int hi, bool first,
+                                         bool sorted, int* bins) {
     const unsigned lane = threadIdx.x & 31u;
-    const uint32_t oo = p.out_off[x], io = p.in_off[x];
-    const int on = p.out_len[x], in = p.in_len[x];
-    int carry_o = 0, carry_i = 0;
-    int hi = cap;
-    for (;;) {
-        int lo = max(0, hi - (kWin - 1));
-        s_ho[lane] = 0;
-        s_ho[lane + 32] = 0;
-        s_hi[lane] = 0;
-        s_hi[lane + 32] = 0;
-        __syncwarp();
-        for (int i = lane; i < on; i += 32) {
-            int cu = ld_vol(&p.cur[p.out_nbr[oo + i]]);
-            if (cu >= lo) {
-                if (cu >= hi) {
-                    if (hi == cap || cu <= hi) atomicAdd(&s_ho[hi - lo], 1);
-                } else {
-                    atomicAdd(&s_ho[cu - lo], 1);
-                }
-            }
-        }
-        for (int i = lane; i < in; i += 32) {
-            int cw = ld_vol(&p.cur[p.in_nbr[io + i]]);
-            if (cw >= lo) {
-                if (cw >= hi) {
-                    if (hi == cap || cw <= hi) atomicAdd(&s_hi[hi - lo], 1);
-                } else {
-                    atomicAdd(&s_hi[cw - lo], 1);
-                }
-            }
-        }
-        __syncwarp();
-        // suffix sums over bins [0, hi-lo]; lane handles bins 2*lane, 2*lane+1
-        int b0 = 2 * lane, b1 = 2 * lane + 1;
-        int o0 = s_ho[b0], o1 = s_ho[b1], i0 = s_hi[b0], i1 = s_hi[b1];
-        int po = o0 + o1, pi = i0 + i1;
-        // reverse inclusive scan (from lane 31 down to lane)
-        int so = po, si = pi;
+    int b = 0;
+    for (; b < n; b += 128) {
+        int cu[4];
 #pragma unroll
-        for (int s = 1; s < 32; s <<= 1) {
-            int yo = __shfl_down_sync(0xFFFFFFFFu, so, s);
-            int yi = __shfl_down_sync(0xFFFFFFFFu, si, s);
-            if (lane + s < 32) {
-                so += yo;
-                si += yi;
+        for (int r = 0; r < 4; ++r) {
+            int e = b + r * 32 + (int)lane;
+            cu[r] = e < n ? ld_vol(&cur[a[e]]) : -1;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int x = cu[r];
+            if (x >= lo) {
+                if (x >= hi) {
+                    if (first || x == hi) atomicAdd(&bins[hi - lo], 1);
+                } else {
+                    atomicAdd(&bins[x - lo], 1);
+                }
             }
         }
-        // cum at bin b1 = carry + (suffix from lane+1) + o1 ; at b0 = that + o0
-        int cum_o1 = carry_o + (so - po) + o1, cum_i1 = carry_i + (si - pi) + i1;
-        int cum_o0 = cum_o1 + o0, cum_i0 = cum_i1 + i0;
-        int L0 = lo + b0, L1 = lo + b1;
-        bool ok1 = (L1 <= hi) && cum_o1 >= L1 && cum_i1 >= kreq;
-        bool ok0 = (L0 <= hi) && cum_o0 >= L0 && cum_i0 >= kreq;
-        unsigned m1 = __ballot_sync(0xFFFFFFFFu, ok1), m0 = __ballot_sync(0xFFFFFFFFu, ok0);
-        int best = -1, bestcnt = 0;
-        // highest L satisfying: compare top lanes of m1 and m0
-        int t1 = m1 ? 31 - __clz(m1) : -1, t0 = m0 ? 31 - __clz(m0) : -1;
-        int c1 = __shfl_sync(0xFFFFFFFFu, cum_i1, t1 < 0 ? 0 : t1);
-        int c0 = __shfl_sync(0xFFFFFFFFu, cum_i0, t0 < 0 ? 0 : t0);
-        if (t1 >= 0) {
-            best = lo + 2 * t1 + 1;
-            bestcnt = c1;
+        int last = min(b + 127, n - 1) - b;
+        int rr = last >> 5;
+        int mine = rr == 0 ? cu[0] : rr == 1 ? cu[1] : rr == 2 ? cu[2] : cu[3];
+        if (sorted && __shfl_sync(0xFFFFFFFFu, mine, last & 31) == -1) {
+            b += 128;
+            break;
         }
-        if (t0 >= 0 && lo + 2 * t0 > best) {
-            best = lo + 2 * t0;
-            bestcnt = c0;
-        }
-        if (best >= 0) {
-            *cnt_out_in = bestcnt;
-            return best;
-        }
-        // carry the whole window into the next one below
-        int wo = __shfl_sync(0xFFFFFFFFu, so, 0), wi = __shfl_sync(0xFFFFFFFFu, si, 0);
-        carry_o += wo;
-        carry_i += wi;
-        if (lo == 0) {  // cannot happen for members of C_kreq; report value 0
-            *cnt_out_in = carry_i;
-            return 0;
-        }
-        hi = lo - 1;
-        __syncwarp();
     }
+    return min(b, n);
 }
 
-// Rows 1..K from row 0.  Row j is the greatest fixpoint below row j-1 of
-//   l(v) = max L : |{u in N_out(v) : l(u) >= L}| >= L  and
-//                  |{w in N_in(v)  : l(w) >= L}| >= j,  v in C_j,
-// which is the (j, l)-core number of v (the value the reference's pass k = j
-// produces, main.cu:238-244).  Starting from row j-1 (a pointwise upper
-// bound, since the (j,l)-core is inside the (j-1,l)-core) the kernel only
-// re-evaluates vertices whose bound can be violated: those leaving C_j
-// (kmax == j-1), those whose in-count at their own level is below j, and,
-// transitively, neighbours of every vertex whose value drops.
-__global__ void __launch_bounds__(kThreads) k_transitions(TransParams p) {
+__global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
     const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const unsigned gwarp = blockIdx.x * kWarpsPerBlock + wib;
     const unsigned nwarps = gridDim.x * kWarpsPerBlock;
     EngineCtl* c = p.ctl;
     __shared__ int s_ho[kWarpsPerBlock][kWin];
     __shared__ int s_hi[kWarpsPerBlock][kWin];
-    unsigned long long my_evals = 0, my_drops = 0;
+    int* ho = s_ho[wib];
+    int* hi_ = s_hi[wib];
+    TransHook hook{gridDim.x};
+    unsigned long long my_evals = 0, my_drops = 0, my_entries = 0;
+    unsigned ticket = kNoTicket;
+    __shared__ unsigned s_prod;
+    if (threadIdx.x == 0) s_prod = 0;
+    if (!grid_sync_hook(c, hook)) return;
 
     for (int j = 1; j <= p.K; ++j) {
-        const unsigned cs = j % 3, ns = (j + 1) % 3;
-        if (blockIdx.x == 0 && threadIdx.x == 0) c->producers[ns] = 0;
         const uint32_t vj = p.ck[j], vprev = p.ck[j - 1];
-        // ---- vertices leaving C_j: value -1, wake neighbours they supported
+        // ---- vertices leaving C_j: value -1; neighbours they supported lose one count
         for (uint32_t i = vj + gwarp; i < vprev; i += nwarps) {
             uint32_t x = p.order[i];
-            int a = p.cur[x];
+            int a = ld_vol(&p.cur[x]);
             __syncwarp();
             if (lane == 0) {
-                p.cur[x] = -1;
+                atomicExch(&p.cur[x], -1);
                 __threadfence();
             }
             __syncwarp();
             if (a < 1) continue;
+            __threadfence();
             uint32_t o = p.out_off[x];
             int n = p.out_len[x];
             for (int b = 0; b < n; b += 32) {
-                bool push = false;
+                bool req = false;
                 uint32_t z = 0;
+                int cz = -1;
                 if (b + (int)lane < n) {
                     z = p.out_nbr[o + b + lane];
-                    int cz = ld_vol(&p.cur[z]);
-                    push = cz >= 1 && cz <= a && mark_request(&p.mark[z], c);
+                    cz = ld_vol(&p.cur[z]);
+                    if (cz >= 1 && cz <= a) {
+                        int old = atomicSub(&p.cnt_in[z], 1);
+                        req = (old - 1 < j) && mark_request(&p.mark[z], c);
+                    }
                 }
-                q_push_warp(c, p.q, push, z);
+                tq_push_warp(c, p.q, req, z);
+                int last = min(31, n - 1 - b);
+                if (p.sorted && __shfl_sync(0xFFFFFFFFu, cz, last) == -1) break;
             }
             o = p.in_off[x];
             n = p.in_len[x];
             for (int b = 0; b < n; b += 32) {
-                bool push = false;
+                bool req = false;
                 uint32_t y = 0;
+                int cy = -1;
                 if (b + (int)lane < n) {
                     y = p.in_nbr[o + b + lane];
-                    int cy = ld_vol(&p.cur[y]);
-                    push = cy >= 1 && cy <= a && mark_request(&p.mark[y], c);
+                    cy = ld_vol(&p.cur[y]);
+                    if (cy >= 1 && cy <= a) {
+                        int old = atomicSub(&p.cnt_out[y], 1);
+                        req = (old - 1 < cy) && mark_request(&p.mark[y], c);
+                    }
                 }
-                q_push_warp(c, p.q, push, y);
+                tq_push_warp(c, p.q, req, y);
+                int last = min(31, n - 1 - b);
+                if (p.sorted && __shfl_sync(0xFFFFFFFFu, cy, last) == -1) break;
             }
         }
-        // ---- seeds: members whose in-count at their level is below j
+        // ---- seeds: members whose in-count at their own level is below j
         for (uint32_t base = gwarp * 32; base < vj; base += nwarps * 32) {
             uint32_t i = base + lane;
-            bool push = false;
+            bool req = false;
             uint32_t v = 0;
             if (i < vj) {
                 v = p.order[i];
-                push = p.cur[v] >= 1 && p.cnt_in[v] < j && mark_request(&p.mark[v], c);
+                req = ld_vol(&p.cur[v]) >= 1 && ld_vol(&p.cnt_in[v]) < j && mark_request(&p.mark[v], c);
             }
-            q_push_warp(c, p.q, push, v);
+            tq_push_warp(c, p.q, req, v);
         }
-        __threadfence();
-        __syncwarp();
-        if (lane == 0) atomicAdd(&c->producers[cs], 1u);
+        block_producer_done(c, &s_prod);
 
         // ---- drain
-        IdleClock clk;
-        clk.start(c);
-        for (;;) {
-            unsigned first;
-            bool fin;
-            unsigned n = q_claim_warp(c, 1, nwarps, &c->producers[cs], &first, &fin);
-            if (n == 0) {
-                if (fin || ld_vol(&c->error)) break;
-                if (!clk.tick(c)) break;
-                continue;
-            }
-            uint32_t x = 0;
+        unsigned long long item;
+        while (tq_take_warp(c, p.q, &ticket, &item)) {
+            const uint32_t x = (uint32_t)item;
             if (lane == 0) {
-                x = q_take(c, p.q, first);
-                if (x != kEmptySlot) {
-                    atomicExch(&p.mark[x], 2u);
-                    __threadfence();
-                }
+                atomicExch(&p.mark[x], 2u);
+                __threadfence();
             }
-            x = __shfl_sync(0xFFFFFFFFu, x, 0);
-            if (x == kEmptySlot) {
-                q_done_warp(c, n);
-                continue;
-            }
-            int cap = ld_vol(&p.cur[x]);
+            __syncwarp();
+            const int cap = ld_vol(&p.cur[x]);
             if (p.kmax[x] < j || cap < 1) {
-                // outside C_j or at value 0: nothing can change
-                if (lane == 0) atomicExch(&p.mark[x], 0u);
-                q_done_warp(c, n);
+                if (lane == 0) {
+                    atomicExch(&p.mark[x], 0u);
+                    tq_finish(c, 1);
+                }
                 continue;
             }
-            int cnt = 0;
-            int nv = eval_vertex(p, x, cap, j, s_ho[wib], s_hi[wib], &cnt);
+            int s0o = 0, s0i = 0;
+            if (lane == 0) {
+                s0o = ld_vol(&p.cnt_out[x]);
+                s0i = ld_vol(&p.cnt_in[x]);
+            }
+            __threadfence();
+            const uint32_t oo = p.out_off[x], io = p.in_off[x];
+            // ---- new value from windowed histograms (first pass prunes)
+            int carry_o = 0, carry_i = 0, hi = cap, nv = -1, c_o = 0, c_i = 0;
+            bool first = true;
+            for (;;) {
+                int lo = max(0, hi - (kWin - 1));
+                ho[lane] = 0;
+                ho[lane + 32] = 0;
+                hi_[lane] = 0;
+                hi_[lane + 32] = 0;
+                __syncwarp();
+                my_entries += hist_pass(p.cur, p.out_nbr + oo, p.out_len[x], lo, hi, first, p.sorted != 0, ho);
+                my_entries += hist_pass(p.cur, p.in_nbr + io, p.in_len[x], lo, hi, first, p.sorted != 0, hi_);
+                __syncwarp();
+                int b0 = 2 * lane, b1 = 2 * lane + 1;
+                int o0 = ho[b0], o1 = ho[b1], i0 = hi_[b0], i1 = hi_[b1];
+                int po = o0 + o1, pi = i0 + i1;
+                int so = po, si = pi;
+#pragma unroll
+                for (int s = 1; s < 32; s <<= 1) {
+                    int yo = __shfl_down_sync(0xFFFFFFFFu, so, s);
+                    int yi = __shfl_down_sync(0xFFFFFFFFu, si, s);
+                    if (lane + s < 32) {
+                        so += yo;
+                        si += yi;
+                    }
+                }
+                int cum_o1 = carry_o + (so - po) + o1, cum_i1 = carry_i + (si - pi) + i1;
+                int cum_o0 = cum_o1 + o0, cum_i0 = cum_i1 + i0;
+                int L0 = lo + b0, L1 = lo + b1;
+                bool ok1 = (L1 <= hi) && cum_o1 >= L1 && cum_i1 >= j;
+                bool ok0 = (L0 <= hi) && cum_o0 >= L0 && cum_i0 >= j;
+                unsigned m1 = __ballot_sync(0xFFFFFFFFu, ok1), m0 = __ballot_sync(0xFFFFFFFFu, ok0);
+                int t1 = m1 ? 31 - __clz(m1) : -1, t0 = m0 ? 31 - __clz(m0) : -1;
+                int best = -1, bt = 0, bodd = 0;
+                if (t1 >= 0) {
+                    best = lo + 2 * t1 + 1;
+                    bt = t1;
+                    bodd = 1;
+                }
+                if (t0 >= 0 && lo + 2 * t0 > best) {
+                    best = lo + 2 * t0;
+                    bt = t0;
+                    bodd = 0;
+                }
+                if (best >= 0) {
+                    int xo = bodd ? cum_o1 : cum_o0, xi = bodd ? cum_i1 : cum_i0;
+                    c_o = __shfl_sync(0xFFFFFFFFu, xo, bt);
+                    c_i = __shfl_sync(0xFFFFFFFFu, xi, bt);
+                    nv = best;
+                    break;
+                }
+                carry_o += __shfl_sync(0xFFFFFFFFu, so, 0);
+                carry_i += __shfl_sync(0xFFFFFFFFu, si, 0);
+                first = false;
+                if (lo == 0) {  // unreachable for members of C_j
+                    nv = 0;
+                    c_o = carry_o;
+                    c_i = carry_i;
+                    break;
+                }
+                hi = lo - 1;
+                __syncwarp();
+            }
             ++my_evals;
             if (nv < cap) {
                 ++my_drops;
@@ -647,61 +718,203 @@ __global__ void __launch_bounds__(kThreads) k_transitions(TransParams p) {
                 }
                 __syncwarp();
                 __threadfence();
-                // wake neighbours whose support crossed: value in (nv, cap]
-                uint32_t o = p.out_off[x];
-                int m = p.out_len[x];
-                for (int b = 0; b < m; b += 32) {
-                    bool push = false;
+                // recount at nv after the write, and take x's support away
+                // from neighbours whose level lies in (nv, cap]
+                c_o = 0;
+                c_i = 0;
+                int n = p.out_len[x];
+                for (int b = 0; b < n; b += 32) {
+                    bool req = false;
                     uint32_t z = 0;
-                    if (b + (int)lane < m) {
-                        z = p.out_nbr[o + b + lane];
-                        int cz = ld_vol(&p.cur[z]);
-                        push = cz > nv && cz <= cap && mark_request(&p.mark[z], c);
+                    int cz = -1;
+                    if (b + (int)lane < n) {
+                        z = p.out_nbr[oo + b + lane];
+                        cz = ld_vol(&p.cur[z]);
+                        c_o += (cz >= nv);
+                        if (cz > nv && cz <= cap) {
+                            int old = atomicSub(&p.cnt_in[z], 1);
+                            req = (old - 1 < j) && mark_request(&p.mark[z], c);
+                        }
                     }
-                    q_push_warp(c, p.q, push, z);
+                    tq_push_warp(c, p.q, req, z);
+                    int last = min(31, n - 1 - b);
+                    my_entries += last + 1;
+                    if (p.sorted && __shfl_sync(0xFFFFFFFFu, cz, last) == -1) break;
                 }
-                o = p.in_off[x];
-                m = p.in_len[x];
-                for (int b = 0; b < m; b += 32) {
-                    bool push = false;
+                n = p.in_len[x];
+                for (int b = 0; b < n; b += 32) {
+                    bool req = false;
                     uint32_t y = 0;
-                    if (b + (int)lane < m) {
-                        y = p.in_nbr[o + b + lane];
-                        int cy = ld_vol(&p.cur[y]);
-                        push = cy > nv && cy <= cap && mark_request(&p.mark[y], c);
+                    int cy = -1;
+                    if (b + (int)lane < n) {
+                        y = p.in_nbr[io + b + lane];
+                        cy = ld_vol(&p.cur[y]);
+                        c_i += (cy >= nv);
+                        if (cy > nv && cy <= cap) {
+                            int old = atomicSub(&p.cnt_out[y], 1);
+                            req = (old - 1 < cy) && mark_request(&p.mark[y], c);
+                        }
                     }
-                    q_push_warp(c, p.q, push, y);
+                    tq_push_warp(c, p.q, req, y);
+                    int last = min(31, n - 1 - b);
+                    my_entries += last + 1;
+                    if (p.sorted && __shfl_sync(0xFFFFFFFFu, cy, last) == -1) break;
+                }
+#pragma unroll
+                for (int s = 16; s; s >>= 1) {
+                    c_o += __shfl_xor_sync(0xFFFFFFFFu, c_o, s);
+                    c_i += __shfl_xor_sync(0xFFFFFFFFu, c_i, s);
                 }
             }
-            // release x; after a drop it is re-run once more, so that values
-            // of neighbours that dropped concurrently are seen
             bool requeue = false;
             if (lane == 0) {
-                p.cnt_in[x] = cnt;
+                int no = atomicAdd(&p.cnt_out[x], c_o - s0o) + (c_o - s0o);
+                int ni = atomicAdd(&p.cnt_in[x], c_i - s0i) + (c_i - s0i);
+                bool stable = nv < 1 || (no >= nv && ni >= j);
                 __threadfence();
-                if (nv < cap && nv >= 1) {
+                if (!stable) {
                     atomicExch(&p.mark[x], 1u);
                     requeue = true;
                 } else {
                     unsigned o = atomicCAS(&p.mark[x], 2u, 0u);
                     if (o == 3u) {
-                        if (nv >= 1) {
-                            atomicExch(&p.mark[x], 1u);
-                            requeue = true;
-                        } else {
-                            atomicExch(&p.mark[x], 0u);
-                        }
+                        atomicExch(&p.mark[x], 1u);
+                        requeue = true;
                     }
                 }
             }
-            q_push_warp(c, p.q, requeue, x);
-            q_done_warp(c, n);
+            tq_push_warp(c, p.q, requeue, x);
+            if (lane == 0) tq_finish(c, 1);
         }
-        if (!grid_sync(c)) break;
+        if (!grid_sync_hook(c, hook)) break;
     }
     if (lane == 0) {
         atomicAdd(&c->evals, my_evals);
         atomicAdd(&c->drops, my_drops);
+        atomicAdd(&c->edges_scanned, my_entries);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// adjacency lists ordered by neighbour kmax, descending
+// ---------------------------------------------------------------------------
+// With every list in this order, the neighbours inside C_j = {kmax >= j}
+// form a prefix of the list, so row-to-row evaluations read only that
+// prefix.  Short lists: one thread, insertion sort.  Medium lists: one block,
+// bitonic sort of (kmax, id) pairs in shared memory.  Long lists: one block,
+// counting sort by kmax through a scratch copy of the list.
+static constexpr int kSortShort = 32;
+static constexpr int kSortMid = 4096;
+
+__global__ void k_sort_short(uint32_t V, const uint32_t* off, const int32_t* len, uint32_t* nbr, const int32_t* kmax,
+                             uint32_t* mid_list, unsigned* mid_cnt, uint32_t* big_list, unsigned* big_cnt) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        int n = len[v];
+        if (n > kSortMid) {
+            big_list[atomicAdd(big_cnt, 1u)] = (uint32_t)v;
+            continue;
+        }
+        if (n > kSortShort) {
+            mid_list[atomicAdd(mid_cnt, 1u)] = (uint32_t)v;
+            continue;
+        }
+        if (n < 2) continue;
+        uint32_t* a = nbr + off[v];
+        uint32_t ids[kSortShort];
+        int ks[kSortShort];
+        for (int i = 0; i < n; ++i) {
+            ids[i] = a[i];
+            ks[i] = kmax[ids[i]];
+        }
+        for (int i = 1; i < n; ++i) {
+            uint32_t x = ids[i];
+            int kx = ks[i];
+            int jj = i - 1;
+            while (jj >= 0 && ks[jj] < kx) {
+                ids[jj + 1] = ids[jj];
+                ks[jj + 1] = ks[jj];
+                --jj;
+            }
+            ids[jj + 1] = x;
+            ks[jj + 1] = kx;
+        }
+        for (int i = 0; i < n; ++i) a[i] = ids[i];
+    }
+}
+
+__global__ void k_sort_mid(const uint32_t* off, const int32_t* len, uint32_t* nbr, const int32_t* kmax,
+                           const uint32_t* list, unsigned n_list) {
+    __shared__ unsigned long long sh[kSortMid];
+    for (unsigned li = blockIdx.x; li < n_list; li += gridDim.x) {
+        uint32_t v = list[li];
+        int n = len[v];
+        uint32_t* a = nbr + off[v];
+        int p2 = 1;
+        while (p2 < n) p2 <<= 1;
+        for (int i = threadIdx.x; i < p2; i += blockDim.x) {
+            if (i < n) {
+                uint32_t u = a[i];
+                // ascending order of (~kmax) gives kmax descending
+                sh[i] = ((unsigned long long)(0x7FFFFFFF - kmax[u]) << 32) | u;
+            } else {
+                sh[i] = ~0ull;
+            }
+        }
+        __syncthreads();
+        for (int kk = 2; kk <= p2; kk <<= 1) {
+            for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+                for (int i = threadIdx.x; i < p2; i += blockDim.x) {
+                    int ixj = i ^ jj;
+                    if (ixj > i) {
+                        bool up = (i & kk) == 0;
+                        unsigned long long x = sh[i], y = sh[ixj];
+                        if ((x > y) == up) {
+                            sh[i] = y;
+                            sh[ixj] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = (uint32_t)sh[i];
+        __syncthreads();
+    }
+}
+
+// bins = K + 1 counters in shared memory (K < kSortBigBins)
+static constexpr int kSortBigBins = 11264;
+__global__ void k_sort_big(const uint32_t* off, const int32_t* len, uint32_t* nbr, uint32_t* tmp, const int32_t* kmax,
+                           int K, const uint32_t* list, unsigned n_list) {
+    __shared__ unsigned bins[kSortBigBins];
+    for (unsigned li = blockIdx.x; li < n_list; li += gridDim.x) {
+        uint32_t v = list[li];
+        const int n = len[v];
+        uint32_t* a = nbr + off[v];
+        uint32_t* t = tmp + off[v];
+        for (int i = threadIdx.x; i <= K; i += blockDim.x) bins[i] = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&bins[K - kmax[a[i]]], 1u);
+        __syncthreads();
+        // exclusive scan of bins (K+1 values), chunked by blockDim
+        unsigned long long carry = 0;
+        for (int b0 = 0; b0 <= K; b0 += blockDim.x) {
+            int b = b0 + threadIdx.x;
+            unsigned long long x = b <= K ? bins[b] : 0ull;
+            unsigned long long tot;
+            unsigned long long ex = block_excl_scan64(x, &tot);
+            if (b <= K) bins[b] = (unsigned)(ex + carry);
+            carry += tot;
+            __syncthreads();
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            uint32_t u = a[i];
+            unsigned pos = atomicAdd(&bins[K - kmax[u]], 1u);
+            t[pos] = u;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = t[i];
+        __syncthreads();
     }
 }
 
@@ -936,6 +1149,16 @@ void free_scratch(dc_graph* h) {
     dfree(s->partial);
     dfree(s->cursor);
     if (s->tmp_edges) cudaFree(s->tmp_edges);
+    dfree(s->key2);
+    dfree(s->cdeg2);
+    dfree(s->rem2);
+    dfree(s->rem3);
+    dfree(s->cnt_out);
+    dfree(s->tring);
+    dfree(s->w_out_len);
+    dfree(s->w_in_len);
+    dfree(s->w_out_nbr);
+    dfree(s->w_in_nbr);
     delete s;
     h->scratch = nullptr;
 }
@@ -944,17 +1167,18 @@ int ensure_scratch(dc_graph* h, uint32_t V) {
     if (!h->scratch) h->scratch = new Scratch();
     Scratch* s = h->scratch;
     if (s->cap_V >= V && s->key) return DC_OK;
-    uint32_t keep_ck = s->ck_cap;
-    (void)keep_ck;
     // release V-sized buffers and reallocate
     dfree(s->key); dfree(s->cdeg); dfree(s->cur); dfree(s->row0); dfree(s->mark); dfree(s->stamp);
     dfree(s->logidx); dfree(s->rem0); dfree(s->rem1); dfree(s->order); dfree(s->ring); dfree(s->tmp64);
     dfree(s->partial); dfree(s->cursor);
+    dfree(s->key2); dfree(s->cdeg2); dfree(s->rem2); dfree(s->rem3); dfree(s->cnt_out);
     uint64_t n = (uint64_t)V + 1;
     if (dmalloc(&s->key, n) || dmalloc(&s->cdeg, n) || dmalloc(&s->cur, n) || dmalloc(&s->row0, n) ||
         dmalloc(&s->mark, n) || dmalloc(&s->stamp, n) || dmalloc(&s->logidx, n) || dmalloc(&s->rem0, n) ||
         dmalloc(&s->rem1, n) || dmalloc(&s->order, n) || dmalloc(&s->tmp64, n + 1) ||
-        dmalloc(&s->partial, (uint64_t)h->geom.sms * 64 + 64) || dmalloc(&s->cursor, n + 1))
+        dmalloc(&s->partial, (uint64_t)h->geom.sms * 64 + 64) || dmalloc(&s->cursor, n + 1) ||
+        dmalloc(&s->key2, n) || dmalloc(&s->cdeg2, n) || dmalloc(&s->rem2, n) || dmalloc(&s->rem3, n) ||
+        dmalloc(&s->cnt_out, n))
         return DC_ERR_NOMEM;
     uint64_t need = (uint64_t)V + (uint64_t)h->geom.sms * 64 * 32 + 64;
     uint64_t rc = 1024;
@@ -975,6 +1199,7 @@ static int scan_tmp64(dc_graph* h, uint64_t n) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_scan_coop, 256, 0);
     per_sm = std::max(1, std::min(per_sm, 8));
     DC_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
+    ++g_launches;
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_scan_coop, dim3(per_sm * h->geom.sms), dim3(256), args,
                                                 0, h->stream);
     if (e != cudaSuccess) return set_error(DC_ERR_CUDA, "scan launch failed: %s", cudaGetErrorString(e));
@@ -987,6 +1212,7 @@ static int finish_build(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_s
     // capacities -> offsets (out)
     for (int side = 0; side < 2; ++side) {
         int32_t* len = side == 0 ? g.out_len : g.in_len;
+        ++g_launches;
         k_capacity<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, len, h->gap_min, h->gap_div,
                                                                (unsigned long long*)s->tmp64);
         if (int rc = scan_tmp64(h, V)) return rc;
@@ -998,6 +1224,7 @@ static int finish_build(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_s
         uint32_t** off = side == 0 ? &g.out_off : &g.in_off;
         uint32_t** nbr = side == 0 ? &g.out_nbr : &g.in_nbr;
         if (dmalloc(off, (uint64_t)V + 1) || dmalloc(nbr, total)) return DC_ERR_NOMEM;
+        ++g_launches;
         k_off_to_u32<<<grid_for(h, (uint64_t)V + 1), kThreads, 0, h->stream>>>(V, (unsigned long long*)s->tmp64, *off);
         if (side == 0) g.out_cap = total;
         else g.in_cap = total;
@@ -1005,6 +1232,7 @@ static int finish_build(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_s
     DC_CUDA(cudaMemsetAsync(g.out_len, 0, sizeof(int32_t) * V, h->stream));
     DC_CUDA(cudaMemsetAsync(g.in_len, 0, sizeof(int32_t) * V, h->stream));
     if (E)
+        ++g_launches;
         k_scatter_edges<<<grid_for(h, E), kThreads, 0, h->stream>>>(E, d_src, d_dst, g.out_off, g.out_len, g.out_nbr,
                                                                      g.in_off, g.in_len, g.in_nbr);
     DC_CUDA(cudaGetLastError());
@@ -1094,6 +1322,7 @@ int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_d
     }
     cudaMemcpyAsync(s->tmp64, eo.data(), sizeof(unsigned long long) * ((size_t)V + 1), cudaMemcpyHostToDevice,
                     h->stream);
+    ++g_launches;
     k_csr_to_edges<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, h->stream>>>(
         V, d_off, d_deg, (const unsigned long long*)s->tmp64, d_nbr, d_src, d_dst, 0);
     cudaError_t e = cudaStreamSynchronize(h->stream);
@@ -1111,36 +1340,116 @@ int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_d
     return rc;
 }
 
-// which: 0 = kmax pass (peel in-degree), 1 = row pass (peel out-degree)
-int run_peel(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* d_val, int32_t* maxval, int sync) {
+static int ensure_tring(dc_graph* h, uint64_t need) {
+    Scratch* s = h->scratch;
+    uint64_t cap = 1024;
+    while (cap < need) cap <<= 1;
+    if (s->tring_cap >= cap && s->tring) return DC_OK;
+    dfree(s->tring);
+    s->tring_cap = 0;
+    if (dmalloc(&s->tring, cap)) return DC_ERR_NOMEM;
+    s->tring_cap = cap;
+    DC_CUDA(cudaMemsetAsync(s->tring, 0xFF, sizeof(unsigned long long) * cap, h->stream));
+    return DC_OK;
+}
+
+static int persistent_grid(dc_graph* h, const void* fn, int* blocks) {
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0);
+    if (e != cudaSuccess || per_sm < 1)
+        return set_error(DC_ERR_CUDA, "occupancy query failed (%s)", cudaGetErrorString(e));
+    per_sm = std::min(per_sm, h->blocks_per_sm > 0 ? h->blocks_per_sm : 1);
+    *blocks = per_sm * h->geom.sms;
+    return DC_OK;
+}
+
+// Launches a persistent kernel, waits, and converts its device status.
+static int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out) {
+    int blocks = 0;
+    if (int rc = persistent_grid(h, fn, &blocks)) return rc;
+    {
+        EngineCtl& init = h->ctl_init;
+        memset(&init, 0, sizeof(init));
+        init.step = -1;
+        init.trace = h->trace_dev;
+        init.trace_cap = h->trace_cap;
+        DC_CUDA(cudaMemcpyAsync(h->ctl, &init, sizeof(EngineCtl), cudaMemcpyHostToDevice, h->stream));
+        if (h->trace_dev)
+            DC_CUDA(cudaMemsetAsync(h->trace_dev, 0, 64ull * h->trace_cap, h->stream));
+    }
+    ++g_launches;
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kThreads), args, 0, h->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(DC_ERR_CUDA, "%s: cooperative launch failed (%s)", name, cudaGetErrorString(e));
+    }
+    int rc = check_ctl(h, out, name);
+    if (h->trace_dev && h->trace_host) {
+        cudaMemcpy(h->trace_host, h->trace_dev, 64ull * h->trace_cap, cudaMemcpyDeviceToHost);
+        h->trace_steps = (unsigned)std::max(0, out->step);
+        if (h->trace_cb) h->trace_cb(name, h->trace_host, h->trace_steps, h->trace_user);
+    }
+    if (rc != DC_OK) {
+        // a failed phase may leave items in the ring
+        cudaMemsetAsync(h->scratch->tring, 0xFF, sizeof(unsigned long long) * h->scratch->tring_cap, h->stream);
+        cudaStreamSynchronize(h->stream);
+    }
+    return rc;
+}
+
+static PeelInst make_inst(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* val, int slot) {
     DevGraph& g = h->g;
     Scratch* s = h->scratch;
-    PeelParams p;
-    p.V = g.V;
+    PeelInst I;
     if (which == 0) {
-        p.a_off = g.in_off; p.a_len = g.in_len; p.a_nbr = g.in_nbr;
-        p.b_off = g.out_off; p.b_len = g.out_len; p.b_nbr = g.out_nbr;
+        I.a_off = g.in_off; I.a_len = g.in_len; I.a_nbr = g.in_nbr;
+        I.b_off = g.out_off; I.b_len = g.out_len; I.b_nbr = g.out_nbr;
     } else {
-        p.a_off = g.out_off; p.a_len = g.out_len; p.a_nbr = g.out_nbr;
-        p.b_off = g.in_off; p.b_len = g.in_len; p.b_nbr = g.in_nbr;
+        I.a_off = g.out_off; I.a_len = g.out_len; I.a_nbr = g.out_nbr;
+        I.b_off = g.in_off; I.b_len = g.in_len; I.b_nbr = g.in_nbr;
     }
-    p.member = member;
-    p.k = k;
-    p.key = s->key;
-    p.cdeg = s->cdeg;
-    p.val = d_val;
-    p.rem0 = s->rem0;
-    p.rem1 = s->rem1;
-    p.q.slots = s->ring;
-    p.q.mask = s->ring_mask;
+    I.member = member;
+    I.k = k;
+    I.val = val;
+    if (slot == 0) {
+        I.key = s->key; I.cdeg = s->cdeg; I.rem0 = s->rem0; I.rem1 = s->rem1;
+    } else {
+        I.key = s->key2; I.cdeg = s->cdeg2; I.rem0 = s->rem2; I.rem1 = s->rem3;
+    }
+    return I;
+}
+
+static constexpr unsigned kPeelChunk = 64;
+
+// Runs one or two peels in one persistent launch; maxv[i] = largest value.
+static int run_peel2(dc_graph* h, int ninst, const PeelInst* inst, int32_t* maxv) {
+    Scratch* s = h->scratch;
+    DevGraph& g = h->g;
+    uint64_t need = 2ull * g.V + 2ull * (g.out_cap + g.in_cap) / kPeelChunk + (uint64_t)h->geom.sms * 64 + 4096;
+    if (int rc = ensure_tring(h, need)) return rc;
+    Peel2Params p;
+    p.V = g.V;
+    p.ninst = ninst;
+    p.chunk = kPeelChunk;
+    p.in[0] = inst[0];
+    p.in[1] = ninst > 1 ? inst[1] : inst[0];
+    p.q.slots = s->tring;
+    p.q.mask = (unsigned)(s->tring_cap - 1);
     p.ctl = h->ctl;
-    DC_CUDA(cudaMemsetAsync(s->ring, 0xFF, sizeof(uint32_t) * ((uint64_t)s->ring_mask + 1), h->stream));
     void* args[] = {&p};
-    if (int rc = coop_launch(h, (const void*)k_peel, args, kThreads, "peel")) return rc;
-    if (!sync) return DC_OK;
     EngineCtl hc;
-    if (int rc = check_ctl(h, &hc, "peel")) return rc;
-    if (maxval) *maxval = hc.maxval;
+    if (int rc = run_persistent(h, (const void*)k_peel2, args, "peel", &hc)) return rc;
+    for (int i = 0; i < ninst; ++i) maxv[i] = hc.maxv[i];
+    return DC_OK;
+}
+
+// which: 0 = kmax pass (peel in-degree), 1 = row pass (peel out-degree)
+int run_peel(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* d_val, int32_t* maxval, int sync) {
+    (void)sync;
+    PeelInst I = make_inst(h, which, member, k, d_val, 0);
+    int32_t mv = 0;
+    if (int rc = run_peel2(h, 1, &I, &mv)) return rc;
+    if (maxval) *maxval = mv;
     return DC_OK;
 }
 
@@ -1149,6 +1458,7 @@ static int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
     Decomp& d = h->d;
     uint32_t V = h->g.V;
     unsigned long long* cnt = (unsigned long long*)s->tmp64;
+    ++g_launches;
     k_set_one<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt);
     if (nlog) k_sky_count<<<grid_for(h, nlog), kThreads, 0, h->stream>>>(V, nlog, s->log_v, cnt);
     if (int rc = scan_tmp64(h, V)) return rc;
@@ -1160,10 +1470,13 @@ static int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
         d.corner_cap = total;
     }
     if (!d.sky_off && dmalloc(&d.sky_off, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+    ++g_launches;
     k_sky_fill_row0<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt, s->row0, d.sky_k, d.sky_l, s->cursor);
     if (nlog)
+        ++g_launches;
         k_sky_fill_log<<<grid_for(h, nlog), kThreads, 0, h->stream>>>(nlog, s->log_v, s->log_k, s->log_l, cnt, d.sky_k,
                                                                       d.sky_l, s->cursor);
+    ++g_launches;
     k_sky_sort<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt, d.sky_k, d.sky_l, d.sky_off);
     d.n_corners = total;
     DC_CUDA(cudaGetLastError());
@@ -1184,9 +1497,60 @@ int expand_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* d_dst) {
     Decomp& d = h->d;
     if (!d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
     if (n == 0) return DC_OK;
+    ++g_launches;
     k_expand<<<grid_for(h, h->g.V), kThreads, 0, h->stream>>>(h->g.V, k0, n, d.kmax_v, d.sky_off, d.sky_k, d.sky_l,
                                                                d_dst);
     DC_CUDA(cudaGetLastError());
+    return DC_OK;
+}
+
+// Orders every adjacency list by neighbour kmax, descending.  *sorted = 0
+// when kmax is too large for the long-list counting sort (lists then stay
+// in arbitrary order and evaluations read them whole).
+static int sort_lists_by_kmax(dc_graph* h, int32_t K, int* sorted) {
+    DevGraph& g = h->g;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    *sorted = 0;
+    if (g.sorted_kmax) {
+        *sorted = 1;
+        return DC_OK;
+    }
+    if (K + 1 > kSortBigBins) return DC_OK;
+    for (int side = 0; side < 2; ++side) {
+        const uint32_t* off = side == 0 ? g.out_off : g.in_off;
+        const int32_t* len = side == 0 ? g.out_len : g.in_len;
+        uint32_t* nbr = side == 0 ? g.out_nbr : g.in_nbr;
+        uint64_t cap = side == 0 ? g.out_cap : g.in_cap;
+        unsigned* cnt = s->cursor;
+        DC_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), h->stream));
+        ++g_launches;
+        k_sort_short<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, off, len, nbr, h->d.kmax_v, s->rem0, &cnt[0],
+                                                                  s->rem1, &cnt[1]);
+        unsigned hc[2] = {0, 0};
+        DC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, h->stream));
+        DC_CUDA(cudaStreamSynchronize(h->stream));
+        if (hc[0]) {
+            int blocks = (int)std::min<unsigned>(hc[0], (unsigned)h->geom.sms * 8);
+            ++g_launches;
+            k_sort_mid<<<blocks, 256, 0, h->stream>>>(off, len, nbr, h->d.kmax_v, s->rem0, hc[0]);
+        }
+        if (hc[1]) {
+            uint32_t*& tmp = side == 0 ? s->w_out_nbr : s->w_in_nbr;
+            uint64_t& tcap = side == 0 ? s->w_out_cap : s->w_in_cap;
+            if (tcap < cap || !tmp) {
+                dfree(tmp);
+                if (dmalloc(&tmp, cap)) return DC_ERR_NOMEM;
+                tcap = cap;
+            }
+            int blocks = (int)std::min<unsigned>(hc[1], (unsigned)h->geom.sms * 2);
+            ++g_launches;
+            k_sort_big<<<blocks, 512, 0, h->stream>>>(off, len, nbr, tmp, h->d.kmax_v, K, s->rem1, hc[1]);
+        }
+        DC_CUDA(cudaGetLastError());
+    }
+    g.sorted_kmax = true;
+    *sorted = 1;
     return DC_OK;
 }
 
@@ -1209,28 +1573,32 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
         return DC_OK;
     }
     cudaEventRecord(h->ev[0], h->stream);
-    int32_t K = 0;
-    if (int rc = run_peel(h, 0, nullptr, 0, d.kmax_v, &K, 1)) return rc;
+    // kmax (in-degree peel) and row 0 (out-degree peel) in one grid
+    int32_t mv[2] = {0, 0};
+    {
+        PeelInst I[2] = {make_inst(h, 0, nullptr, 0, d.kmax_v, 0), make_inst(h, 1, nullptr, 0, s->row0, 1)};
+        if (int rc = run_peel2(h, 2, I, mv)) return rc;
+    }
     cudaEventRecord(h->ev[1], h->stream);
+    const int32_t K = mv[0];
     d.kmax = K;
+    d.lmax = mv[1];
     if (method == 1) {
-        // one fresh peel per row (the reference's schedule, main.cu:238-244)
+        // one fresh peel per row (the reference's schedule, main.cu:238-244),
+        // two rows per launch
         if (int rc = ensure_rows(h, (uint64_t)(K + 1) * V)) return rc;
-        int32_t lm = 0;
-        for (int32_t k = 0; k <= K; ++k) {
-            int32_t mv = 0;
-            if (int rc = run_peel(h, 1, k == 0 ? nullptr : d.kmax_v, k, d.rows + (uint64_t)k * V, &mv, 1)) return rc;
+        DC_CUDA(cudaMemcpyAsync(d.rows, s->row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+        for (int32_t k = 1; k <= K; k += 2) {
+            int n = (k + 1 <= K) ? 2 : 1;
+            PeelInst I[2] = {make_inst(h, 1, d.kmax_v, k, d.rows + (uint64_t)k * V, 0),
+                             make_inst(h, 1, d.kmax_v, k + 1, d.rows + (uint64_t)(k + 1) * V, 1)};
+            int32_t m2[2];
+            if (int rc = run_peel2(h, n, I, m2)) return rc;
         }
-        EngineCtl hc;
-        if (int rc = check_ctl(h, &hc, "row peel")) return rc;
-        int* dmax = (int*)s->cursor;
-        DC_CUDA(cudaMemsetAsync(dmax, 0, sizeof(int), h->stream));
-        k_max_reduce<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.rows, dmax);
-        DC_CUDA(cudaMemcpyAsync(&lm, dmax, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         cudaEventRecord(h->ev[2], h->stream);
         cudaEventRecord(h->ev[3], h->stream);
-        // skyline from rows
         unsigned long long* cnt = (unsigned long long*)s->tmp64;
+        ++g_launches;
         k_rows_corner_count<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, K, d.kmax_v, d.rows, cnt);
         if (int rc = scan_tmp64(h, V)) return rc;
         unsigned long long total = 0;
@@ -1243,23 +1611,28 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
             d.corner_cap = total;
         }
         if (!d.sky_off && dmalloc(&d.sky_off, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+        ++g_launches;
         k_rows_corner_fill<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, d.rows, cnt, d.sky_k, d.sky_l,
                                                                         d.sky_off);
         d.n_corners = total;
-        d.lmax = lm;
         d.rows_valid = true;
         cudaEventRecord(h->ev[4], h->stream);
         cudaEventRecord(h->ev[5], h->stream);
+        cudaEventRecord(h->ev[6], h->stream);
         DC_CUDA(cudaStreamSynchronize(h->stream));
         d.valid = true;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+        h->times.kmax_ms = ms;
+        h->times.row0_ms = 0;
+        cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]);
+        h->times.trans_ms = ms;
+        cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
+        h->times.sky_ms = ms;
+        h->times.expand_ms = 0;
         return DC_OK;
     }
-    // ---- method 0: row 0 by peel, rows 1..K by incremental transitions
-    int32_t l0 = 0;
-    if (int rc = run_peel(h, 1, nullptr, 0, s->row0, &l0, 1)) return rc;
-    cudaEventRecord(h->ev[2], h->stream);
-    d.lmax = l0;
-    // order by kmax descending; ck[k] = |{v : kmax >= k}|
+    // ---- method 0: rows 1..K derived row to row
     if (s->ck_cap < (uint32_t)K + 2) {
         dfree(s->ck);
         if (dmalloc(&s->ck, (uint64_t)K + 2)) return DC_ERR_NOMEM;
@@ -1267,12 +1640,13 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     }
     uint32_t* hist = s->cursor;
     DC_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * ((uint64_t)K + 2), h->stream));
+    ++g_launches;
     k_kmax_hist<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist);
     std::vector<uint32_t> hh((size_t)K + 2), ck((size_t)K + 2), start((size_t)K + 2);
     DC_CUDA(cudaMemcpyAsync(hh.data(), hist, sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyDeviceToHost, h->stream));
-    // corner bound
     unsigned long long* acc = (unsigned long long*)s->tmp64;
     DC_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), h->stream));
+    ++g_launches;
     k_corner_bound<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, s->row0, acc);
     unsigned long long bound = 0;
     DC_CUDA(cudaMemcpyAsync(&bound, acc, sizeof(bound), cudaMemcpyDeviceToHost, h->stream));
@@ -1281,15 +1655,15 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
         uint64_t run = 0;
         ck[K + 1] = 0;
         for (int32_t k = K; k >= 0; --k) {
-            start[k] = (uint32_t)run;  // descending order: bucket K first
+            start[k] = (uint32_t)run;
             run += hh[k];
             ck[k] = (uint32_t)run;
         }
     }
     DC_CUDA(cudaMemcpyAsync(s->ck, ck.data(), sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyHostToDevice, h->stream));
     DC_CUDA(cudaMemcpyAsync(hist, start.data(), sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyHostToDevice, h->stream));
+    ++g_launches;
     k_order_scatter<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist, s->order);
-    // log capacity = corner bound
     uint64_t lc = bound + 1;
     if (s->log_cap < lc) {
         dfree(s->log_v);
@@ -1298,22 +1672,27 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
         if (dmalloc(&s->log_v, lc) || dmalloc(&s->log_k, lc) || dmalloc(&s->log_l, lc)) return DC_ERR_NOMEM;
         s->log_cap = lc;
     }
-    // transition state
+    // adjacency lists ordered by neighbour kmax (kept until the graph changes)
+    int sorted = 0;
+    if (int rc = sort_lists_by_kmax(h, K, &sorted)) return rc;
     DC_CUDA(cudaMemcpyAsync(s->cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, h->stream));
-    k_cnt_in_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, h->stream>>>(V, g.in_off, g.in_len, g.in_nbr, s->cur,
-                                                                             s->key);
+    ++g_launches;
+    k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, h->stream>>>(
+        V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, s->cur, s->cnt_out, s->key);
     DC_CUDA(cudaMemsetAsync(s->mark, 0, sizeof(uint32_t) * V, h->stream));
     DC_CUDA(cudaMemsetAsync(s->stamp, 0xFF, sizeof(int32_t) * V, h->stream));
-    DC_CUDA(cudaMemsetAsync(s->ring, 0xFF, sizeof(uint32_t) * ((uint64_t)s->ring_mask + 1), h->stream));
-    TransParams tp;
+    if (int rc = ensure_tring(h, 2ull * V + (uint64_t)h->geom.sms * 64 + 4096)) return rc;
+    Trans2Params tp;
     tp.V = V;
     tp.out_off = g.out_off; tp.out_len = g.out_len; tp.out_nbr = g.out_nbr;
     tp.in_off = g.in_off; tp.in_len = g.in_len; tp.in_nbr = g.in_nbr;
     tp.kmax = d.kmax_v;
     tp.K = K;
+    tp.sorted = sorted;
     tp.order = s->order;
     tp.ck = s->ck;
     tp.cur = s->cur;
+    tp.cnt_out = s->cnt_out;
     tp.cnt_in = s->key;
     tp.mark = s->mark;
     tp.stamp = s->stamp;
@@ -1322,19 +1701,19 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     tp.log_k = s->log_k;
     tp.log_l = s->log_l;
     tp.log_cap = s->log_cap;
-    tp.q.slots = s->ring;
-    tp.q.mask = s->ring_mask;
+    tp.q.slots = s->tring;
+    tp.q.mask = (unsigned)(s->tring_cap - 1);
     tp.ctl = h->ctl;
     cudaEventRecord(h->ev[3], h->stream);
     uint64_t nlog = 0;
     if (K >= 1) {
         void* args[] = {&tp};
-        if (int rc = coop_launch(h, (const void*)k_transitions, args, kThreads, "transitions")) return rc;
         EngineCtl hc;
-        if (int rc = check_ctl(h, &hc, "transitions")) return rc;
+        if (int rc = run_persistent(h, (const void*)k_trans2, args, "transitions", &hc)) return rc;
         nlog = hc.log_count;
         h->stat_evals = hc.evals;
         h->stat_drops = hc.drops;
+        h->stat_entries = hc.edges_scanned;
     }
     cudaEventRecord(h->ev[4], h->stream);
     if (int rc = build_skyline_from_log(h, nlog)) return rc;
@@ -1350,7 +1729,7 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
     h->times.kmax_ms = ms;
-    cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]);
+    cudaEventElapsedTime(&ms, h->ev[1], h->ev[3]);
     h->times.row0_ms = ms;
     cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
     h->times.trans_ms = ms;

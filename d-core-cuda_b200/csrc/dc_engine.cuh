@@ -31,6 +31,21 @@ struct Scratch {
     uint32_t* cursor = nullptr;  // [V+1]
     void* tmp_edges = nullptr;   // staging for uploaded edge arrays
     uint64_t tmp_edges_bytes = 0;
+    // second peel instance
+    int32_t* key2 = nullptr;
+    int32_t* cdeg2 = nullptr;
+    uint32_t* rem2 = nullptr;
+    uint32_t* rem3 = nullptr;
+    int32_t* cnt_out = nullptr;  // [V]
+    // ticket-queue ring
+    unsigned long long* tring = nullptr;
+    uint64_t tring_cap = 0;
+    // prunable working copies of the adjacency
+    int32_t* w_out_len = nullptr;
+    int32_t* w_in_len = nullptr;
+    uint32_t* w_out_nbr = nullptr;
+    uint32_t* w_in_nbr = nullptr;
+    uint64_t w_out_cap = 0, w_in_cap = 0;
 };
 
 // Allocation / release (all errors reported through set_error, return DC_*).

@@ -33,6 +33,7 @@ struct DevGraph {
     int32_t* in_len = nullptr;
     uint32_t* in_nbr = nullptr;
     uint64_t out_cap = 0, in_cap = 0;
+    bool sorted_kmax = false;  // lists ordered by neighbour kmax of the current graph
 };
 
 // Persistent-kernel launch geometry for the current device.
@@ -78,5 +79,14 @@ struct dc_graph {
     uint32_t gap_min = 1;      // minimum free slots per list
     uint32_t gap_div = 0;      // extra slack = len / gap_div (0 = none)
     int method = 0;            // 0 = incremental rows, 1 = per-row peel
-    uint64_t stat_evals = 0, stat_drops = 0;
+    int blocks_per_sm = 0;     // persistent-kernel blocks per SM (0 = default)
+    uint64_t stat_evals = 0, stat_drops = 0, stat_entries = 0;
+    dc::EngineCtl ctl_init{};
+    // optional per-step trace of persistent kernels (diagnostics)
+    unsigned long long* trace_dev = nullptr;
+    unsigned long long* trace_host = nullptr;
+    unsigned trace_cap = 0;
+    unsigned trace_steps = 0;
+    void (*trace_cb)(const char* phase, const unsigned long long* rec, unsigned steps, void* user) = nullptr;
+    void* trace_user = nullptr;
 };

@@ -48,7 +48,7 @@ class DecompInfo(ctypes.Structure):
     _fields_ = [("kmax", ctypes.c_int32), ("lmax", ctypes.c_int32), ("n_corners", ctypes.c_uint64),
                 ("kmax_ms", ctypes.c_float), ("row0_ms", ctypes.c_float), ("rows_ms", ctypes.c_float),
                 ("skyline_ms", ctypes.c_float), ("expand_ms", ctypes.c_float),
-                ("evals", ctypes.c_uint64), ("drops", ctypes.c_uint64)]
+                ("evals", ctypes.c_uint64), ("drops", ctypes.c_uint64), ("entries", ctypes.c_uint64)]
 
 
 # name -> argtypes; every function returns int status unless listed in _VOID / _STR
@@ -87,6 +87,9 @@ SIGNATURES = {
     "dc_host_free": [vp],
     "dc_synchronize": [vp],
     "dc_graph_stream": [vp, ctypes.POINTER(vp)],
+    "dc_set_trace": [vp, ctypes.c_uint32, vp, vp],
+    "dc_set_launch": [vp, ctypes.c_int],
+    "dc_launch_count": [u64p],
     "dc_last_error": [],
     "dc_version": [],
 }
@@ -125,10 +128,39 @@ def last_error():
     return lib().dc_last_error().decode()
 
 
+def launch_count():
+    n = ctypes.c_uint64(0)
+    _check(lib().dc_launch_count(ctypes.byref(n)))
+    return n.value
+
+
 def device_count():
     n = ctypes.c_int(0)
     _check(lib().dc_device_count(ctypes.byref(n)))
     return n.value
+
+
+# ---------------------------------------------------------------- pinned host memory
+_PINNED = {}
+
+
+def pinned_array(n, dtype):
+    """numpy array of n elements in pinned host memory (dc_host_alloc); it
+    stays allocated until free_pinned(arr) or process exit."""
+    dt = np.dtype(dtype)
+    nbytes = max(int(n) * dt.itemsize, 1)
+    p = vp()
+    _check(lib().dc_host_alloc(nbytes, ctypes.byref(p)))
+    buf = (ctypes.c_uint8 * nbytes).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=dt, count=int(n))
+    _PINNED[arr.ctypes.data] = (p.value, buf)
+    return arr
+
+
+def free_pinned(arr):
+    ent = _PINNED.pop(arr.ctypes.data, None)
+    if ent:
+        lib().dc_host_free(vp(ent[0]))
 
 
 # ---------------------------------------------------------------- generators
@@ -301,9 +333,10 @@ class Graph:
         _check(lib().dc_decomp_info_get(self._h, ctypes.byref(info)))
         return {f: getattr(info, f) for f, _ in DecompInfo._fields_}
 
-    def kmaxes(self):
+    def kmaxes(self, out=None):
         V = self.V
-        out = np.empty(max(V, 1), np.int32)
+        if out is None:
+            out = np.empty(max(V, 1), np.int32)
         _check(lib().dc_get_kmaxes(self._h, _p(out, i32p)))
         return out[:V]
 
@@ -342,6 +375,23 @@ class Graph:
 
     def write_decomp_cpu(self, path):
         _check(lib().dc_write_decomp_cpu(self._h, path.encode()))
+
+    def set_trace(self, max_steps, callback):
+        """callback(phase, records[steps, 4] uint64) after each persistent kernel."""
+        if callback is None:
+            _check(lib().dc_set_trace(self._h, 0, None, None))
+            self._trace_cb = None
+            return
+        CB = ctypes.CFUNCTYPE(None, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint, ctypes.c_void_p)
+
+        def _cb(phase, rec, steps, user):
+            arr = np.ctypeslib.as_array(rec, shape=(max_steps * 8,)).reshape(max_steps, 8)[:steps].copy()
+            callback(phase.decode(), arr)
+        self._trace_cb = CB(_cb)
+        _check(lib().dc_set_trace(self._h, max_steps, ctypes.cast(self._trace_cb, vp), None))
+
+    def set_launch(self, blocks_per_sm):
+        _check(lib().dc_set_launch(self._h, blocks_per_sm))
 
     def synchronize(self):
         _check(lib().dc_synchronize(self._h))

@@ -144,6 +144,7 @@ typedef struct dc_decomp_info {
     uint64_t n_corners; /* skyline corners stored on the device */
     float kmax_ms, row0_ms, rows_ms, skyline_ms, expand_ms;
     uint64_t evals, drops; /* row-to-row evaluations and value drops */
+    uint64_t entries;      /* adjacency entries read by the row-to-row kernel */
 } dc_decomp_info;
 int dc_decomp_info_get(dc_graph* g, dc_decomp_info* info);
 
@@ -165,6 +166,21 @@ int dc_get_skyline(dc_graph* g, uint32_t* off, int32_t* ks, int32_t* ls, uint64_
 /* writeDecompFile / writeDecompFileCPU of the current decomposition. */
 int dc_write_decomp(dc_graph* g, const char* path);
 int dc_write_decomp_cpu(dc_graph* g, const char* path);
+
+/* ---- diagnostics ------------------------------------------------------- */
+/* Per-step timing of the persistent kernels: after each kernel, fn is called
+ * with its phase name and `steps` records of 8 words (%globaltimer ns at step
+ * start, when the step's work ran out, queue items of the step,
+ * %globaltimer at the closing barrier, latest block wake-up, latest block
+ * seeding done, earliest block wake-up, unused).  max_steps = 0 turns
+ * tracing off. */
+typedef void (*dc_trace_fn)(const char* phase, const unsigned long long* rec, unsigned steps, void* user);
+int dc_set_trace(dc_graph* g, uint32_t max_steps, dc_trace_fn fn, void* user);
+/* Persistent-kernel blocks per SM (0 = default). */
+int dc_set_launch(dc_graph* g, int blocks_per_sm);
+
+/* Engine kernel launches since the library was loaded. */
+int dc_launch_count(unsigned long long* n);
 
 /* ---- utilities ----------------------------------------------------------- */
 int dc_host_alloc(uint64_t bytes, void** p); /* pinned host memory */

@@ -401,3 +401,65 @@ int64_t or_kedge_batches(uint32_t V, const int32_t* kmaxes, uint64_t B,
     free(root); free(rk); free(used); free(taken); free(members); free(cnt); free(order); free(fill);
     return nb;
 }
+
+/*
+ * CPU-baseline sample: rows k = 0, stride, 2*stride, ... <= kmax of the
+ * decomposition above, in parallel over `threads` threads (<= 0: all), each
+ * into a per-thread scratch row.  Returns the number of rows computed (or a
+ * negative error); *row_seconds receives the summed per-row wall time.  Used to time the CPU path on a bounded share of a large
+ * decomposition; the full time is extrapolated by the caller.
+ */
+int64_t or_rows_sample(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, int threads,
+                       const int32_t* kmaxes, int32_t kmax, int32_t stride, double* row_seconds) {
+    or_graph g;
+    if (or_graph_build(V, E, src, dst, &g) != OR_OK) return -2;
+    uint64_t mo = max_list(V, g.out_off);
+    int nt = threads;
+#ifdef _OPENMP
+    if (nt <= 0) nt = omp_get_max_threads();
+#else
+    nt = 1;
+#endif
+    if (stride < 1) stride = 1;
+    int64_t nrows = (int64_t)kmax / stride + 1;
+    if (nt > nrows) nt = (int)nrows;
+    int failed = 0;
+    double secs = 0.0;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nt) reduction(| : failed) reduction(+ : secs)
+#endif
+    {
+        or_scratch s;
+        int32_t* out = (int32_t*)malloc(((size_t)V + 1) * sizeof(int32_t));
+        if (scratch_init(&s, V, mo) != OR_OK || !out) failed = 1;
+        else {
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+            for (int64_t r = 0; r < nrows; ++r) {
+                int32_t k = (int32_t)(r * stride);
+#ifdef _OPENMP
+                double t0 = omp_get_wtime();
+#endif
+                or_bz_pass(V, g.out_off, g.out_nbr, g.in_off, g.in_nbr, kmaxes, k, out, &s);
+#ifdef _OPENMP
+                secs += omp_get_wtime() - t0;
+#endif
+            }
+        }
+        free(out);
+        scratch_free(&s);
+    }
+    or_graph_free(&g);
+    if (row_seconds) *row_seconds = secs;
+    return failed ? -3 : nrows;
+}
+
+/* Number of threads the oracle's parallel regions use by default. */
+int or_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

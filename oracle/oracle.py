@@ -106,3 +106,26 @@ def kedge_batches(V, kmaxes, frm, to):
     out = np.empty(max(len(frm), 1), np.int64)
     nb = lib().or_kedge_batches(V, _ptr(kmaxes, i32p), len(frm), _ptr(frm, u32p), _ptr(to, u32p), _ptr(out, i64p))
     return nb, out[:len(frm)]
+
+
+def rows_sample(V, src, dst, kmaxes, kmax, stride, threads=0):
+    """Computes rows 0, stride, ... <= kmax in parallel; returns (rows
+    computed, summed per-row seconds)."""
+    L = lib()
+    L.or_rows_sample.argtypes = [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_int, i32p, ctypes.c_int32,
+                                 ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+    L.or_rows_sample.restype = ctypes.c_int64
+    src, dst = _u32(src), _u32(dst)
+    kmaxes = np.ascontiguousarray(kmaxes, np.int32)
+    secs = ctypes.c_double(0)
+    n = L.or_rows_sample(V, len(src), _ptr(src, u32p), _ptr(dst, u32p), threads, _ptr(kmaxes, i32p), kmax, stride,
+                         ctypes.byref(secs))
+    if n < 0:
+        raise RuntimeError(f"oracle or_rows_sample failed: {n}")
+    return n, secs.value
+
+
+def max_threads():
+    L = lib()
+    L.or_max_threads.restype = ctypes.c_int
+    return L.or_max_threads()
