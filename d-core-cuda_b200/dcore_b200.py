@@ -89,6 +89,7 @@ SIGNATURES = {
     "dc_graph_stream": [vp, ctypes.POINTER(vp)],
     "dc_set_trace": [vp, ctypes.c_uint32, vp, vp],
     "dc_set_launch": [vp, ctypes.c_int],
+    "dc_kmax_noalloc": [ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp, vp, i32p, vp],
     "dc_launch_count": [u64p],
     "dc_last_error": [],
     "dc_version": [],

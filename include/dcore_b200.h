@@ -167,6 +167,25 @@ int dc_get_skyline(dc_graph* g, uint32_t* off, int32_t* ks, int32_t* ls, uint64_
 int dc_write_decomp(dc_graph* g, const char* path);
 int dc_write_decomp_cpu(dc_graph* g, const char* path);
 
+/* kmax of every vertex (in-degree core numbers, the values dc_decompose
+ * reports through dc_get_kmaxes) without allocating any device memory.  No
+ * counterpart in the reference: it is for callers that cannot let a library
+ * call cudaMalloc -- code that owns all device memory through its own pool,
+ * or serving loops where cudaMalloc's device-wide synchronisation would stall
+ * other work.  The graph comes as plain device arrays: in_off[V+1] (CSC
+ * offsets; in-degree of v = in_off[v+1] - in_off[v]), out_off[V+1] and
+ * out_nbr[E] (CSR).  kmax[V] is written on the device, the largest value to
+ * *kmax_max (may be NULL); the call waits for the GPU before returning.
+ * Limits: V <= 262,144 and E <= 4,194,304 (DC_ERR_CAPACITY beyond).  All
+ * intermediate state lives in one fixed device array of about 11 MB that
+ * this library reserves on every GPU that loads it, until process exit; all
+ * calls share it, so calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on each device looks up that
+ * array's address (cudaGetSymbolAddress) and should come before any stream
+ * capture on that device.  stream is a cudaStream_t (NULL: default stream). */
+int dc_kmax_noalloc(uint32_t V, uint64_t E, const uint32_t* d_in_off, const uint32_t* d_out_off,
+                    const uint32_t* d_out_nbr, int32_t* d_kmax, int32_t* kmax_max, void* stream);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* Per-step timing of the persistent kernels: after each kernel, fn is called
  * with its phase name and `steps` records of 8 words (%globaltimer ns at step
