@@ -267,6 +267,13 @@ extern "C" int dc_decompose(dc_graph* h, int method, int32_t* kmax, int32_t* lma
     return DC_OK;
 }
 
+extern "C" int dc_maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_delete, uint64_t b, int method,
+                           dc_maint_stats* stats) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    API_CUDA(cudaSetDevice(h->device));
+    return maintain(h, pairs, is_delete, b, method, stats);
+}
+
 extern "C" int dc_decomp_info_get(dc_graph* h, dc_decomp_info* info) {
     if (!h || !info) return set_error(DC_ERR_INVALID, "null argument");
     if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");

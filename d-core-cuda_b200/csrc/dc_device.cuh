@@ -55,6 +55,9 @@ struct EngineCtl {
     int maxv[2];            // largest value per peel instance
     int step;               // level / transition index
     unsigned nworkers;      // producers per phase (warps in the grid)
+    int level;              // current level / row of the persistent loop
+    int next_min;           // smallest level / row a skipped step may jump to
+    int minkey[2];          // per peel instance: least peeling degree kept by the scan
     // optional per-step timing trace: 8 words per step
     //   [0] %globaltimer at step start, [1] when its work ran out,
     //   [2] queue items of the step, [3] %globaltimer at the closing barrier,
@@ -335,6 +338,33 @@ __device__ __forceinline__ void tq_push_warp(EngineCtl* c, TicketQueue q, bool p
         __threadfence();
         volatile unsigned long long* s = &q.slots[(base + __popc(m & ((1u << lane) - 1u))) & q.mask];
         *s = item;
+    }
+}
+
+// Converged warp: each lane pushes its first cnt (<= 4) entries of items[].
+__device__ __forceinline__ void tq_push_warp4(EngineCtl* c, TicketQueue q, unsigned cnt, const uint32_t* items) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (unsigned)o) x += y;
+    }
+    unsigned total = __shfl_sync(0xFFFFFFFFu, x, 31);
+    if (total == 0) return;
+    unsigned base = 0;
+    if (lane == 0) {
+        atomicAdd(&c->outstanding, (int)total);
+        base = atomicAdd(&c->t_tail, total);
+    }
+    base = __shfl_sync(0xFFFFFFFFu, base, 0) + (x - cnt);
+    if (cnt) __threadfence();
+#pragma unroll
+    for (unsigned i = 0; i < 4; ++i) {
+        if (i < cnt) {
+            volatile unsigned long long* s = &q.slots[(base + i) & q.mask];
+            *s = (unsigned long long)items[i];
+        }
     }
 }
 

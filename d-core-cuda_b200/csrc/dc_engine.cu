@@ -275,9 +275,23 @@ struct PeelHook {
     int ninst;
     unsigned nworkers;
     __device__ void operator()(EngineCtl* c) const {
+        // next level: a level whose scan found nothing to remove changed no
+        // degree, so the following levels up to the least degree kept are
+        // empty too and are skipped
+        if (c->step < 0) {
+            c->level = 0;
+        } else if (c->t_tail == c->trace_tail0) {
+            int m = 0x7FFFFFFF;
+            for (int i = 0; i < ninst; ++i)
+                if (c->rc_next[i]) m = min(m, c->minkey[i]);
+            c->level = max(c->level + 1, m == 0x7FFFFFFF ? c->level + 1 : m);
+        } else {
+            c->level = c->level + 1;
+        }
         for (int i = 0; i < ninst; ++i) {
             c->rc_cur[i] = c->rc_next[i];
             c->rc_next[i] = 0;
+            c->minkey[i] = 0x7FFFFFFF;
         }
         trace_step_end(c);
         c->t_tail = c->t_head;
@@ -340,7 +354,8 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
     if (!grid_sync_hook(c, hook)) return;
 
     unsigned ticket = kNoTicket;
-    for (int L = 0;; ++L) {
+    for (int it = 0;; ++it) {
+        const int L = ld_vol(&c->level);
         bool any_left = false;
         for (int i = 0; i < p.ninst; ++i) any_left |= ld_vol(&c->rc_cur[i]) != 0u;
         if (!any_left) break;
@@ -349,18 +364,22 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
         for (int i = 0; i < p.ninst; ++i) {
             const PeelInst& I = p.in[i];
             const unsigned n_rem = ld_vol(&c->rc_cur[i]);
-            const uint32_t* rc = (L & 1) ? I.rem1 : I.rem0;
-            uint32_t* rn = (L & 1) ? I.rem0 : I.rem1;
+            const uint32_t* rc = (it & 1) ? I.rem1 : I.rem0;
+            uint32_t* rn = (it & 1) ? I.rem0 : I.rem1;
+            int kmin = 0x7FFFFFFF;
             for (unsigned base = gwarp * 32; base < n_rem; base += nwarps * 32) {
                 unsigned idx = base + lane;
                 bool ok = idx < n_rem;
                 uint32_t v = ok ? rc[idx] : 0;
                 bool keep = false, push = false;
                 if (ok && ld_vol(&I.val[v]) == -1) {
-                    if (ld_vol(&I.key[v]) <= L)
+                    int kv = ld_vol(&I.key[v]);
+                    if (kv <= L) {
                         push = atomicCAS(&I.val[v], -1, L) == -1;
-                    else
+                    } else {
                         keep = true;
+                        kmin = min(kmin, kv);
+                    }
                 }
                 unsigned pos = warp_append(&c->rc_next[i], keep);
                 if (keep) rn[pos] = v;
@@ -368,6 +387,9 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
                 tq_push_warp_multi(c, p.q, cnt, peel_item(v, 0, i), 1ull << 32);
                 if (__any_sync(0xFFFFFFFFu, push)) pushed_mask |= 1u << i;
             }
+#pragma unroll
+            for (int s = 16; s; s >>= 1) kmin = min(kmin, __shfl_xor_sync(0xFFFFFFFFu, kmin, s));
+            if (lane == 0 && kmin != 0x7FFFFFFF) atomicMin(&c->minkey[i], kmin);
         }
         block_producer_done(c, &s_prod);
         // ---- drain the cascade
@@ -433,7 +455,8 @@ struct Trans2Params {
     uint32_t* in_nbr;
     const int32_t* kmax;
     int32_t K;
-    int sorted;  // lists ordered by neighbour kmax, descending
+    int32_t Kstop;  // last row to compute (rows above stay untouched)
+    int sorted;     // lists ordered by neighbour kmax, descending
     const uint32_t* order;
     const uint32_t* ck;
     int32_t* cur;
@@ -452,7 +475,14 @@ struct Trans2Params {
 
 struct TransHook {
     unsigned nworkers;
+    int K;
     __device__ void operator()(EngineCtl* c) const {
+        // next row: after a row that needed no work, jump to the first row
+        // whose leaving set or seed set can be non-empty (next_min)
+        if (c->step < 0) c->level = 1;
+        else if (c->t_tail == c->trace_tail0) c->level = max(c->level + 1, c->next_min);
+        else c->level = c->level + 1;
+        c->next_min = K + 1;
         trace_step_end(c);
         c->t_tail = c->t_head;
         c->trace_tail0 = c->t_tail;
@@ -528,6 +558,58 @@ __device__ __forceinline__ int hist_pass(const int32_t* cur, const uint32_t* a, 
     return min(b, n);
 }
 
+// After x dropped from cap to nv (value already written): counts the
+// neighbours of one list with value >= nv into *cnt (this lane's share) and
+// takes x's support away from neighbours whose level lies in (nv, cap]:
+// out-neighbours lose one unit of cnt_in (unstable below j), in-neighbours
+// one unit of cnt_out (unstable below their own value).  Four entries per
+// lane per step; stops like hist_pass on kmax-sorted lists.  Returns the
+// entries read.
+__device__ __forceinline__ int recount_pass(const Trans2Params& p, EngineCtl* c, const uint32_t* a, int n, int nv,
+                                            int cap, int j, bool out_list, int* cnt) {
+    const unsigned lane = threadIdx.x & 31u;
+    int b = 0;
+    for (; b < n; b += 128) {
+        uint32_t u[4];
+        int cu[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int e = b + r * 32 + (int)lane;
+            u[r] = e < n ? a[e] : 0u;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int e = b + r * 32 + (int)lane;
+            cu[r] = e < n ? ld_vol(&p.cur[u[r]]) : -1;
+        }
+        uint32_t req[4];
+        unsigned nreq = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int x = cu[r];
+            *cnt += (x >= nv);
+            if (x > nv && x <= cap) {
+                if (out_list) {
+                    int old = atomicSub(&p.cnt_in[u[r]], 1);
+                    if (old - 1 < j && mark_request(&p.mark[u[r]], c)) req[nreq++] = u[r];
+                } else {
+                    int old = atomicSub(&p.cnt_out[u[r]], 1);
+                    if (old - 1 < x && mark_request(&p.mark[u[r]], c)) req[nreq++] = u[r];
+                }
+            }
+        }
+        tq_push_warp4(c, p.q, nreq, req);
+        int last = min(b + 127, n - 1) - b;
+        int rr = last >> 5;
+        int mine = rr == 0 ? cu[0] : rr == 1 ? cu[1] : rr == 2 ? cu[2] : cu[3];
+        if (p.sorted && __shfl_sync(0xFFFFFFFFu, mine, last & 31) == -1) {
+            b += 128;
+            break;
+        }
+    }
+    return min(b, n);
+}
+
 __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
     const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const unsigned gwarp = blockIdx.x * kWarpsPerBlock + wib;
@@ -537,16 +619,22 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
     __shared__ int s_hi[kWarpsPerBlock][kWin];
     int* ho = s_ho[wib];
     int* hi_ = s_hi[wib];
-    TransHook hook{gridDim.x};
+    TransHook hook{gridDim.x, p.Kstop};
     unsigned long long my_evals = 0, my_drops = 0, my_entries = 0;
     unsigned ticket = kNoTicket;
     __shared__ unsigned s_prod;
     if (threadIdx.x == 0) s_prod = 0;
     if (!grid_sync_hook(c, hook)) return;
 
-    for (int j = 1; j <= p.K; ++j) {
-        const uint32_t vj = p.ck[j], vprev = p.ck[j - 1];
+    int jprev = 0;  // row currently held in cur
+    for (;;) {
+        const int j = ld_vol(&c->level);
+        if (j > p.Kstop) break;
+        // rows jprev+1 .. j-1 equal row jprev; vertices with kmax in
+        // [jprev, j-1] leave now (all but those with kmax == j-1 have value 0)
+        const uint32_t vj = p.ck[j], vprev = p.ck[jprev];
         // ---- vertices leaving C_j: value -1; neighbours they supported lose one count
+        int lmin = 0x7FFFFFFF;  // bound on the next row that can need work (see hook)
         for (uint32_t i = vj + gwarp; i < vprev; i += nwarps) {
             uint32_t x = p.order[i];
             int a = ld_vol(&p.cur[x]);
@@ -569,7 +657,8 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
                     cz = ld_vol(&p.cur[z]);
                     if (cz >= 1 && cz <= a) {
                         int old = atomicSub(&p.cnt_in[z], 1);
-                        req = (old - 1 < j) && mark_request(&p.mark[z], c);
+                        if (old - 1 < j) req = mark_request(&p.mark[z], c);
+                        else lmin = min(lmin, min(old - 1, p.kmax[z]) + 1);
                     }
                 }
                 tq_push_warp(c, p.q, req, z);
@@ -595,17 +684,30 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
                 if (p.sorted && __shfl_sync(0xFFFFFFFFu, cy, last) == -1) break;
             }
         }
-        // ---- seeds: members whose in-count at their own level is below j
+#pragma unroll
+        for (int s = 16; s; s >>= 1) lmin = min(lmin, __shfl_xor_sync(0xFFFFFFFFu, lmin, s));
+        if (lane == 0 && lmin != 0x7FFFFFFF) atomicMin(&c->next_min, lmin);
+        // ---- seeds: members whose in-count at their own level is below j;
+        // the least min(cnt_in, kmax) + 1 of the others bounds the next row
+        // that can need work
+        int jmin = 0x7FFFFFFF;
         for (uint32_t base = gwarp * 32; base < vj; base += nwarps * 32) {
             uint32_t i = base + lane;
             bool req = false;
             uint32_t v = 0;
             if (i < vj) {
                 v = p.order[i];
-                req = ld_vol(&p.cur[v]) >= 1 && ld_vol(&p.cnt_in[v]) < j && mark_request(&p.mark[v], c);
+                if (ld_vol(&p.cur[v]) >= 1) {
+                    int ci = ld_vol(&p.cnt_in[v]);
+                    if (ci < j) req = mark_request(&p.mark[v], c);
+                    else jmin = min(jmin, min(ci, p.kmax[v]) + 1);
+                }
             }
             tq_push_warp(c, p.q, req, v);
         }
+#pragma unroll
+        for (int s = 16; s; s >>= 1) jmin = min(jmin, __shfl_xor_sync(0xFFFFFFFFu, jmin, s));
+        if (lane == 0 && jmin != 0x7FFFFFFF) atomicMin(&c->next_min, jmin);
         block_producer_done(c, &s_prod);
 
         // ---- drain
@@ -632,7 +734,8 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
             }
             __threadfence();
             const uint32_t oo = p.out_off[x], io = p.in_off[x];
-            // ---- new value from windowed histograms (first pass prunes)
+            const unsigned long long ev_entries0 = my_entries;
+            // ---- new value from windowed histograms
             int carry_o = 0, carry_i = 0, hi = cap, nv = -1, c_o = 0, c_i = 0;
             bool first = true;
             for (;;) {
@@ -696,6 +799,11 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
                 __syncwarp();
             }
             ++my_evals;
+            if (c->trace && lane == 0) {
+                int st = ld_vol(&c->step);
+                if (st >= 0 && (unsigned)st < c->trace_cap)
+                    atomicMax(&c->trace[8 * st + 7], (unsigned long long)(my_entries - ev_entries0));
+            }
             if (nv < cap) {
                 ++my_drops;
                 if (lane == 0) {
@@ -722,44 +830,9 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
                 // from neighbours whose level lies in (nv, cap]
                 c_o = 0;
                 c_i = 0;
-                int n = p.out_len[x];
-                for (int b = 0; b < n; b += 32) {
-                    bool req = false;
-                    uint32_t z = 0;
-                    int cz = -1;
-                    if (b + (int)lane < n) {
-                        z = p.out_nbr[oo + b + lane];
-                        cz = ld_vol(&p.cur[z]);
-                        c_o += (cz >= nv);
-                        if (cz > nv && cz <= cap) {
-                            int old = atomicSub(&p.cnt_in[z], 1);
-                            req = (old - 1 < j) && mark_request(&p.mark[z], c);
-                        }
-                    }
-                    tq_push_warp(c, p.q, req, z);
-                    int last = min(31, n - 1 - b);
-                    my_entries += last + 1;
-                    if (p.sorted && __shfl_sync(0xFFFFFFFFu, cz, last) == -1) break;
-                }
-                n = p.in_len[x];
-                for (int b = 0; b < n; b += 32) {
-                    bool req = false;
-                    uint32_t y = 0;
-                    int cy = -1;
-                    if (b + (int)lane < n) {
-                        y = p.in_nbr[io + b + lane];
-                        cy = ld_vol(&p.cur[y]);
-                        c_i += (cy >= nv);
-                        if (cy > nv && cy <= cap) {
-                            int old = atomicSub(&p.cnt_out[y], 1);
-                            req = (old - 1 < cy) && mark_request(&p.mark[y], c);
-                        }
-                    }
-                    tq_push_warp(c, p.q, req, y);
-                    int last = min(31, n - 1 - b);
-                    my_entries += last + 1;
-                    if (p.sorted && __shfl_sync(0xFFFFFFFFu, cy, last) == -1) break;
-                }
+                // out-neighbours z hold x in cnt_in; in-neighbours y hold x in cnt_out
+                my_entries += recount_pass(p, c, p.out_nbr + oo, p.out_len[x], nv, cap, j, true, &c_o);
+                my_entries += recount_pass(p, c, p.in_nbr + io, p.in_len[x], nv, cap, j, false, &c_i);
 #pragma unroll
                 for (int s = 16; s; s >>= 1) {
                     c_o += __shfl_xor_sync(0xFFFFFFFFu, c_o, s);
@@ -786,6 +859,7 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
             tq_push_warp(c, p.q, requeue, x);
             if (lane == 0) tq_finish(c, 1);
         }
+        jprev = j;
         if (!grid_sync_hook(c, hook)) break;
     }
     if (lane == 0) {
@@ -1079,7 +1153,7 @@ int coop_launch(dc_graph* h, const void* fn, void** args, int threads, const cha
     return DC_OK;
 }
 
-static int check_ctl(dc_graph* h, EngineCtl* hc, const char* what) {
+int check_ctl(dc_graph* h, EngineCtl* hc, const char* what) {
     DC_CUDA(cudaMemcpyAsync(hc, h->ctl, sizeof(EngineCtl), cudaMemcpyDeviceToHost, h->stream));
     DC_CUDA(cudaStreamSynchronize(h->stream));
     if (hc->error) {
@@ -1117,6 +1191,7 @@ void free_graph_arrays(DevGraph& g) {
 
 void free_decomp(Decomp& d) {
     dfree(d.kmax_v);
+    dfree(d.row0);
     dfree(d.sky_off);
     dfree(d.sky_k);
     dfree(d.sky_l);
@@ -1159,6 +1234,8 @@ void free_scratch(dc_graph* h) {
     dfree(s->w_in_len);
     dfree(s->w_out_nbr);
     dfree(s->w_in_nbr);
+    dfree(s->kmax_old);
+    dfree(s->row0_old);
     delete s;
     h->scratch = nullptr;
 }
@@ -1190,7 +1267,7 @@ int ensure_scratch(dc_graph* h, uint32_t V) {
 }
 
 // Exclusive scan of n u64 values in s->tmp64 (tmp64[n] receives the total).
-static int scan_tmp64(dc_graph* h, uint64_t n) {
+int scan_tmp64(dc_graph* h, uint64_t n) {
     Scratch* s = h->scratch;
     unsigned long long* data = (unsigned long long*)s->tmp64;
     unsigned long long* part = (unsigned long long*)s->partial;
@@ -1238,6 +1315,7 @@ static int finish_build(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_s
     DC_CUDA(cudaGetLastError());
     g.V = V;
     g.E = E;
+    g.sorted_kmax = false;
     return DC_OK;
 }
 
@@ -1340,7 +1418,7 @@ int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_d
     return rc;
 }
 
-static int ensure_tring(dc_graph* h, uint64_t need) {
+int ensure_tring(dc_graph* h, uint64_t need) {
     Scratch* s = h->scratch;
     uint64_t cap = 1024;
     while (cap < need) cap <<= 1;
@@ -1364,7 +1442,7 @@ static int persistent_grid(dc_graph* h, const void* fn, int* blocks) {
 }
 
 // Launches a persistent kernel, waits, and converts its device status.
-static int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out) {
+int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out) {
     int blocks = 0;
     if (int rc = persistent_grid(h, fn, &blocks)) return rc;
     {
@@ -1397,7 +1475,7 @@ static int run_persistent(dc_graph* h, const void* fn, void** args, const char* 
     return rc;
 }
 
-static PeelInst make_inst(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* val, int slot) {
+PeelInst make_inst(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* val, int slot) {
     DevGraph& g = h->g;
     Scratch* s = h->scratch;
     PeelInst I;
@@ -1422,7 +1500,7 @@ static PeelInst make_inst(dc_graph* h, int which, const int32_t* member, int32_t
 static constexpr unsigned kPeelChunk = 64;
 
 // Runs one or two peels in one persistent launch; maxv[i] = largest value.
-static int run_peel2(dc_graph* h, int ninst, const PeelInst* inst, int32_t* maxv) {
+int run_peel2(dc_graph* h, int ninst, const PeelInst* inst, int32_t* maxv) {
     Scratch* s = h->scratch;
     DevGraph& g = h->g;
     uint64_t need = 2ull * g.V + 2ull * (g.out_cap + g.in_cap) / kPeelChunk + (uint64_t)h->geom.sms * 64 + 4096;
@@ -1443,6 +1521,15 @@ static int run_peel2(dc_graph* h, int ninst, const PeelInst* inst, int32_t* maxv
     return DC_OK;
 }
 
+int peel_kmax_row0(dc_graph* h, int32_t* kmax, int32_t* lmax) {
+    int32_t mv[2] = {0, 0};
+    PeelInst I[2] = {make_inst(h, 0, nullptr, 0, h->d.kmax_v, 0), make_inst(h, 1, nullptr, 0, h->scratch->row0, 1)};
+    if (int rc = run_peel2(h, 2, I, mv)) return rc;
+    *kmax = mv[0];
+    *lmax = mv[1];
+    return DC_OK;
+}
+
 // which: 0 = kmax pass (peel in-degree), 1 = row pass (peel out-degree)
 int run_peel(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* d_val, int32_t* maxval, int sync) {
     (void)sync;
@@ -1453,7 +1540,7 @@ int run_peel(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* 
     return DC_OK;
 }
 
-static int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
+int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
     Scratch* s = h->scratch;
     Decomp& d = h->d;
     uint32_t V = h->g.V;
@@ -1554,6 +1641,107 @@ static int sort_lists_by_kmax(dc_graph* h, int32_t K, int* sorted) {
     return DC_OK;
 }
 
+// Rows 1..Kstop from row 0 (scratch row0) and kmax (d.kmax_v): orders
+// vertices by kmax, initialises the support counters and runs the
+// row-to-row kernel.  Corners of rows 1..Kstop are left in the scratch log
+// (*nlog entries).  allow_sort: order adjacency lists by neighbour kmax
+// first (otherwise lists are read whole).
+int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out) {
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    *nlog_out = 0;
+    cudaEventRecord(h->ev[2], h->stream);
+    if (s->ck_cap < (uint32_t)K + 2) {
+        dfree(s->ck);
+        if (dmalloc(&s->ck, (uint64_t)K + 2)) return DC_ERR_NOMEM;
+        s->ck_cap = K + 2;
+    }
+    uint32_t* hist = s->cursor;
+    DC_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * ((uint64_t)K + 2), h->stream));
+    ++g_launches;
+    k_kmax_hist<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist);
+    std::vector<uint32_t> hh((size_t)K + 2), ck((size_t)K + 2), start((size_t)K + 2);
+    DC_CUDA(cudaMemcpyAsync(hh.data(), hist, sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyDeviceToHost, h->stream));
+    unsigned long long* acc = (unsigned long long*)s->tmp64;
+    DC_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), h->stream));
+    ++g_launches;
+    k_corner_bound<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, s->row0, acc);
+    unsigned long long bound = 0;
+    DC_CUDA(cudaMemcpyAsync(&bound, acc, sizeof(bound), cudaMemcpyDeviceToHost, h->stream));
+    DC_CUDA(cudaStreamSynchronize(h->stream));
+    {
+        uint64_t run = 0;
+        ck[K + 1] = 0;
+        for (int32_t k = K; k >= 0; --k) {
+            start[k] = (uint32_t)run;
+            run += hh[k];
+            ck[k] = (uint32_t)run;
+        }
+    }
+    DC_CUDA(cudaMemcpyAsync(s->ck, ck.data(), sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyHostToDevice, h->stream));
+    DC_CUDA(cudaMemcpyAsync(hist, start.data(), sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyHostToDevice, h->stream));
+    ++g_launches;
+    k_order_scatter<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist, s->order);
+    uint64_t lc = bound + 1;
+    if (s->log_cap < lc) {
+        dfree(s->log_v);
+        dfree(s->log_k);
+        dfree(s->log_l);
+        if (dmalloc(&s->log_v, lc) || dmalloc(&s->log_k, lc) || dmalloc(&s->log_l, lc)) return DC_ERR_NOMEM;
+        s->log_cap = lc;
+    }
+    // adjacency lists ordered by neighbour kmax (kept until the graph changes)
+    int sorted = 0;
+    if (allow_sort || g.sorted_kmax)
+        if (int rc = sort_lists_by_kmax(h, K, &sorted)) return rc;
+    DC_CUDA(cudaMemcpyAsync(s->cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, h->stream));
+    ++g_launches;
+    k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, h->stream>>>(
+        V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, s->cur, s->cnt_out, s->key);
+    DC_CUDA(cudaMemsetAsync(s->mark, 0, sizeof(uint32_t) * V, h->stream));
+    DC_CUDA(cudaMemsetAsync(s->stamp, 0xFF, sizeof(int32_t) * V, h->stream));
+    if (int rc = ensure_tring(h, 2ull * V + (uint64_t)h->geom.sms * 64 + 4096)) return rc;
+    Trans2Params tp;
+    tp.V = V;
+    tp.out_off = g.out_off; tp.out_len = g.out_len; tp.out_nbr = g.out_nbr;
+    tp.in_off = g.in_off; tp.in_len = g.in_len; tp.in_nbr = g.in_nbr;
+    tp.kmax = d.kmax_v;
+    tp.K = K;
+    tp.Kstop = Kstop;
+    tp.sorted = sorted;
+    tp.order = s->order;
+    tp.ck = s->ck;
+    tp.cur = s->cur;
+    tp.cnt_out = s->cnt_out;
+    tp.cnt_in = s->key;
+    tp.mark = s->mark;
+    tp.stamp = s->stamp;
+    tp.logidx = s->logidx;
+    tp.log_v = s->log_v;
+    tp.log_k = s->log_k;
+    tp.log_l = s->log_l;
+    tp.log_cap = s->log_cap;
+    tp.q.slots = s->tring;
+    tp.q.mask = (unsigned)(s->tring_cap - 1);
+    tp.ctl = h->ctl;
+    uint64_t nlog = 0;
+    cudaEventRecord(h->ev[3], h->stream);
+    if (Kstop >= 1) {
+        void* args[] = {&tp};
+        EngineCtl hc;
+        if (int rc = run_persistent(h, (const void*)k_trans2, args, "transitions", &hc)) return rc;
+        nlog = hc.log_count;
+        h->stat_evals = hc.evals;
+        h->stat_drops = hc.drops;
+        h->stat_entries = hc.edges_scanned;
+    }
+    cudaEventRecord(h->ev[4], h->stream);
+    *nlog_out = nlog;
+    return DC_OK;
+}
+
 int decompose(dc_graph* h, int method, int materialize_rows) {
     DevGraph& g = h->g;
     Decomp& d = h->d;
@@ -1583,6 +1771,8 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     const int32_t K = mv[0];
     d.kmax = K;
     d.lmax = mv[1];
+    if (!d.row0 && dmalloc(&d.row0, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+    DC_CUDA(cudaMemcpyAsync(d.row0, s->row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
     if (method == 1) {
         // one fresh peel per row (the reference's schedule, main.cu:238-244),
         // two rows per launch
@@ -1633,89 +1823,8 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
         return DC_OK;
     }
     // ---- method 0: rows 1..K derived row to row
-    if (s->ck_cap < (uint32_t)K + 2) {
-        dfree(s->ck);
-        if (dmalloc(&s->ck, (uint64_t)K + 2)) return DC_ERR_NOMEM;
-        s->ck_cap = K + 2;
-    }
-    uint32_t* hist = s->cursor;
-    DC_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * ((uint64_t)K + 2), h->stream));
-    ++g_launches;
-    k_kmax_hist<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist);
-    std::vector<uint32_t> hh((size_t)K + 2), ck((size_t)K + 2), start((size_t)K + 2);
-    DC_CUDA(cudaMemcpyAsync(hh.data(), hist, sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyDeviceToHost, h->stream));
-    unsigned long long* acc = (unsigned long long*)s->tmp64;
-    DC_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), h->stream));
-    ++g_launches;
-    k_corner_bound<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, s->row0, acc);
-    unsigned long long bound = 0;
-    DC_CUDA(cudaMemcpyAsync(&bound, acc, sizeof(bound), cudaMemcpyDeviceToHost, h->stream));
-    DC_CUDA(cudaStreamSynchronize(h->stream));
-    {
-        uint64_t run = 0;
-        ck[K + 1] = 0;
-        for (int32_t k = K; k >= 0; --k) {
-            start[k] = (uint32_t)run;
-            run += hh[k];
-            ck[k] = (uint32_t)run;
-        }
-    }
-    DC_CUDA(cudaMemcpyAsync(s->ck, ck.data(), sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyHostToDevice, h->stream));
-    DC_CUDA(cudaMemcpyAsync(hist, start.data(), sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyHostToDevice, h->stream));
-    ++g_launches;
-    k_order_scatter<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist, s->order);
-    uint64_t lc = bound + 1;
-    if (s->log_cap < lc) {
-        dfree(s->log_v);
-        dfree(s->log_k);
-        dfree(s->log_l);
-        if (dmalloc(&s->log_v, lc) || dmalloc(&s->log_k, lc) || dmalloc(&s->log_l, lc)) return DC_ERR_NOMEM;
-        s->log_cap = lc;
-    }
-    // adjacency lists ordered by neighbour kmax (kept until the graph changes)
-    int sorted = 0;
-    if (int rc = sort_lists_by_kmax(h, K, &sorted)) return rc;
-    DC_CUDA(cudaMemcpyAsync(s->cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, h->stream));
-    ++g_launches;
-    k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, h->stream>>>(
-        V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, s->cur, s->cnt_out, s->key);
-    DC_CUDA(cudaMemsetAsync(s->mark, 0, sizeof(uint32_t) * V, h->stream));
-    DC_CUDA(cudaMemsetAsync(s->stamp, 0xFF, sizeof(int32_t) * V, h->stream));
-    if (int rc = ensure_tring(h, 2ull * V + (uint64_t)h->geom.sms * 64 + 4096)) return rc;
-    Trans2Params tp;
-    tp.V = V;
-    tp.out_off = g.out_off; tp.out_len = g.out_len; tp.out_nbr = g.out_nbr;
-    tp.in_off = g.in_off; tp.in_len = g.in_len; tp.in_nbr = g.in_nbr;
-    tp.kmax = d.kmax_v;
-    tp.K = K;
-    tp.sorted = sorted;
-    tp.order = s->order;
-    tp.ck = s->ck;
-    tp.cur = s->cur;
-    tp.cnt_out = s->cnt_out;
-    tp.cnt_in = s->key;
-    tp.mark = s->mark;
-    tp.stamp = s->stamp;
-    tp.logidx = s->logidx;
-    tp.log_v = s->log_v;
-    tp.log_k = s->log_k;
-    tp.log_l = s->log_l;
-    tp.log_cap = s->log_cap;
-    tp.q.slots = s->tring;
-    tp.q.mask = (unsigned)(s->tring_cap - 1);
-    tp.ctl = h->ctl;
-    cudaEventRecord(h->ev[3], h->stream);
     uint64_t nlog = 0;
-    if (K >= 1) {
-        void* args[] = {&tp};
-        EngineCtl hc;
-        if (int rc = run_persistent(h, (const void*)k_trans2, args, "transitions", &hc)) return rc;
-        nlog = hc.log_count;
-        h->stat_evals = hc.evals;
-        h->stat_drops = hc.drops;
-        h->stat_entries = hc.edges_scanned;
-    }
-    cudaEventRecord(h->ev[4], h->stream);
+    if (int rc = rows_from_row0(h, K, K, true, &nlog)) return rc;
     if (int rc = build_skyline_from_log(h, nlog)) return rc;
     cudaEventRecord(h->ev[5], h->stream);
     d.valid = true;

@@ -46,6 +46,9 @@ struct Scratch {
     uint32_t* w_out_nbr = nullptr;
     uint32_t* w_in_nbr = nullptr;
     uint64_t w_out_cap = 0, w_in_cap = 0;
+    // maintenance
+    int32_t* kmax_old = nullptr;  // [V]
+    int32_t* row0_old = nullptr;  // [V]
 };
 
 // Allocation / release (all errors reported through set_error, return DC_*).
@@ -62,8 +65,15 @@ int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_d
                         const uint32_t* in_off, const uint32_t* out_off, const uint32_t* in_nbr,
                         const uint32_t* out_nbr, uint64_t nbr_len);
 
+// Batch maintenance (dc_maint.cu).
+int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t b, int method, dc_maint_stats* st);
+// Maintenance method for a batch (rule of thumb or the learned scheduler).
+int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del);
+
 // Full decomposition; method 0 = incremental rows, 1 = per-row peel.
 int decompose(dc_graph* h, int method, int materialize_rows);
+// Rows 1..Kstop from row 0 and kmax; corners left in the scratch log.
+int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out);
 // Dense rows [k0, k0+n) into dst (device pointer, row-major, V per row).
 int expand_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* d_dst);
 
@@ -72,5 +82,15 @@ int run_peel(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* 
 
 // Cooperative launch helper.
 int coop_launch(dc_graph* h, const void* fn, void** args, int threads, const char* name);
+
+// Shared host helpers of the engine (dc_engine.cu).
+int ensure_tring(dc_graph* h, uint64_t need);
+int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out);
+int check_ctl(dc_graph* h, EngineCtl* hc, const char* what);
+int scan_tmp64(dc_graph* h, uint64_t n);
+int build_skyline_from_log(dc_graph* h, uint64_t nlog);
+// kmax (in-degree peel) and row 0 (out-degree peel) of the current graph into
+// d.kmax_v and the scratch row 0; reports the largest values.
+int peel_kmax_row0(dc_graph* h, int32_t* kmax, int32_t* lmax);
 
 }  // namespace dc

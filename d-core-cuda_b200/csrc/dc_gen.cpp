@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <unordered_map>
 #include <vector>
 #include <omp.h>
 
@@ -184,6 +185,89 @@ extern "C" int dc_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, doubl
     for (int64_t i = 0; i < int64_t(uniq); ++i) {
         src[i] = uint32_t(keys[i] >> scale);
         dst[i] = uint32_t(keys[i] & mask);
+    }
+    return DC_OK;
+}
+
+// Update stream over a graph given as a sorted, duplicate-free edge list:
+// n_ops operations, each an insertion of a uniformly random absent edge
+// (u != v) with probability insert_frac, otherwise a deletion of a uniformly
+// random present edge.  The stream is generated by applying every operation
+// to a host copy of the edge set, so it is valid in sequence.
+extern "C" int dc_gen_updates(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, uint64_t n_ops,
+                              double insert_frac, uint64_t seed, uint32_t* out_u, uint32_t* out_v, uint8_t* out_del) {
+    if (V < 2) return dc::set_error(DC_ERR_INVALID, "dc_gen_updates: need V >= 2");
+    if (n_ops && (!out_u || !out_v || !out_del)) return dc::set_error(DC_ERR_INVALID, "dc_gen_updates: null output");
+    std::vector<uint64_t> keys(E);
+    for (uint64_t e = 0; e < E; ++e) {
+        if (src[e] >= V || dst[e] >= V) return dc::set_error(DC_ERR_INVALID, "dc_gen_updates: id out of range");
+        keys[e] = ((uint64_t)src[e] << 32) | dst[e];
+        if (e && keys[e] <= keys[e - 1])
+            return dc::set_error(DC_ERR_INVALID, "dc_gen_updates: edges must be sorted by (src, dst) without duplicates");
+    }
+    std::vector<uint8_t> gone(E, 0);  // original edge deleted
+    uint64_t n_gone = 0;
+    std::vector<uint64_t> added;      // inserted edges not present originally
+    std::unordered_map<uint64_t, uint64_t> added_pos;
+    added_pos.reserve(n_ops);
+    dc::Xoshiro256ss rng(dc::derive_seed(seed, 0x555044ull));
+    const uint64_t thr = (uint64_t)(insert_frac * 18446744073709551615.0);
+    auto present = [&](uint64_t k, int64_t* orig) -> bool {
+        auto it = std::lower_bound(keys.begin(), keys.end(), k);
+        *orig = -1;
+        if (it != keys.end() && *it == k) {
+            *orig = it - keys.begin();
+            return !gone[*orig];
+        }
+        return added_pos.count(k) != 0;
+    };
+    for (uint64_t i = 0; i < n_ops; ++i) {
+        uint64_t live = E - n_gone + added.size();
+        bool ins = rng.next() <= thr || live == 0;
+        if (ins && live >= (uint64_t)V * (V - 1)) ins = false;
+        if (ins) {
+            for (;;) {
+                uint32_t u = rng.bounded(V), v = rng.bounded(V);
+                if (u == v) continue;
+                uint64_t k = ((uint64_t)u << 32) | v;
+                int64_t orig;
+                if (present(k, &orig)) continue;
+                if (orig >= 0) {
+                    gone[orig] = 0;
+                    --n_gone;
+                } else {
+                    added_pos[k] = added.size();
+                    added.push_back(k);
+                }
+                out_u[i] = u;
+                out_v[i] = v;
+                out_del[i] = 0;
+                break;
+            }
+        } else {
+            for (;;) {
+                uint64_t r = rng.bounded64(E + added.size());
+                uint64_t k;
+                if (r < E) {
+                    if (gone[r]) continue;
+                    gone[r] = 1;
+                    ++n_gone;
+                    k = keys[r];
+                } else {
+                    uint64_t j = r - E;
+                    k = added[j];
+                    uint64_t last = added.back();
+                    added[j] = last;
+                    added_pos[last] = j;
+                    added.pop_back();
+                    added_pos.erase(k);
+                }
+                out_u[i] = (uint32_t)(k >> 32);
+                out_v[i] = (uint32_t)k;
+                out_del[i] = 1;
+                break;
+            }
+        }
     }
     return DC_OK;
 }

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include "dc_device.cuh"
+#include "../../include/dcore_b200.h"
 
 namespace dc {
 
@@ -50,6 +51,7 @@ struct Decomp {
     int32_t kmax = 0;
     int32_t lmax = 0;
     int32_t* kmax_v = nullptr;  // [V]
+    int32_t* row0 = nullptr;    // [V] row 0 (out-degree core numbers)
     uint32_t* sky_off = nullptr;
     int32_t* sky_k = nullptr;
     int32_t* sky_l = nullptr;
@@ -58,6 +60,10 @@ struct Decomp {
     int32_t* rows = nullptr;  // dense rows when materialised
     uint64_t rows_cap = 0;    // elements allocated
     bool rows_valid = false;
+};
+
+struct MaintTimes {
+    float apply_ms = 0, core_ms = 0, rows_ms = 0, total_ms = 0;
 };
 
 struct PhaseTimes {
@@ -75,6 +81,7 @@ struct dc_graph {
     dc::EngineCtl* ctl = nullptr;  // device
     dc::Scratch* scratch = nullptr;
     dc::PhaseTimes times;
+    dc::MaintTimes mtimes;
     cudaEvent_t ev[8] = {};
     uint32_t gap_min = 1;      // minimum free slots per list
     uint32_t gap_div = 0;      // extra slack = len / gap_div (0 = none)

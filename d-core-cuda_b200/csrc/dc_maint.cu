@@ -1,0 +1,988 @@
+// D-core maintenance under batches of edge insertions and deletions.
+//
+// Reference path (llysdal/d-core-cuda):
+//   maintenanceFast (main.cu:1665-1751) and maintenance (main.cu:1536-1663):
+//   device-side edge insertion (graphInsertEdges, src/graph_gpu.cu:49-74),
+//   kmax maintenance by h-index refinement from +1 upper bounds
+//   (kmaxMaintenance, main.cu:668-759, over sub-batches from
+//   getKmaxEdgeBatches, main.cu:1441-1525), then a full re-peel of rows
+//   k = 0..M+1 where M = max over batch edges of min(kmax[u], kmax[v])
+//   (findMValue, main.cu:344-364; main.cu:1735-1743).  Deletion is not
+//   implemented there (graph.cpp:73-108, graph_gpu.h:18-19).
+//
+// This engine keeps the same outcome -- after every batch the result equals
+// a full decomposition of the updated graph -- and supports deletions:
+//   1. the batch is reduced to its net effect per edge (sequential
+//      semantics), deletions are validated, then applied by swap-remove;
+//      insertions go into per-list free slots (the store is rebuilt with
+//      more slack when a list is full);
+//   2. kmax and row 0 are updated either locally (h-index refinement from
+//      valid upper bounds on the region that can change) or by the fused
+//      full peel;
+//   3. rows 1..R are recomputed row to row from the new row 0, where R bounds
+//      every row an updated edge or a changed kmax can reach; rows above R
+//      keep their skyline corners.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "dc_engine.cuh"
+#include "dc_internal.h"
+
+namespace dc {
+
+extern unsigned long long g_launches;
+
+#define MT_CUDA(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t _e = (call);                                                             \
+        if (_e != cudaSuccess)                                                               \
+            return set_error(DC_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), \
+                             __FILE__, __LINE__);                                            \
+    } while (0)
+
+static constexpr int kMThreads = 256;
+static constexpr int kMWarps = kMThreads / 32;
+
+template <typename T>
+static int mt_malloc(T** p, uint64_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc((void**)p, n * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return set_error(DC_ERR_NOMEM, "device allocation of %llu bytes failed", (unsigned long long)(n * sizeof(T)));
+    }
+    return DC_OK;
+}
+template <typename T>
+static void mt_free(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+static int mgrid(dc_graph* h, uint64_t n) {
+    uint64_t b = (n + kMThreads - 1) / kMThreads;
+    uint64_t cap = (uint64_t)h->geom.sms * 16;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+// ---------------------------------------------------------------------------
+// graph updates
+// ---------------------------------------------------------------------------
+
+// Warp per distinct deleted pair: the out-list of u must hold v at least
+// `need` times.
+__global__ void k_del_validate(uint32_t n, const uint32_t* du, const uint32_t* dv, const int32_t* need,
+                               const uint32_t* out_off, const int32_t* out_len, const uint32_t* out_nbr,
+                               EngineCtl* c) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = gw; i < n; i += nw) {
+        uint32_t u = du[i], v = dv[i];
+        const uint32_t* a = out_nbr + out_off[u];
+        int len = out_len[u], cnt = 0;
+        for (int e = lane; e < len; e += 32) cnt += (a[e] == v);
+#pragma unroll
+        for (int s = 16; s; s >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, s);
+        if (lane == 0 && cnt < need[i]) set_dev_error(c, DC_DEV_ERR_NOTFOUND, 30);
+    }
+}
+
+// Warp per list: removes the listed neighbours (one occurrence each, in
+// order) by swapping with the last live entry.  All deletions of one list
+// are in one group, so no two warps touch the same list.
+__global__ void k_del_apply(uint32_t ngroups, const uint32_t* gvert, const uint32_t* goff, const uint32_t* gnbr,
+                            const uint32_t* off, int32_t* len, uint32_t* nbr, EngineCtl* c) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t g = gw; g < ngroups; g += nw) {
+        uint32_t v = gvert[g];
+        uint32_t* a = nbr + off[v];
+        int n = len[v];
+        for (uint32_t t = goff[g]; t < goff[g + 1]; ++t) {
+            uint32_t x = gnbr[t];
+            int pos = -1;
+            for (int b = 0; b < n && pos < 0; b += 32) {
+                int e = b + (int)lane;
+                unsigned m = __ballot_sync(0xFFFFFFFFu, e < n && a[e] == x);
+                if (m) pos = b + __ffs(m) - 1;
+            }
+            if (pos < 0) {
+                if (lane == 0) set_dev_error(c, DC_DEV_ERR_NOTFOUND, 31);
+                break;
+            }
+            if (lane == 0) {
+                a[pos] = a[n - 1];
+            }
+            --n;
+            __syncwarp();
+        }
+        if (lane == 0) len[v] = n;
+    }
+}
+
+__global__ void k_ins_need(uint32_t n, const uint32_t* iu, const uint32_t* iv, int32_t* need_out, int32_t* need_in) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        atomicAdd(&need_out[iu[i]], 1);
+        atomicAdd(&need_in[iv[i]], 1);
+    }
+}
+
+__global__ void k_ins_fits(uint32_t V, const uint32_t* out_off, const int32_t* out_len, const int32_t* need_out,
+                           const uint32_t* in_off, const int32_t* in_len, const int32_t* need_in, EngineCtl* c) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        if ((uint64_t)out_len[v] + need_out[v] > out_off[v + 1] - out_off[v] ||
+            (uint64_t)in_len[v] + need_in[v] > in_off[v + 1] - in_off[v])
+            set_dev_error(c, DC_DEV_ERR_CAPACITY, 32);
+    }
+}
+
+// Appends each edge to the free slots of both lists (capacity checked).
+__global__ void k_ins_apply(uint32_t n, const uint32_t* iu, const uint32_t* iv, const uint32_t* out_off,
+                            int32_t* out_len, uint32_t* out_nbr, const uint32_t* in_off, int32_t* in_len,
+                            uint32_t* in_nbr) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t u = iu[i], v = iv[i];
+        int po = atomicAdd(&out_len[u], 1);
+        out_nbr[out_off[u] + po] = v;
+        int pi = atomicAdd(&in_len[v], 1);
+        in_nbr[in_off[v] + pi] = u;
+    }
+}
+
+// Edge list of the current store (src ascending) into src/dst, using the
+// exclusive scan of out_len in eoff.
+__global__ void k_store_edges(uint32_t V, const uint32_t* off, const int32_t* len, const unsigned long long* eoff,
+                              const uint32_t* nbr, uint32_t* src, uint32_t* dst) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = gw; v < V; v += nw) {
+        uint32_t o = off[v];
+        int n = len[v];
+        uint64_t e0 = eoff[v];
+        for (int i = lane; i < n; i += 32) {
+            src[e0 + i] = (uint32_t)v;
+            dst[e0 + i] = nbr[o + i];
+        }
+    }
+}
+
+__global__ void k_len_to_u64(uint32_t V, const int32_t* len, unsigned long long* out) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+        out[v] = (unsigned long long)len[v];
+}
+
+// ---------------------------------------------------------------------------
+// local maintenance of one core (kmax: in-degree core; row 0: out-degree core)
+// ---------------------------------------------------------------------------
+// val(v) = max L such that at least L neighbours w in v's count list have
+// val(w) >= L (the h-index of the count-list values).  For kmax the count
+// list is the in-list (the in-degree core, KList over swapped lists,
+// main.cu:218-220); for row 0 it is the out-list.  A vertex's dependents are
+// the vertices whose count lists contain it.
+struct CoreParams {
+    uint32_t V;
+    const uint32_t* c_off;
+    const int32_t* c_len;
+    const uint32_t* c_nbr;
+    const uint32_t* d_off;
+    const int32_t* d_len;
+    const uint32_t* d_nbr;
+    int32_t* val;        // exact values before the update on entry, exact after on exit
+    const int32_t* old;  // copy of val at entry
+    uint32_t* mark;      // queue state per vertex (0 at entry and exit)
+    int32_t* stamp;      // region marks
+    int32_t stamp_id;
+    uint32_t* cand;      // region (insert mode)
+    unsigned cand_cap;
+    const uint32_t* seeds;
+    uint32_t n_seeds;
+    int insert_mode;
+    int32_t b;  // an insert batch raises no value by more than b
+    TicketQueue q;
+    EngineCtl* ctl;
+};
+
+__device__ __forceinline__ bool core_request(uint32_t* m, EngineCtl* c) {
+    unsigned s = ld_vol(m);
+    for (int it = 0; it < 1024; ++it) {
+        if (s == 0u) {
+            unsigned o = atomicCAS(m, 0u, 1u);
+            if (o == 0u) return true;
+            s = o;
+        } else if (s == 2u) {
+            unsigned o = atomicCAS(m, 2u, 3u);
+            if (o == 2u) return false;
+            s = o;
+        } else {
+            return false;
+        }
+    }
+    set_dev_error(c, DC_DEV_ERR_TIMEOUT, 33);
+    return false;
+}
+
+struct CoreHook {
+    unsigned nworkers;
+    __device__ void operator()(EngineCtl* c) const {
+        c->t_tail = c->t_head;
+        c->outstanding = (int)nworkers;
+        c->phase_done = 0;
+        c->step++;
+        __threadfence();
+    }
+};
+
+__device__ __forceinline__ void core_block_done(EngineCtl* c, unsigned* s_cnt) {
+    __syncwarp();
+    if ((threadIdx.x & 31u) == 0) {
+        __threadfence();
+        unsigned o = atomicAdd(s_cnt, 1u);
+        if (o == kMWarps - 1) {
+            *s_cnt = 0;
+            tq_finish(c, 1);
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kMThreads) k_core_local(CoreParams p) {
+    const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const unsigned gwarp = blockIdx.x * kMWarps + wib;
+    const unsigned nwarps = gridDim.x * kMWarps;
+    EngineCtl* c = p.ctl;
+    CoreHook hook{gridDim.x};
+    __shared__ unsigned s_prod;
+    __shared__ int s_bins[kMWarps][64];
+    int* bins = s_bins[wib];
+    if (threadIdx.x == 0) s_prod = 0;
+    if (!grid_sync_hook(c, hook)) return;
+    unsigned ticket = kNoTicket;
+    unsigned long long item;
+
+    if (p.insert_mode) {
+        // ---- phase A: region that can rise, grown from the roots along
+        // dependents whose old value is within b-1 of the current vertex, and
+        // kept only where enough count-list neighbours could end at or above
+        // the next level
+        for (uint32_t base = gwarp * 32; base < p.n_seeds; base += nwarps * 32) {
+            uint32_t i = base + lane;
+            bool push = false;
+            uint32_t r = 0;
+            if (i < p.n_seeds) {
+                r = p.seeds[i];
+                push = atomicExch(&p.stamp[r], p.stamp_id) != p.stamp_id;
+            }
+            tq_push_warp(c, p.q, push, r);
+        }
+        core_block_done(c, &s_prod);
+        while (tq_take_warp(c, p.q, &ticket, &item)) {
+            const uint32_t x = (uint32_t)item;
+            const int ox = p.old[x];
+            const uint32_t* a = p.c_nbr + p.c_off[x];
+            const int n = p.c_len[x];
+            int sup = 0;
+            for (int e = lane; e < n; e += 32) sup += (p.old[a[e]] >= ox + 1 - p.b);
+#pragma unroll
+            for (int s = 16; s; s >>= 1) sup += __shfl_xor_sync(0xFFFFFFFFu, sup, s);
+            if (sup >= ox + 1) {
+                if (lane == 0) {
+                    unsigned pos = atomicAdd(&c->log_count, 1u);
+                    if (pos < p.cand_cap) p.cand[pos] = x;
+                    else set_dev_error(c, DC_DEV_ERR_CAPACITY, 34);
+                }
+                const uint32_t* dl = p.d_nbr + p.d_off[x];
+                const int m = p.d_len[x];
+                for (int b0 = 0; b0 < m; b0 += 32) {
+                    int e = b0 + (int)lane;
+                    bool push = false;
+                    uint32_t y = 0;
+                    if (e < m) {
+                        y = dl[e];
+                        int oy = p.old[y];
+                        push = oy >= ox - (p.b - 1) && oy <= ox + (p.b - 1) &&
+                               atomicExch(&p.stamp[y], p.stamp_id) != p.stamp_id;
+                    }
+                    tq_push_warp(c, p.q, push, y);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) tq_finish(c, 1);
+        }
+        if (!grid_sync_hook(c, hook)) return;
+        // raise the region to its bound
+        const unsigned ncand = min(ld_vol(&c->log_count), p.cand_cap);
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ncand; i += gridDim.x * blockDim.x) {
+            uint32_t x = p.cand[i];
+            p.val[x] = min(p.old[x] + p.b, p.c_len[x]);
+        }
+        if (!grid_sync_hook(c, hook)) return;
+    }
+
+    // ---- phase B: h-index refinement from the upper bounds
+    {
+        const uint32_t* src = p.insert_mode ? p.cand : p.seeds;
+        const uint32_t nsrc = p.insert_mode ? min(ld_vol(&c->log_count), p.cand_cap) : p.n_seeds;
+        for (uint32_t base = gwarp * 32; base < nsrc; base += nwarps * 32) {
+            uint32_t i = base + lane;
+            bool push = false;
+            uint32_t x = 0;
+            if (i < nsrc) {
+                x = src[i];
+                push = core_request(&p.mark[x], c);
+            }
+            tq_push_warp(c, p.q, push, x);
+        }
+    }
+    core_block_done(c, &s_prod);
+    unsigned long long drops = 0;
+    while (tq_take_warp(c, p.q, &ticket, &item)) {
+        const uint32_t x = (uint32_t)item;
+        if (lane == 0) {
+            atomicExch(&p.mark[x], 2u);
+            __threadfence();
+        }
+        __syncwarp();
+        const int cap = ld_vol(&p.val[x]);
+        const uint32_t* a = p.c_nbr + p.c_off[x];
+        const int n = p.c_len[x];
+        int nv = 0;
+        if (cap > 0) {
+            int carry = 0, hi = cap;
+            bool first = true;
+            for (;;) {
+                int lo = max(0, hi - 63);
+                bins[lane] = 0;
+                bins[lane + 32] = 0;
+                __syncwarp();
+                for (int e = lane; e < n; e += 32) {
+                    int cw = ld_vol(&p.val[a[e]]);
+                    if (cw >= lo) {
+                        if (cw >= hi) {
+                            if (first || cw == hi) atomicAdd(&bins[hi - lo], 1);
+                        } else {
+                            atomicAdd(&bins[cw - lo], 1);
+                        }
+                    }
+                }
+                __syncwarp();
+                int b0 = 2 * lane, b1 = 2 * lane + 1;
+                int h0 = bins[b0], h1 = bins[b1];
+                int pp = h0 + h1, sc = pp;
+#pragma unroll
+                for (int s = 1; s < 32; s <<= 1) {
+                    int y = __shfl_down_sync(0xFFFFFFFFu, sc, s);
+                    if (lane + s < 32) sc += y;
+                }
+                int cum1 = carry + (sc - pp) + h1, cum0 = cum1 + h0;
+                bool ok1 = lo + b1 <= hi && cum1 >= lo + b1;
+                bool ok0 = lo + b0 <= hi && cum0 >= lo + b0;
+                unsigned m1 = __ballot_sync(0xFFFFFFFFu, ok1), m0 = __ballot_sync(0xFFFFFFFFu, ok0);
+                int best = -1;
+                if (m1) best = lo + 2 * (31 - __clz(m1)) + 1;
+                if (m0) best = max(best, lo + 2 * (31 - __clz(m0)));
+                if (best >= 0) {
+                    nv = best;
+                    break;
+                }
+                carry += __shfl_sync(0xFFFFFFFFu, sc, 0);
+                first = false;
+                if (lo == 0) {
+                    nv = 0;
+                    break;
+                }
+                hi = lo - 1;
+                __syncwarp();
+            }
+        }
+        bool requeue = false;
+        if (nv < cap) {
+            ++drops;
+            if (lane == 0) {
+                atomicExch(&p.val[x], nv);
+                __threadfence();
+            }
+            __syncwarp();
+            __threadfence();
+            const uint32_t* dl = p.d_nbr + p.d_off[x];
+            const int m = p.d_len[x];
+            for (int b0 = 0; b0 < m; b0 += 32) {
+                int e = b0 + (int)lane;
+                bool push = false;
+                uint32_t y = 0;
+                if (e < m) {
+                    y = dl[e];
+                    int cy = ld_vol(&p.val[y]);
+                    push = cy > nv && cy <= cap && core_request(&p.mark[y], c);
+                }
+                tq_push_warp(c, p.q, push, y);
+            }
+        }
+        if (lane == 0) {
+            if (nv < cap && nv > 0) {
+                atomicExch(&p.mark[x], 1u);
+                requeue = true;
+            } else {
+                unsigned o = atomicCAS(&p.mark[x], 2u, 0u);
+                if (o == 3u) {
+                    if (nv > 0) {
+                        atomicExch(&p.mark[x], 1u);
+                        requeue = true;
+                    } else {
+                        atomicExch(&p.mark[x], 0u);
+                    }
+                }
+            }
+        }
+        tq_push_warp(c, p.q, requeue, x);
+        if (lane == 0) tq_finish(c, 1);
+    }
+    if (lane == 0) atomicAdd(&c->drops, drops);
+}
+
+// ---------------------------------------------------------------------------
+// bound on the rows a batch can change
+// ---------------------------------------------------------------------------
+__global__ void k_rows_bound_edges(uint32_t n, const uint32_t* u, const uint32_t* v, const int32_t* kold,
+                                   const int32_t* knew, int* out) {
+    int m = -1;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        m = max(m, min(kold[u[i]], kold[v[i]]));
+        m = max(m, min(knew[u[i]], knew[v[i]]));
+    }
+#pragma unroll
+    for (int s = 16; s; s >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, s));
+    if ((threadIdx.x & 31u) == 0) atomicMax(out, m);
+}
+__global__ void k_rows_bound_changed(uint32_t V, const int32_t* kold, const int32_t* knew, int* out, int* kmax_new) {
+    int m = -1, km = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (kold[i] != knew[i]) m = max(m, max(kold[i], knew[i]));
+        km = max(km, knew[i]);
+    }
+#pragma unroll
+    for (int s = 16; s; s >>= 1) {
+        m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, s));
+        km = max(km, __shfl_xor_sync(0xFFFFFFFFu, km, s));
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        atomicMax(out, m);
+        atomicMax(kmax_new, km);
+    }
+}
+__global__ void k_vmax(uint32_t V, const int32_t* a, int* out) {
+    int m = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V; i += (uint64_t)gridDim.x * blockDim.x)
+        m = max(m, a[i]);
+#pragma unroll
+    for (int s = 16; s; s >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, s));
+    if ((threadIdx.x & 31u) == 0) atomicMax(out, m);
+}
+
+// ---------------------------------------------------------------------------
+// skyline merge: rows <= R from the fresh partial skyline, rows > R from the
+// previous one
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int sky_value_at(const uint32_t* off, const int32_t* ks, const int32_t* ls, uint32_t v,
+                                            int k) {
+    uint32_t a = off[v], b = off[v + 1];
+    int val = 0;
+    for (uint32_t i = a; i < b && ks[i] <= k; ++i) val = ls[i];
+    return val;
+}
+
+__global__ void k_merge_count(uint32_t V, int R, const int32_t* kmax, const uint32_t* noff, const int32_t* nk,
+                              const int32_t* nl, const uint32_t* ooff, const int32_t* ok, const int32_t* ol,
+                              unsigned long long* cnt) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        unsigned long long c = 0;
+        for (uint32_t i = noff[v]; i < noff[v + 1]; ++i) c += nk[i] <= R;
+        if (R + 1 <= kmax[v]) {
+            int last = sky_value_at(noff, nk, nl, (uint32_t)v, R);
+            int at = sky_value_at(ooff, ok, ol, (uint32_t)v, R + 1);
+            c += at != last;
+            for (uint32_t i = ooff[v]; i < ooff[v + 1]; ++i) c += ok[i] > R + 1;
+        }
+        cnt[v] = c;
+    }
+}
+
+__global__ void k_merge_fill(uint32_t V, int R, const int32_t* kmax, const uint32_t* noff, const int32_t* nk,
+                             const int32_t* nl, const uint32_t* ooff, const int32_t* ok, const int32_t* ol,
+                             const unsigned long long* moff, int32_t* mk, int32_t* ml, uint32_t* moff32) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t o = moff[v];
+        for (uint32_t i = noff[v]; i < noff[v + 1]; ++i)
+            if (nk[i] <= R) {
+                mk[o] = nk[i];
+                ml[o] = nl[i];
+                ++o;
+            }
+        if (R + 1 <= kmax[v]) {
+            int last = sky_value_at(noff, nk, nl, (uint32_t)v, R);
+            int at = sky_value_at(ooff, ok, ol, (uint32_t)v, R + 1);
+            if (at != last) {
+                mk[o] = R + 1;
+                ml[o] = at;
+                ++o;
+            }
+            for (uint32_t i = ooff[v]; i < ooff[v + 1]; ++i)
+                if (ok[i] > R + 1) {
+                    mk[o] = ok[i];
+                    ml[o] = ol[i];
+                    ++o;
+                }
+        }
+        moff32[v] = (uint32_t)moff[v];
+        if (v == V - 1) moff32[V] = (uint32_t)moff[V];
+    }
+}
+
+}  // namespace dc
+
+// ---------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------
+namespace dc {
+
+// Rule of thumb: the local update of kmax and row 0 costs about its region
+// per inserted edge, the fused peel a fixed pass over the whole graph.
+int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del) {
+    (void)h;
+    return (n_ins + n_del <= 4096) ? DC_MAINT_LOCAL : DC_MAINT_REPEEL;
+}
+
+struct NetBatch {
+    std::vector<uint32_t> del_u, del_v;  // distinct pairs with a net deletion
+    std::vector<int32_t> del_n;          // occurrences to delete
+    std::vector<uint32_t> ins_u, ins_v;  // net insertions, one entry per occurrence
+    uint64_t n_del = 0, n_ins = 0;
+};
+
+// Net effect of a batch under sequential semantics: per distinct (u, v),
+// occurrences inserted minus occurrences deleted.
+static int net_batch(uint32_t V, const uint32_t* pairs, const uint8_t* is_del, uint64_t b, NetBatch& nb) {
+    std::vector<uint64_t> key(b);
+    for (uint64_t i = 0; i < b; ++i) {
+        uint32_t u = pairs[2 * i], v = pairs[2 * i + 1];
+        if (u >= V || v >= V)
+            return set_error(DC_ERR_INVALID, "dc_maintain: edge %llu (%u, %u) has a vertex id >= V=%u",
+                             (unsigned long long)i, u, v, V);
+        key[i] = ((uint64_t)u << 32) | v;
+    }
+    std::vector<uint64_t> idx(b);
+    for (uint64_t i = 0; i < b; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](uint64_t x, uint64_t y) { return key[x] < key[y] || (key[x] == key[y] && x < y); });
+    for (uint64_t i = 0; i < b;) {
+        uint64_t j = i;
+        int64_t net = 0;
+        while (j < b && key[idx[j]] == key[idx[i]]) {
+            net += (is_del && is_del[idx[j]]) ? -1 : 1;
+            ++j;
+        }
+        uint32_t u = (uint32_t)(key[idx[i]] >> 32), v = (uint32_t)key[idx[i]];
+        if (net < 0) {
+            nb.del_u.push_back(u);
+            nb.del_v.push_back(v);
+            nb.del_n.push_back((int32_t)-net);
+            nb.n_del += (uint64_t)-net;
+        } else {
+            for (int64_t r = 0; r < net; ++r) {
+                nb.ins_u.push_back(u);
+                nb.ins_v.push_back(v);
+            }
+            nb.n_ins += (uint64_t)net;
+        }
+        i = j;
+    }
+    return DC_OK;
+}
+
+template <typename T>
+static int upload(dc_graph* h, T** d, const std::vector<T>& hv) {
+    if (mt_malloc(d, hv.size())) return DC_ERR_NOMEM;
+    if (!hv.empty()) MT_CUDA(cudaMemcpyAsync(*d, hv.data(), sizeof(T) * hv.size(), cudaMemcpyHostToDevice, h->stream));
+    return DC_OK;
+}
+
+// Groups (vertex, neighbour) deletions by vertex: one group per list.
+static void group_by(const std::vector<uint32_t>& key, const std::vector<uint32_t>& other,
+                     const std::vector<int32_t>& count, std::vector<uint32_t>& gvert, std::vector<uint32_t>& goff,
+                     std::vector<uint32_t>& gnbr) {
+    std::vector<uint64_t> idx(key.size());
+    for (uint64_t i = 0; i < idx.size(); ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) { return key[a] < key[b]; });
+    gvert.clear();
+    goff.clear();
+    gnbr.clear();
+    for (uint64_t i = 0; i < idx.size(); ++i) {
+        if (i == 0 || key[idx[i]] != key[idx[i - 1]]) {
+            gvert.push_back(key[idx[i]]);
+            goff.push_back((uint32_t)gnbr.size());
+        }
+        for (int32_t r = 0; r < count[idx[i]]; ++r) gnbr.push_back(other[idx[i]]);
+    }
+    goff.push_back((uint32_t)gnbr.size());
+}
+
+// Applies the validated deletions to both adjacency sides.
+static int apply_deletions(dc_graph* h, const NetBatch& nb) {
+    DevGraph& g = h->g;
+    if (nb.del_u.empty()) return DC_OK;
+    int rc = DC_OK;
+    uint32_t *du = nullptr, *dv = nullptr;
+    int32_t* dn = nullptr;
+    if ((rc = upload(h, &du, nb.del_u)) || (rc = upload(h, &dv, nb.del_v)) || (rc = upload(h, &dn, nb.del_n))) {
+        mt_free(du); mt_free(dv); mt_free(dn);
+        return rc;
+    }
+    MT_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
+    ++g_launches;
+    k_del_validate<<<mgrid(h, nb.del_u.size() * 32), kMThreads, 0, h->stream>>>(
+        (uint32_t)nb.del_u.size(), du, dv, dn, g.out_off, g.out_len, g.out_nbr, h->ctl);
+    EngineCtl hc;
+    rc = check_ctl(h, &hc, "dc_maintain: deletion check");
+    mt_free(du);
+    mt_free(dv);
+    mt_free(dn);
+    if (rc != DC_OK) {
+        if (hc.error & DC_DEV_ERR_NOTFOUND)
+            return set_error(DC_ERR_NOT_FOUND, "dc_maintain: a deleted edge is not in the graph (batch not applied)");
+        return rc;
+    }
+    for (int side = 0; side < 2; ++side) {
+        std::vector<uint32_t> gvert, goff, gnbr;
+        if (side == 0) group_by(nb.del_u, nb.del_v, nb.del_n, gvert, goff, gnbr);
+        else group_by(nb.del_v, nb.del_u, nb.del_n, gvert, goff, gnbr);
+        uint32_t *d_gv = nullptr, *d_go = nullptr, *d_gn = nullptr;
+        if ((rc = upload(h, &d_gv, gvert)) || (rc = upload(h, &d_go, goff)) || (rc = upload(h, &d_gn, gnbr))) {
+            mt_free(d_gv); mt_free(d_go); mt_free(d_gn);
+            return rc;
+        }
+        ++g_launches;
+        k_del_apply<<<mgrid(h, gvert.size() * 32), kMThreads, 0, h->stream>>>(
+            (uint32_t)gvert.size(), d_gv, d_go, d_gn, side == 0 ? g.out_off : g.in_off,
+            side == 0 ? g.out_len : g.in_len, side == 0 ? g.out_nbr : g.in_nbr, h->ctl);
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        mt_free(d_gv);
+        mt_free(d_go);
+        mt_free(d_gn);
+        if (e != cudaSuccess) return set_error(DC_ERR_CUDA, "deletion apply: %s", cudaGetErrorString(e));
+    }
+    rc = check_ctl(h, &hc, "dc_maintain: deletion apply");
+    if (rc != DC_OK) return rc;
+    g.E -= nb.n_del;
+    g.sorted_kmax = false;
+    return DC_OK;
+}
+
+// Rebuilds the adjacency store with more free slots (keeps the decomposition).
+static int rebuild_store(dc_graph* h, const uint32_t* d_iu, const uint32_t* d_iv, uint64_t n_ins) {
+    DevGraph& g = h->g;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    uint64_t E = g.E + n_ins;
+    uint32_t *src = nullptr, *dst = nullptr;
+    if (mt_malloc(&src, E) || mt_malloc(&dst, E)) {
+        mt_free(src);
+        return DC_ERR_NOMEM;
+    }
+    ++g_launches;
+    k_len_to_u64<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, g.out_len, (unsigned long long*)s->tmp64);
+    if (int rc = scan_tmp64(h, V)) {
+        mt_free(src); mt_free(dst);
+        return rc;
+    }
+    ++g_launches;
+    k_store_edges<<<mgrid(h, (uint64_t)V * 32), kMThreads, 0, h->stream>>>(
+        V, g.out_off, g.out_len, (const unsigned long long*)s->tmp64, g.out_nbr, src, dst);
+    MT_CUDA(cudaMemcpyAsync(src + g.E, d_iu, 4 * n_ins, cudaMemcpyDeviceToDevice, h->stream));
+    MT_CUDA(cudaMemcpyAsync(dst + g.E, d_iv, 4 * n_ins, cudaMemcpyDeviceToDevice, h->stream));
+    MT_CUDA(cudaStreamSynchronize(h->stream));
+    Decomp keep = h->d;
+    h->d = Decomp();
+    uint32_t gm = h->gap_min, gd = h->gap_div;
+    h->gap_min = std::max<uint32_t>(gm, 2);
+    h->gap_div = gd ? std::min<uint32_t>(gd, 8) : 8;
+    int rc = build_from_device_edges(h, V, E, src, dst);
+    cudaStreamSynchronize(h->stream);
+    free_decomp(h->d);
+    h->d = keep;
+    mt_free(src);
+    mt_free(dst);
+    return rc;
+}
+
+// Inserts the net insertions; returns 1 in *rebuilt when the store grew.
+static int apply_insertions(dc_graph* h, const NetBatch& nb, uint32_t** d_iu_out, uint32_t** d_iv_out, int* rebuilt) {
+    DevGraph& g = h->g;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    *rebuilt = 0;
+    *d_iu_out = *d_iv_out = nullptr;
+    if (nb.ins_u.empty()) return DC_OK;
+    uint32_t *iu = nullptr, *iv = nullptr;
+    int rc = DC_OK;
+    if ((rc = upload(h, &iu, nb.ins_u)) || (rc = upload(h, &iv, nb.ins_v))) {
+        mt_free(iu); mt_free(iv);
+        return rc;
+    }
+    const uint32_t n = (uint32_t)nb.ins_u.size();
+    MT_CUDA(cudaMemsetAsync(s->key2, 0, 4ull * V, h->stream));
+    MT_CUDA(cudaMemsetAsync(s->cdeg2, 0, 4ull * V, h->stream));
+    MT_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
+    ++g_launches;
+    k_ins_need<<<mgrid(h, n), kMThreads, 0, h->stream>>>(n, iu, iv, s->key2, s->cdeg2);
+    ++g_launches;
+    k_ins_fits<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, g.out_off, g.out_len, s->key2, g.in_off, g.in_len,
+                                                         s->cdeg2, h->ctl);
+    EngineCtl hc;
+    rc = check_ctl(h, &hc, "dc_maintain: capacity check");
+    if (rc != DC_OK && (hc.error & DC_DEV_ERR_CAPACITY)) {
+        set_error(DC_OK, "%s", "");
+        rc = rebuild_store(h, iu, iv, n);
+        *rebuilt = 1;
+    } else if (rc == DC_OK) {
+        ++g_launches;
+        k_ins_apply<<<mgrid(h, n), kMThreads, 0, h->stream>>>(n, iu, iv, g.out_off, g.out_len, g.out_nbr, g.in_off,
+                                                              g.in_len, g.in_nbr);
+        g.E += n;
+    }
+    if (rc != DC_OK) {
+        mt_free(iu); mt_free(iv);
+        return rc;
+    }
+    g.sorted_kmax = false;
+    *d_iu_out = iu;
+    *d_iv_out = iv;
+    return DC_OK;
+}
+
+// One local core update.  which: 0 = kmax (count list = in-list),
+// 1 = row 0 (count list = out-list).  insert_mode: roots + bound b.
+static int core_local(dc_graph* h, int which, int32_t* val, const int32_t* old, const uint32_t* d_seeds,
+                      uint32_t n_seeds, int insert_mode, int32_t b, uint64_t* region) {
+    DevGraph& g = h->g;
+    Scratch* s = h->scratch;
+    if (n_seeds == 0) return DC_OK;
+    CoreParams p;
+    p.V = g.V;
+    if (which == 0) {
+        p.c_off = g.in_off; p.c_len = g.in_len; p.c_nbr = g.in_nbr;
+        p.d_off = g.out_off; p.d_len = g.out_len; p.d_nbr = g.out_nbr;
+    } else {
+        p.c_off = g.out_off; p.c_len = g.out_len; p.c_nbr = g.out_nbr;
+        p.d_off = g.in_off; p.d_len = g.in_len; p.d_nbr = g.in_nbr;
+    }
+    p.val = val;
+    p.old = old;
+    p.mark = s->mark;
+    p.stamp = s->stamp;
+    p.stamp_id = 1;
+    p.cand = s->rem0;
+    p.cand_cap = g.V + 1;
+    p.seeds = d_seeds;
+    p.n_seeds = n_seeds;
+    p.insert_mode = insert_mode;
+    p.b = b;
+    if (int rc = ensure_tring(h, 2ull * g.V + (uint64_t)h->geom.sms * 64 + 4096)) return rc;
+    p.q.slots = s->tring;
+    p.q.mask = (unsigned)(s->tring_cap - 1);
+    p.ctl = h->ctl;
+    if (insert_mode) MT_CUDA(cudaMemsetAsync(s->stamp, 0xFF, 4ull * g.V, h->stream));
+    void* args[] = {&p};
+    EngineCtl hc;
+    if (int rc = run_persistent(h, (const void*)k_core_local, args, "core update", &hc)) return rc;
+    if (region) *region += insert_mode ? hc.log_count : n_seeds;
+    return DC_OK;
+}
+
+int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t b, int method, dc_maint_stats* st) {
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    const uint32_t V = g.V;
+    dc_maint_stats local_st;
+    if (!st) st = &local_st;
+    memset(st, 0, sizeof(*st));
+    if (b && !pairs) return set_error(DC_ERR_INVALID, "dc_maintain: null edge array");
+    if (method < DC_MAINT_AUTO || method > DC_MAINT_REPEEL) return set_error(DC_ERR_INVALID, "dc_maintain: bad method %d", method);
+    if (int rc = ensure_scratch(h, V)) return rc;
+    Scratch* s = h->scratch;
+    if (!d.valid)
+        if (int rc = decompose(h, 0, 0)) return rc;
+    NetBatch nb;
+    if (int rc = net_batch(V, pairs, is_del, b, nb)) return rc;
+    st->deleted = nb.n_del;
+    st->inserted = nb.n_ins;
+    if (method == DC_MAINT_AUTO) method = choose_method(h, nb.n_ins, nb.n_del);
+    st->method = method;
+    cudaEvent_t* ev = h->ev;
+    cudaEventRecord(ev[0], h->stream);
+    if (!s->kmax_old && (mt_malloc(&s->kmax_old, (uint64_t)V + 1) || mt_malloc(&s->row0_old, (uint64_t)V + 1)))
+        return DC_ERR_NOMEM;
+    // values before the batch (for the row bound) and row 0 in scratch
+    MT_CUDA(cudaMemcpyAsync(s->kmax_old, d.kmax_v, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+    uint32_t *d_du = nullptr, *d_dv = nullptr, *d_iu = nullptr, *d_iv = nullptr;
+    int rc = DC_OK;
+    int rebuilt = 0;
+    uint64_t region = 0;
+    // ---- deletions
+    if (!nb.del_u.empty()) {
+        if ((rc = apply_deletions(h, nb))) return rc;
+        std::vector<uint32_t> heads(nb.del_v), tails(nb.del_u);
+        if ((rc = upload(h, &d_dv, heads)) || (rc = upload(h, &d_du, tails))) goto out;
+        if (method == DC_MAINT_LOCAL) {
+            MT_CUDA(cudaMemcpyAsync(s->row0_old, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+            if ((rc = core_local(h, 0, d.kmax_v, s->kmax_old, d_dv, (uint32_t)heads.size(), 0, 0, &region))) goto out;
+            if ((rc = core_local(h, 1, d.row0, s->row0_old, d_du, (uint32_t)tails.size(), 0, 0, &region))) goto out;
+        }
+    }
+    // ---- insertions
+    if (!nb.ins_u.empty()) {
+        if ((rc = apply_insertions(h, nb, &d_iu, &d_iv, &rebuilt))) goto out;
+        if (method == DC_MAINT_LOCAL) {
+            int32_t bb = (int32_t)std::min<uint64_t>(nb.n_ins, 0x3FFFFFFF);
+            int32_t* old_k = s->cdeg2;  // values before the insertions
+            int32_t* old_r = s->key2;
+            MT_CUDA(cudaMemcpyAsync(old_k, d.kmax_v, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+            MT_CUDA(cudaMemcpyAsync(old_r, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+            if ((rc = core_local(h, 0, d.kmax_v, old_k, d_iv, (uint32_t)nb.ins_u.size(), 1, bb, &region))) goto out;
+            if ((rc = core_local(h, 1, d.row0, old_r, d_iu, (uint32_t)nb.ins_u.size(), 1, bb, &region))) goto out;
+        }
+    }
+    cudaEventRecord(ev[1], h->stream);
+    if (method == DC_MAINT_REPEEL) {
+        int32_t km = 0, lm = 0;
+        if ((rc = peel_kmax_row0(h, &km, &lm))) goto out;
+        MT_CUDA(cudaMemcpyAsync(d.row0, s->row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    cudaEventRecord(ev[2], h->stream);
+    st->region = region;
+    st->rebuilt = (uint32_t)rebuilt;
+    {
+        // ---- rows that can change: rows up to R
+        int* dbuf = (int*)s->cursor;  // [0] = R, [1] = new kmax, [2] = new lmax
+        int init[3] = {-1, 0, 0};
+        MT_CUDA(cudaMemcpyAsync(dbuf, init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
+        if (!nb.del_u.empty()) {
+            ++g_launches;
+            k_rows_bound_edges<<<mgrid(h, nb.del_u.size()), kMThreads, 0, h->stream>>>(
+                (uint32_t)nb.del_u.size(), d_du, d_dv, s->kmax_old, d.kmax_v, dbuf);
+        }
+        if (!nb.ins_u.empty()) {
+            ++g_launches;
+            k_rows_bound_edges<<<mgrid(h, nb.ins_u.size()), kMThreads, 0, h->stream>>>(
+                (uint32_t)nb.ins_u.size(), d_iu, d_iv, s->kmax_old, d.kmax_v, dbuf);
+        }
+        ++g_launches;
+        k_rows_bound_changed<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, s->kmax_old, d.kmax_v, dbuf, dbuf + 1);
+        ++g_launches;
+        k_vmax<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, d.row0, dbuf + 2);
+        int res[3];
+        MT_CUDA(cudaMemcpyAsync(res, dbuf, sizeof(res), cudaMemcpyDeviceToHost, h->stream));
+        MT_CUDA(cudaStreamSynchronize(h->stream));
+        const int32_t Knew = res[1];
+        const int32_t R = std::min(res[0], Knew);
+        st->rows_recomputed = R + 1;
+        if (R < 0) {
+            // nothing changed
+            d.kmax = Knew;
+            d.lmax = res[2];
+            d.rows_valid = false;
+            st->kmax = d.kmax;
+            st->lmax = d.lmax;
+            goto timing;
+        }
+        // ---- rows 0..R from the new row 0, rows above R from the old skyline
+        MT_CUDA(cudaMemcpyAsync(s->row0, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+        uint64_t nlog = 0;
+        if ((rc = rows_from_row0(h, Knew, R, R > 48, &nlog))) goto out;
+        uint32_t* o_off = d.sky_off;
+        int32_t* o_k = d.sky_k;
+        int32_t* o_l = d.sky_l;
+        d.sky_off = nullptr;
+        d.sky_k = nullptr;
+        d.sky_l = nullptr;
+        d.corner_cap = 0;
+        rc = build_skyline_from_log(h, nlog);
+        if (rc == DC_OK) {
+            unsigned long long* cnt = (unsigned long long*)s->tmp64;
+            ++g_launches;
+            k_merge_count<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, R, d.kmax_v, d.sky_off, d.sky_k, d.sky_l, o_off,
+                                                                    o_k, o_l, cnt);
+            rc = scan_tmp64(h, V);
+            unsigned long long total = 0;
+            if (rc == DC_OK) {
+                cudaMemcpyAsync(&total, s->tmp64 + V, sizeof(total), cudaMemcpyDeviceToHost, h->stream);
+                cudaStreamSynchronize(h->stream);
+            }
+            uint32_t* m_off = nullptr;
+            int32_t *m_k = nullptr, *m_l = nullptr;
+            if (rc == DC_OK && (mt_malloc(&m_off, (uint64_t)V + 1) || mt_malloc(&m_k, total) || mt_malloc(&m_l, total))) {
+                rc = DC_ERR_NOMEM;
+            }
+            if (rc == DC_OK) {
+                ++g_launches;
+                k_merge_fill<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, R, d.kmax_v, d.sky_off, d.sky_k, d.sky_l,
+                                                                       o_off, o_k, o_l, cnt, m_k, m_l, m_off);
+                cudaStreamSynchronize(h->stream);
+                mt_free(d.sky_off);
+                mt_free(d.sky_k);
+                mt_free(d.sky_l);
+                d.sky_off = m_off;
+                d.sky_k = m_k;
+                d.sky_l = m_l;
+                d.corner_cap = total;
+                d.n_corners = total;
+            } else {
+                mt_free(m_off); mt_free(m_k); mt_free(m_l);
+            }
+        }
+        mt_free(o_off);
+        mt_free(o_k);
+        mt_free(o_l);
+        if (rc != DC_OK) {
+            d.valid = false;
+            goto out;
+        }
+        d.kmax = Knew;
+        d.lmax = res[2];
+        d.rows_valid = false;
+        d.valid = true;
+        st->kmax = d.kmax;
+        st->lmax = d.lmax;
+    }
+timing:
+    cudaEventRecord(ev[3], h->stream);
+    MT_CUDA(cudaStreamSynchronize(h->stream));
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        st->apply_ms = ms;
+        cudaEventElapsedTime(&ms, ev[1], ev[2]);
+        st->core_ms = ms;
+        cudaEventElapsedTime(&ms, ev[2], ev[3]);
+        st->rows_ms = ms;
+        cudaEventElapsedTime(&ms, ev[0], ev[3]);
+        st->total_ms = ms;
+        h->mtimes.total_ms = ms;
+    }
+    st->kmax = d.kmax;
+    st->lmax = d.lmax;
+out:
+    mt_free(d_du);
+    mt_free(d_dv);
+    mt_free(d_iu);
+    mt_free(d_iv);
+    if (rc != DC_OK) d.valid = false;
+    return rc;
+}
+
+}  // namespace dc

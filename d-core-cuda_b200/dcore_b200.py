@@ -51,11 +51,23 @@ class DecompInfo(ctypes.Structure):
                 ("evals", ctypes.c_uint64), ("drops", ctypes.c_uint64), ("entries", ctypes.c_uint64)]
 
 
+class MaintStats(ctypes.Structure):
+    _fields_ = [("inserted", ctypes.c_uint64), ("deleted", ctypes.c_uint64), ("kmax", ctypes.c_int32),
+                ("lmax", ctypes.c_int32), ("rows_recomputed", ctypes.c_int32), ("method", ctypes.c_int32),
+                ("rebuilt", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("region", ctypes.c_uint64),
+                ("apply_ms", ctypes.c_float), ("core_ms", ctypes.c_float), ("rows_ms", ctypes.c_float),
+                ("total_ms", ctypes.c_float)]
+
+
+MAINT_AUTO, MAINT_LOCAL, MAINT_REPEEL = 0, 1, 2
+
 # name -> argtypes; every function returns int status unless listed in _VOID / _STR
 SIGNATURES = {
     "dc_gen_er": [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p, u32p],
     "dc_gen_rmat": [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                     ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, u32p, u32p, u64p],
+    "dc_gen_updates": [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_uint64, ctypes.c_double,
+                       ctypes.c_uint64, u32p, u32p, u8p],
     "dc_text_read_edges": [ctypes.c_char_p, ctypes.c_int, u32p, u64p, u32p, u32p, ctypes.c_uint64],
     "dc_binary_read_edges": [ctypes.c_char_p, u32p, u64p, u32p, u32p, ctypes.c_uint64],
     "dc_binary_write_edges": [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_uint32],
@@ -74,6 +86,7 @@ SIGNATURES = {
     "dc_graph_get_edges": [vp, u32p, u32p, ctypes.c_uint64, u64p],
     "dc_graph_write_binary": [vp, ctypes.c_char_p, ctypes.c_uint32],
     "dc_decompose": [vp, ctypes.c_int, i32p, i32p],
+    "dc_maintain": [vp, u32p, u8p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(MaintStats)],
     "dc_decomp_info_get": [vp, ctypes.POINTER(DecompInfo)],
     "dc_get_kmaxes": [vp, i32p],
     "dc_get_lmax_rows": [vp, ctypes.c_uint32, ctypes.c_uint32, i32p],
@@ -182,6 +195,18 @@ def gen_rmat(scale, edge_factor, seed, a=0.57, b=0.19, c=0.19, permute=True):
     _check(lib().dc_gen_rmat(scale, edge_factor, a, b, c, seed, int(permute), cap, _p(src, u32p), _p(dst, u32p),
                              ctypes.byref(n)))
     return 1 << scale, src[:n.value], dst[:n.value]
+
+
+def gen_updates(V, src, dst, n_ops, insert_frac, seed):
+    """Seeded valid-in-sequence update stream: (u, v, is_delete) arrays."""
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    u = np.empty(max(n_ops, 1), np.uint32)
+    v = np.empty(max(n_ops, 1), np.uint32)
+    dl = np.empty(max(n_ops, 1), np.uint8)
+    _check(lib().dc_gen_updates(V, len(src), _p(src, u32p), _p(dst, u32p), n_ops, insert_frac, seed, _p(u, u32p),
+                                _p(v, u32p), _p(dl, u8p)))
+    return u[:n_ops], v[:n_ops], dl[:n_ops]
 
 
 # ---------------------------------------------------------------- file formats
@@ -328,6 +353,21 @@ class Graph:
         lm = ctypes.c_int32(0)
         _check(lib().dc_decompose(self._h, method, ctypes.byref(km), ctypes.byref(lm)))
         return km.value, lm.value
+
+    def maintain(self, src, dst, is_delete=None, method=MAINT_AUTO):
+        """maintenanceFast: applies the update batch; returns the stats dict."""
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        pairs = np.empty(2 * len(src), np.uint32)
+        pairs[0::2] = src
+        pairs[1::2] = dst
+        dl = None
+        if is_delete is not None:
+            dl = np.ascontiguousarray(is_delete, np.uint8)
+        st = MaintStats()
+        _check(lib().dc_maintain(self._h, _p(pairs, u32p), None if dl is None else _p(dl, u8p), len(src), method,
+                                 ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in MaintStats._fields_ if f != "pad"}
 
     def decomp_info(self):
         info = DecompInfo()

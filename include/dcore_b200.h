@@ -62,6 +62,15 @@ int dc_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double
                 uint32_t* src, uint32_t* dst, uint64_t* n_edges);
 
 
+/* Update stream over a sorted, duplicate-free edge list: n_ops operations,
+ * each an insertion of a uniformly random absent edge (u != v) with
+ * probability insert_frac, else a deletion of a uniformly random present
+ * edge; generated by applying each operation to a host copy of the edge set,
+ * so the stream is valid in sequence.  out_del[i] = 1 marks a deletion.
+ * Replaces getRandomInsertEdge / getRandomDeleteEdge (src/graph.cpp:327-380). */
+int dc_gen_updates(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, uint64_t n_ops,
+                   double insert_frac, uint64_t seed, uint32_t* out_u, uint32_t* out_v, uint8_t* out_del);
+
 /* ---- file formats (host only, no GPU needed) ---------------------------- */
 
 /* Text graph: "# V" header, then "s t" lines.  Self-loops dropped, duplicate
@@ -166,6 +175,35 @@ int dc_get_skyline(dc_graph* g, uint32_t* off, int32_t* ks, int32_t* ls, uint64_
 /* writeDecompFile / writeDecompFileCPU of the current decomposition. */
 int dc_write_decomp(dc_graph* g, const char* path);
 int dc_write_decomp_cpu(dc_graph* g, const char* path);
+
+/* ---- maintenance ------------------------------------------------------- */
+
+#define DC_MAINT_AUTO 0   /* the engine's scheduler picks per batch            */
+#define DC_MAINT_LOCAL 1  /* kmax and row 0 updated locally (h-index refine)   */
+#define DC_MAINT_REPEEL 2 /* kmax and row 0 recomputed by the fused full peel  */
+
+typedef struct dc_maint_stats {
+    uint64_t inserted, deleted; /* net edge insertions / deletions applied            */
+    int32_t kmax, lmax;         /* after the batch                                    */
+    int32_t rows_recomputed;    /* rows 0..R recomputed (R + 1); rows above kept      */
+    int32_t method;             /* DC_MAINT_LOCAL or DC_MAINT_REPEEL                  */
+    uint32_t rebuilt;           /* 1 when the adjacency store grew (slack exhausted)  */
+    uint32_t pad;
+    uint64_t region;            /* vertices visited by the local kmax / row-0 update  */
+    float apply_ms, core_ms, rows_ms, total_ms;
+} dc_maint_stats;
+
+/* maintenanceFast (main.cu:1665-1751) / maintenance (main.cu:1536-1663):
+ * applies a batch of b edge updates to the device graph and brings the
+ * decomposition up to date.  pairs[2*i], pairs[2*i+1] = (from, to);
+ * is_delete[i] != 0 marks a deletion (is_delete NULL: all insertions).  The
+ * batch has sequential semantics and is applied as its net effect per edge;
+ * deleting an edge that is not present fails with DC_ERR_NOT_FOUND and leaves
+ * the graph unchanged.  Afterwards kmaxes and every row equal a full
+ * decomposition of the updated graph.  A graph without a decomposition is
+ * decomposed first.  stats may be NULL. */
+int dc_maintain(dc_graph* g, const uint32_t* pairs, const uint8_t* is_delete, uint64_t b, int method,
+                dc_maint_stats* stats);
 
 /* kmax of every vertex (in-degree core numbers, the values dc_decompose
  * reports through dc_get_kmaxes) without allocating any device memory.  No

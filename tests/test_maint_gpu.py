@@ -1,0 +1,159 @@
+"""Batch maintenance against full recomputation (the reference's own test
+criterion: main.cu:2116-2143 compares maintained kmaxes/lmaxes with
+checkDCore on the updated graph).  Integer results, compared exactly."""
+from collections import Counter
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+METHODS = [1, 2]  # DC_MAINT_LOCAL, DC_MAINT_REPEEL
+
+
+def _edges(cnt):
+    s, d = [], []
+    for (a, b), m in cnt.items():
+        s += [a] * m
+        d += [b] * m
+    return np.array(s, np.uint32), np.array(d, np.uint32)
+
+
+def _apply(cnt, u, v, dl):
+    for a, b, x in zip(u.tolist(), v.tolist(), dl.tolist()):
+        if x:
+            cnt[(a, b)] -= 1
+            assert cnt[(a, b)] >= 0
+            if cnt[(a, b)] == 0:
+                del cnt[(a, b)]
+        else:
+            cnt[(a, b)] += 1
+
+
+def _check(orc, g, V, cnt):
+    s, d = _edges(cnt)
+    okm, olm, okmaxes, orows = orc.dcore(V, s, d)
+    info = g.decomp_info()
+    assert (info["kmax"], info["lmax"]) == (okm, olm)
+    assert np.array_equal(g.kmaxes(), okmaxes)
+    rows = g.rows()
+    bad = np.argwhere(rows != orows)
+    assert bad.size == 0, f"{len(bad)} mismatches, first (k, v) = {bad[:5].tolist()}"
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("scale,seed", [(11, 5), (13, 6)])
+def test_mixed_stream_matches_recompute(dc, orc, gpu, method, scale, seed):
+    V, s, d = dc.gen_rmat(scale, 8, seed)
+    u, v, dl = dc.gen_updates(V, s, d, 700, 0.5, seed + 100)
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    with dc.Graph.from_edges(V, s, d) as g:
+        g.decompose()
+        i = 0
+        for bs in [1, 1, 2, 5, 20, 100, 571]:
+            st = g.maintain(u[i:i + bs], v[i:i + bs], dl[i:i + bs], method)
+            assert st["method"] == method
+            _apply(cnt, u[i:i + bs], v[i:i + bs], dl[i:i + bs])
+            _check(orc, g, V, cnt)
+            i += bs
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_er10k_single_inserts_and_deletes(dc, orc, gpu, method):
+    s, d = dc.gen_er(10_000, 100_000, 2)
+    u, v, dl = dc.gen_updates(10_000, s, d, 40, 0.5, 9)
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    with dc.Graph.from_edges(10_000, s, d) as g:
+        g.decompose()
+        for i in range(len(u)):
+            g.maintain(u[i:i + 1], v[i:i + 1], dl[i:i + 1], method)
+            _apply(cnt, u[i:i + 1], v[i:i + 1], dl[i:i + 1])
+            if i % 8 == 7:
+                _check(orc, g, 10_000, cnt)
+        _check(orc, g, 10_000, cnt)
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_insert_only_and_delete_only_batches(dc, orc, gpu, method):
+    V, s, d = dc.gen_rmat(12, 8, 8)
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    u, v, dl = dc.gen_updates(V, s, d, 400, 1.0, 3)  # inserts only
+    with dc.Graph.from_edges(V, s, d) as g:
+        g.decompose()
+        g.maintain(u, v, dl, method)
+        _apply(cnt, u, v, dl)
+        _check(orc, g, V, cnt)
+        # delete 300 present edges in one batch
+        es = list(cnt.keys())[:300]
+        du = np.array([a for a, _ in es], np.uint32)
+        dv = np.array([b for _, b in es], np.uint32)
+        g.maintain(du, dv, np.ones(len(du), np.uint8), method)
+        _apply(cnt, du, dv, np.ones(len(du), np.uint8))
+        _check(orc, g, V, cnt)
+
+
+def test_delete_missing_edge_rejected_graph_unchanged(dc, orc, gpu):
+    s, d = dc.gen_er(500, 3000, 4)
+    present = set(zip(s.tolist(), d.tolist()))
+    absent = [(a, b) for a in range(500) for b in range(500) if a != b and (a, b) not in present][:2]
+    ins, miss = absent
+    with dc.Graph.from_edges(500, s, d) as g:
+        g.decompose()
+        before = g.rows().copy()
+        # a valid insertion plus a deletion of an absent edge: nothing is applied
+        with pytest.raises(dc.DCoreError) as e:
+            g.maintain(np.array([ins[0], miss[0]], np.uint32), np.array([ins[1], miss[1]], np.uint32),
+                       np.array([0, 1], np.uint8))
+        assert e.value.code == -7
+        g2s, g2d = g.edges()
+        assert sorted(zip(g2s.tolist(), g2d.tolist())) == sorted(present)
+        g.decompose()
+        assert np.array_equal(g.rows(), before)
+
+
+def test_net_zero_and_multi_edges(dc, orc, gpu):
+    s, d = dc.gen_er(300, 2000, 6)
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    a, b = int(s[0]), int(d[0])  # present edge
+    with dc.Graph.from_edges(300, s, d) as g:
+        g.decompose()
+        # delete and re-insert the same edge, insert a duplicate of another
+        u = np.array([a, a, s[1], s[1]], np.uint32)
+        v = np.array([b, b, d[1], d[1]], np.uint32)
+        dl = np.array([1, 0, 0, 0], np.uint8)
+        st = g.maintain(u, v, dl)
+        assert st["deleted"] == 0 and st["inserted"] == 2
+        _apply(cnt, u, v, dl)
+        _check(orc, g, 300, cnt)
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_slack_overflow_rebuilds_store(dc, orc, gpu, method):
+    V, s, d = dc.gen_rmat(10, 8, 12)
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    present = set(cnt)
+    hub = int(np.bincount(s, minlength=V).argmax())
+    targets = [t for t in range(V) if t != hub and (hub, t) not in present][:40]
+    u = np.full(len(targets), hub, np.uint32)
+    v = np.array(targets, np.uint32)
+    with dc.Graph.from_edges(V, s, d, gap_min=1) as g:
+        g.decompose()
+        st = g.maintain(u, v, np.zeros(len(u), np.uint8), method)
+        assert st["rebuilt"] == 1
+        _apply(cnt, u, v, np.zeros(len(u), np.uint8))
+        _check(orc, g, V, cnt)
+        # the rebuilt store takes further updates
+        st = g.maintain(v[:5], u[:5], np.zeros(5, np.uint8), method)
+        _apply(cnt, v[:5], u[:5], np.zeros(5, np.uint8))
+        _check(orc, g, V, cnt)
+
+
+def test_maintain_before_decompose_and_auto(dc, orc, gpu):
+    V, s, d = dc.gen_rmat(11, 8, 13)
+    u, v, dl = dc.gen_updates(V, s, d, 50, 0.5, 14)
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    with dc.Graph.from_edges(V, s, d) as g:
+        st = g.maintain(u, v, dl, 0)  # decomposes first, scheduler picks
+        assert st["method"] in (1, 2)
+        _apply(cnt, u, v, dl)
+        _check(orc, g, V, cnt)
