@@ -66,6 +66,7 @@ SIGNATURES = {
     "dc_gen_er": [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p, u32p],
     "dc_gen_rmat": [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                     ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, u32p, u32p, u64p],
+    "dc_kmax_edge_batches": [ctypes.c_uint32, i32p, ctypes.c_uint64, u32p, u32p, i64p, i64p],
     "dc_gen_updates": [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_uint64, ctypes.c_double,
                        ctypes.c_uint64, u32p, u32p, u8p],
     "dc_text_read_edges": [ctypes.c_char_p, ctypes.c_int, u32p, u64p, u32p, u32p, ctypes.c_uint64],
@@ -207,6 +208,18 @@ def gen_updates(V, src, dst, n_ops, insert_frac, seed):
     _check(lib().dc_gen_updates(V, len(src), _p(src, u32p), _p(dst, u32p), n_ops, insert_frac, seed, _p(u, u32p),
                                 _p(v, u32p), _p(dl, u8p)))
     return u[:n_ops], v[:n_ops], dl[:n_ops]
+
+
+def kmax_edge_batches(kmaxes, frm, to):
+    """getKmaxEdgeBatches (KEDGE_BATCHING): (number of sub-batches, sub-batch of every edge)."""
+    kmaxes = np.ascontiguousarray(kmaxes, np.int32)
+    frm = np.ascontiguousarray(frm, np.uint32)
+    to = np.ascontiguousarray(to, np.uint32)
+    out = np.empty(max(len(frm), 1), np.int64)
+    nb = ctypes.c_int64(0)
+    _check(lib().dc_kmax_edge_batches(len(kmaxes), _p(kmaxes, i32p), len(frm), _p(frm, u32p), _p(to, u32p),
+                                      _p(out, i64p), ctypes.byref(nb)))
+    return nb.value, out[:len(frm)]
 
 
 # ---------------------------------------------------------------- file formats

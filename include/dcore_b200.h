@@ -205,6 +205,15 @@ typedef struct dc_maint_stats {
 int dc_maintain(dc_graph* g, const uint32_t* pairs, const uint8_t* is_delete, uint64_t b, int method,
                 dc_maint_stats* stats);
 
+/* getKmaxEdgeBatches with KEDGE_BATCHING (main.cu:1441-1488): partitions an
+ * insert batch into sub-batches whose roots (endpoint with the larger kmax,
+ * target on ties) share one kmax and are pairwise distinct, buckets in
+ * ascending kmax, edges in input order.  batch_of[e] = sub-batch of edge e
+ * (numbered as the reference appends them); *n_batches = their number.
+ * Host only. */
+int dc_kmax_edge_batches(uint32_t V, const int32_t* kmaxes, uint64_t B, const uint32_t* from, const uint32_t* to,
+                         int64_t* batch_of, int64_t* n_batches);
+
 /* kmax of every vertex (in-degree core numbers, the values dc_decompose
  * reports through dc_get_kmaxes) without allocating any device memory.  No
  * counterpart in the reference: it is for callers that cannot let a library
