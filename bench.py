@@ -43,7 +43,16 @@ WORKLOADS = {
     "decomp-rmat20": dict(gen="rmat", scale=20, ef=16, seed=1,
                           desc="R-MAT scale 20, edge factor 16, a=.57 b=.19 c=.19, dedup, permuted"),
     "decomp-er10k": dict(gen="er", n=10_000, m=100_000, seed=1, desc="directed G(n=10000, m=100000)"),
+    # maintenance: R-MAT graph + stream of 50% inserts of absent edges and 50%
+    # deletes of present edges, valid in sequence, in several batch sizes
+    "maint-rmat24": dict(gen="rmat", scale=24, ef=16, seed=1, ops=1_000_000, maint=True,
+                         sizes=[(1, 20), (100, 20), (10_000, 20), (1_000_000, 1)],
+                         desc="R-MAT scale 24, edge factor 16 + 1e6-op update stream (50% insert / 50% delete)"),
+    "maint-rmat22": dict(gen="rmat", scale=22, ef=16, seed=1, ops=1_000_000, maint=True,
+                         sizes=[(1, 20), (100, 20), (10_000, 20), (1_000_000, 1)],
+                         desc="R-MAT scale 22, edge factor 16 + 1e6-op update stream (50% insert / 50% delete)"),
 }
+METRIC_MAINT = "updates/s batched D-core maintenance"
 METRIC = "edges/s full D-core decomposition"
 
 
@@ -162,14 +171,68 @@ def run_reference(args, w, rank, world):
             vals.append(b["value"])
             base = b
     value = float(np.mean(vals))
-    line = {"metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": args.gpus, "steps": args.steps,
+    metric, unit = METRIC, "edges/s"
+    if w.get("maint"):
+        # the CPU path maintains by recomputing (the reference's own check,
+        # checkDCore): one batch of 10,000 updates costs one decomposition
+        metric, unit = METRIC_MAINT, "updates/s"
+        value = 10_000 * value / len(s)
+        base = dict(base, unit=unit, sample=base["sample"] + "; one recomputation per batch of 10,000 updates")
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * len(s) / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": args.workload, "graph": w["desc"], "V": V, "E": int(len(s))},
             "cpu_baseline": dict(base, value=value),
-            "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_maintenance(args, w, rank, world, local):
+    """Update stream in batches of several sizes; every batch leaves the
+    decomposition equal to a full recomputation of the updated graph."""
+    import torch
+    import dcore_b200 as dc
+    torch.cuda.set_device(local)
+    V, s, d = make_graph(dc, w, rank)
+    u, v, dl = dc.gen_updates(V, s, d, w["ops"], 0.5, w["seed"] + 1000 + rank)
+    g = dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16)
+    g.decompose(dc.METHOD_INCREMENTAL)
+    sampler = ClockSampler(local)
+    launches0 = dc.launch_count()
+    sampler.start()
+    pos = 0
+    per_size = {}
+    for bs, nb in w["sizes"]:
+        nb = min(nb, (len(u) - pos) // bs)
+        if nb <= 0:
+            continue
+        lat = []
+        methods = []
+        for _ in range(nb):
+            st = g.maintain(u[pos:pos + bs], v[pos:pos + bs], dl[pos:pos + bs], args.maint_method)
+            lat.append(st["total_ms"])
+            methods.append(st["method"])
+            pos += bs
+        lat = np.array(lat)
+        per_size[str(bs)] = {"batches": nb, "updates_per_s": bs * nb / (lat.sum() / 1000.0),
+                             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                             "methods": {"local": methods.count(1), "repeel": methods.count(2)}}
+    clocks = sampler.stop()
+    launches = dc.launch_count() - launches0
+    head = per_size.get("10000") or per_size[max(per_size, key=lambda k: int(k))]
+    line = {"metric": METRIC_MAINT, "value": head["updates_per_s"], "unit": "updates/s", "n_gpus": world,
+            "steps": sum(x["batches"] for x in per_size.values()), "warmup": 1,
+            "ms_per_step": head["p50_ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic",
+            "config": {"workload": args.workload, "graph": w["desc"], "V": V, "E": int(len(s)),
+                       "headline": "batches of 10,000 updates", "per_batch_size": per_size,
+                       "exactness": "each batch leaves kmaxes and rows equal to a full recomputation",
+                       "method": {0: "scheduler", 1: "local", 2: "re-peel"}[args.maint_method]},
+            "gpu_launches": int(launches), "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.free()
 
 
 def main():
@@ -182,6 +245,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--maint-method", type=int, default=0, help="0 scheduler, 1 local, 2 re-peel")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -190,6 +254,9 @@ def main():
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, w, rank, world)
+        return
+    if w.get("maint"):
+        run_maintenance(args, w, rank, world, local)
         return
 
     import torch
