@@ -274,6 +274,38 @@ extern "C" int dc_maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is
     return maintain(h, pairs, is_delete, b, method, stats);
 }
 
+extern "C" int dc_graph_set_scheduler(dc_graph* h, dc_sched* s) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    h->sched = s;
+    return DC_OK;
+}
+
+extern "C" int dc_maint_log_enable(dc_graph* h, int on) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    h->log_maint = on != 0;
+    if (!on) h->maint_log.clear();
+    return DC_OK;
+}
+
+// Records of the batches maintained since logging was enabled: features[16],
+// method, and total / core / rows milliseconds.
+extern "C" int dc_maint_log_get(dc_graph* h, float* features, int32_t* methods, float* times_ms, uint64_t capacity,
+                                uint64_t* n) {
+    if (!h || !n) return set_error(DC_ERR_INVALID, "null argument");
+    *n = h->maint_log.size();
+    if (!features || !methods || !times_ms) return DC_OK;
+    if (capacity < *n) return set_error(DC_ERR_CAPACITY, "dc_maint_log_get: capacity too small");
+    for (uint64_t i = 0; i < *n; ++i) {
+        const dc::MaintLogRec& r = h->maint_log[i];
+        memcpy(features + 16 * i, r.feat, sizeof(r.feat));
+        methods[i] = r.method;
+        times_ms[3 * i] = r.total_ms;
+        times_ms[3 * i + 1] = r.core_ms;
+        times_ms[3 * i + 2] = r.rows_ms;
+    }
+    return DC_OK;
+}
+
 extern "C" int dc_decomp_info_get(dc_graph* h, dc_decomp_info* info) {
     if (!h || !info) return set_error(DC_ERR_INVALID, "null argument");
     if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");

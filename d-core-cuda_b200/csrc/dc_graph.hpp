@@ -17,6 +17,7 @@
 //   rows[(kmax+1) * V]       optional dense rows, row-major (g.lmaxes)
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "dc_device.cuh"
@@ -62,6 +63,12 @@ struct Decomp {
     bool rows_valid = false;
 };
 
+struct MaintLogRec {
+    float feat[16];
+    int32_t method;
+    float total_ms, core_ms, rows_ms;
+};
+
 struct MaintTimes {
     float apply_ms = 0, core_ms = 0, rows_ms = 0, total_ms = 0;
 };
@@ -82,6 +89,9 @@ struct dc_graph {
     dc::Scratch* scratch = nullptr;
     dc::PhaseTimes times;
     dc::MaintTimes mtimes;
+    struct dc_sched* sched = nullptr;      // learned maintenance scheduler (not owned)
+    bool log_maint = false;                // record features and timings of each batch
+    std::vector<dc::MaintLogRec> maint_log;
     cudaEvent_t ev[8] = {};
     uint32_t gap_min = 1;      // minimum free slots per list
     uint32_t gap_div = 0;      // extra slack = len / gap_div (0 = none)

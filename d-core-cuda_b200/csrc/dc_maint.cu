@@ -23,6 +23,7 @@
 //      every row an updated edge or a changed kmax can reach; rows above R
 //      keep their skyline corners.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -448,6 +449,47 @@ __global__ void __launch_bounds__(kMThreads) k_core_local(CoreParams p) {
 }
 
 // ---------------------------------------------------------------------------
+// batch features for the scheduler
+// ---------------------------------------------------------------------------
+// acc: [0] sum log2(1+deg) over endpoints, [1] sum min-kmax, [2] dense-core
+// edges, [3] sum row-0 value over endpoints (floats); iacc: [0] max deg,
+// [1] max min-kmax (ints)
+__global__ void k_batch_features(uint32_t n, const uint32_t* u, const uint32_t* v, const int32_t* kmax,
+                                 const int32_t* row0, const int32_t* in_len, const int32_t* out_len, int K, float* acc,
+                                 int* iacc) {
+    float a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    int m0 = 0, m1 = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t x = u[i], y = v[i];
+        int dx = in_len[x] + out_len[x], dy = in_len[y] + out_len[y];
+        a0 += log2f(1.f + dx) + log2f(1.f + dy);
+        int mk = min(kmax[x], kmax[y]);
+        a1 += mk;
+        a2 += (2 * mk >= K) ? 1.f : 0.f;
+        a3 += row0[x] + row0[y];
+        m0 = max(m0, max(dx, dy));
+        m1 = max(m1, mk);
+    }
+#pragma unroll
+    for (int s = 16; s; s >>= 1) {
+        a0 += __shfl_xor_sync(0xFFFFFFFFu, a0, s);
+        a1 += __shfl_xor_sync(0xFFFFFFFFu, a1, s);
+        a2 += __shfl_xor_sync(0xFFFFFFFFu, a2, s);
+        a3 += __shfl_xor_sync(0xFFFFFFFFu, a3, s);
+        m0 = max(m0, __shfl_xor_sync(0xFFFFFFFFu, m0, s));
+        m1 = max(m1, __shfl_xor_sync(0xFFFFFFFFu, m1, s));
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(&acc[0], a0);
+        atomicAdd(&acc[1], a1);
+        atomicAdd(&acc[2], a2);
+        atomicAdd(&acc[3], a3);
+        atomicMax(&iacc[0], m0);
+        atomicMax(&iacc[1], m1);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // bound on the rows a batch can change
 // ---------------------------------------------------------------------------
 __global__ void k_rows_bound_edges(uint32_t n, const uint32_t* u, const uint32_t* v, const int32_t* kold,
@@ -552,13 +594,6 @@ __global__ void k_merge_fill(uint32_t V, int R, const int32_t* kmax, const uint3
 // ---------------------------------------------------------------------------
 namespace dc {
 
-// Rule of thumb: the local update of kmax and row 0 costs about its region
-// per inserted edge, the fused peel a fixed pass over the whole graph.
-int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del) {
-    (void)h;
-    return (n_ins + n_del <= 4096) ? DC_MAINT_LOCAL : DC_MAINT_REPEEL;
-}
-
 struct NetBatch {
     std::vector<uint32_t> del_u, del_v;  // distinct pairs with a net deletion
     std::vector<int32_t> del_n;          // occurrences to delete
@@ -609,6 +644,66 @@ template <typename T>
 static int upload(dc_graph* h, T** d, const std::vector<T>& hv) {
     if (mt_malloc(d, hv.size())) return DC_ERR_NOMEM;
     if (!hv.empty()) MT_CUDA(cudaMemcpyAsync(*d, hv.data(), sizeof(T) * hv.size(), cudaMemcpyHostToDevice, h->stream));
+    return DC_OK;
+}
+
+int sched_choose(dc_sched* s, const float* feat);
+
+// Rule of thumb (the scheduler's fallback): the local update of kmax and
+// row 0 grows with the batch (its bound on how far a value can rise is the
+// number of inserted edges), the fused peel is a fixed pass over the graph.
+int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del) {
+    (void)h;
+    return (n_ins + n_del <= 64) ? DC_MAINT_LOCAL : DC_MAINT_REPEEL;
+}
+
+// The 16 scheduler features of a net batch against the current graph and
+// decomposition (before the batch is applied).
+static int batch_features(dc_graph* h, const NetBatch& nb, float* f) {
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    std::vector<uint32_t> u(nb.del_u), v(nb.del_v);
+    u.insert(u.end(), nb.ins_u.begin(), nb.ins_u.end());
+    v.insert(v.end(), nb.ins_v.begin(), nb.ins_v.end());
+    const uint64_t n = u.size();
+    float acc[4] = {0, 0, 0, 0};
+    int iacc[2] = {0, 0};
+    if (n) {
+        uint32_t *du = nullptr, *dv = nullptr;
+        if (upload(h, &du, u) || upload(h, &dv, v)) {
+            mt_free(du);
+            mt_free(dv);
+            return DC_ERR_NOMEM;
+        }
+        float* dacc = (float*)h->scratch->tmp64;
+        int* diacc = (int*)(dacc + 4);
+        MT_CUDA(cudaMemsetAsync(dacc, 0, 32, h->stream));
+        ++g_launches;
+        k_batch_features<<<mgrid(h, n), kMThreads, 0, h->stream>>>((uint32_t)n, du, dv, d.kmax_v, d.row0, g.in_len,
+                                                                   g.out_len, d.kmax, dacc, diacc);
+        MT_CUDA(cudaMemcpyAsync(acc, dacc, 16, cudaMemcpyDeviceToHost, h->stream));
+        MT_CUDA(cudaMemcpyAsync(iacc, diacc, 8, cudaMemcpyDeviceToHost, h->stream));
+        MT_CUDA(cudaStreamSynchronize(h->stream));
+        mt_free(du);
+        mt_free(dv);
+    }
+    const double nn = n ? (double)n : 1.0, K1 = d.kmax + 1.0, L1 = d.lmax + 1.0;
+    f[0] = (float)std::log2(1.0 + nb.n_ins);
+    f[1] = (float)std::log2(1.0 + nb.n_del);
+    f[2] = (float)std::log2(1.0 + g.V);
+    f[3] = (float)std::log2(1.0 + g.E);
+    f[4] = (float)std::log2(K1);
+    f[5] = (float)std::log2(L1);
+    f[6] = (float)(acc[0] / (2.0 * nn));
+    f[7] = (float)std::log2(1.0 + iacc[0]);
+    f[8] = (float)(acc[1] / nn / K1);
+    f[9] = (float)(iacc[1] / K1);
+    f[10] = (float)(acc[2] / nn);
+    f[11] = (float)(acc[3] / (2.0 * nn) / L1);
+    f[12] = (float)std::log2(1.0 + (double)d.n_corners / (g.V ? g.V : 1));
+    f[13] = (float)((double)nb.n_ins / (double)std::max<uint64_t>(1, nb.n_ins + nb.n_del));
+    f[14] = (float)std::log2(1.0 + n);
+    f[15] = 1.0f;
     return DC_OK;
 }
 
@@ -821,7 +916,14 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
     if (int rc = net_batch(V, pairs, is_del, b, nb)) return rc;
     st->deleted = nb.n_del;
     st->inserted = nb.n_ins;
-    if (method == DC_MAINT_AUTO) method = choose_method(h, nb.n_ins, nb.n_del);
+    float feat[16];
+    const bool want_feat = h->log_maint || (method == DC_MAINT_AUTO && h->sched);
+    if (want_feat)
+        if (int rc = batch_features(h, nb, feat)) return rc;
+    if (method == DC_MAINT_AUTO) {
+        int m = h->sched ? sched_choose(h->sched, feat) : -1;
+        method = m > 0 ? m : choose_method(h, nb.n_ins, nb.n_del);
+    }
     st->method = method;
     cudaEvent_t* ev = h->ev;
     cudaEventRecord(ev[0], h->stream);
@@ -976,6 +1078,15 @@ timing:
     }
     st->kmax = d.kmax;
     st->lmax = d.lmax;
+    if (h->log_maint && want_feat) {
+        MaintLogRec r;
+        memcpy(r.feat, feat, sizeof(feat));
+        r.method = st->method;
+        r.total_ms = st->total_ms;
+        r.core_ms = st->core_ms;
+        r.rows_ms = st->rows_ms;
+        h->maint_log.push_back(r);
+    }
 out:
     mt_free(d_du);
     mt_free(d_dv);

@@ -37,6 +37,7 @@ i32p = ctypes.POINTER(ctypes.c_int32)
 u64p = ctypes.POINTER(ctypes.c_uint64)
 i64p = ctypes.POINTER(ctypes.c_int64)
 u8p = ctypes.POINTER(ctypes.c_uint8)
+f32p = ctypes.POINTER(ctypes.c_float)
 vp = ctypes.c_void_p
 
 
@@ -103,6 +104,21 @@ SIGNATURES = {
     "dc_graph_stream": [vp, ctypes.POINTER(vp)],
     "dc_set_trace": [vp, ctypes.c_uint32, vp, vp],
     "dc_set_launch": [vp, ctypes.c_int],
+    "dc_sched_create": [ctypes.c_uint64, ctypes.POINTER(vp)],
+    "dc_sched_free": [vp],
+    "dc_sched_param_count": [],
+    "dc_sched_get_params": [vp, ctypes.POINTER(ctypes.c_float)],
+    "dc_sched_set_params": [vp, ctypes.POINTER(ctypes.c_float)],
+    "dc_sched_set_norm": [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
+    "dc_sched_predict": [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)],
+    "dc_sched_grad": [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), u8p, ctypes.c_uint64,
+                      ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
+    "dc_sched_train": [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), u8p, ctypes.c_uint64,
+                       ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_float)],
+    "dc_graph_set_scheduler": [vp, vp],
+    "dc_maint_log_enable": [vp, ctypes.c_int],
+    "dc_maint_log_get": [vp, ctypes.POINTER(ctypes.c_float), i32p, ctypes.POINTER(ctypes.c_float), ctypes.c_uint64,
+                         u64p],
     "dc_kmax_noalloc": [ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp, vp, i32p, vp],
     "dc_launch_count": [u64p],
     "dc_last_error": [],
@@ -382,6 +398,22 @@ class Graph:
                                  ctypes.byref(st)))
         return {f: getattr(st, f) for f, _ in MaintStats._fields_ if f != "pad"}
 
+    def set_scheduler(self, sched):
+        _check(lib().dc_graph_set_scheduler(self._h, sched.handle if sched is not None else None))
+        self._sched_ref = sched
+
+    def maint_log(self, enable=None):
+        """With enable=True/False switches logging; returns (features[n,16], methods[n], times_ms[n,3])."""
+        if enable is not None:
+            _check(lib().dc_maint_log_enable(self._h, int(enable)))
+        n = ctypes.c_uint64(0)
+        _check(lib().dc_maint_log_get(self._h, None, None, None, 0, ctypes.byref(n)))
+        f = np.empty((max(n.value, 1), 16), np.float32)
+        m = np.empty(max(n.value, 1), np.int32)
+        t = np.empty((max(n.value, 1), 3), np.float32)
+        _check(lib().dc_maint_log_get(self._h, _p(f, f32p), _p(m, i32p), _p(t, f32p), n.value, ctypes.byref(n)))
+        return f[:n.value], m[:n.value], t[:n.value]
+
     def decomp_info(self):
         info = DecompInfo()
         _check(lib().dc_decomp_info_get(self._h, ctypes.byref(info)))
@@ -454,6 +486,70 @@ class Graph:
         s = vp()
         _check(lib().dc_graph_stream(self._h, ctypes.byref(s)))
         return s.value or 0
+
+
+class Scheduler:
+    """The learned maintenance scheduler (BF16 MLP 16-64-64-2 on the GPU)."""
+
+    def __init__(self, seed=0):
+        h = vp()
+        _check(lib().dc_sched_create(seed, ctypes.byref(h)))
+        self._h = h
+        self.nparams = lib().dc_sched_param_count()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def free(self):
+        if self._h and self._h.value:
+            lib().dc_sched_free(self._h)
+            self._h = vp()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def params(self):
+        p = np.empty(self.nparams, np.float32)
+        _check(lib().dc_sched_get_params(self._h, _p(p, f32p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        _check(lib().dc_sched_set_params(self._h, _p(p, f32p)))
+
+    def set_norm(self, mean, scale):
+        mean = np.ascontiguousarray(mean, np.float32)
+        scale = np.ascontiguousarray(scale, np.float32)
+        _check(lib().dc_sched_set_norm(self._h, _p(mean, f32p), _p(scale, f32p)))
+
+    def predict(self, X):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, 16)
+        Y = np.empty((len(X), 2), np.float32)
+        _check(lib().dc_sched_predict(self._h, _p(X, f32p), len(X), _p(Y, f32p)))
+        return Y
+
+    def grad(self, X, T, M):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, 16)
+        T = np.ascontiguousarray(T, np.float32).reshape(-1, 2)
+        M = np.ascontiguousarray(M, np.uint8).reshape(-1, 2)
+        g = np.empty(self.nparams, np.float32)
+        loss = ctypes.c_float(0)
+        _check(lib().dc_sched_grad(self._h, _p(X, f32p), _p(T, f32p), _p(M, u8p), len(X), _p(g, f32p),
+                                   ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, X, T, M, epochs=200, lr=3e-3):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, 16)
+        T = np.ascontiguousarray(T, np.float32).reshape(-1, 2)
+        M = np.ascontiguousarray(M, np.uint8).reshape(-1, 2)
+        loss = ctypes.c_float(0)
+        _check(lib().dc_sched_train(self._h, _p(X, f32p), _p(T, f32p), _p(M, u8p), len(X), epochs, lr,
+                                    ctypes.byref(loss)))
+        return loss.value
 
 
 def exported_symbols():

@@ -205,6 +205,37 @@ typedef struct dc_maint_stats {
 int dc_maintain(dc_graph* g, const uint32_t* pairs, const uint8_t* is_delete, uint64_t b, int method,
                 dc_maint_stats* stats);
 
+/* ---- learned maintenance scheduler -------------------------------------- */
+/* A BF16 MLP (16 -> 64 -> 64 -> 2, ReLU) predicting the log of the wall time
+ * of DC_MAINT_LOCAL (output 0) and DC_MAINT_REPEEL (output 1) from 16
+ * features of a batch (dc_maint_log_get lists them); DC_MAINT_AUTO runs the
+ * method with the smaller prediction, the rule of thumb when no network is
+ * attached.  Either method gives exact results.  Training and inference run
+ * in the engine's own CUDA kernels.  No reference counterpart (the reference
+ * fixes its batching mode at compile time, src/common.h:18-19). */
+typedef struct dc_sched dc_sched;
+int dc_sched_create(uint64_t seed, dc_sched** out);
+int dc_sched_free(dc_sched* s);
+int dc_sched_param_count(void);
+/* fp32 parameters, layout W1[64][16], b1[64], W2[64][64], b2[64], W3[2][64], b3[2] */
+int dc_sched_get_params(dc_sched* s, float* params);
+int dc_sched_set_params(dc_sched* s, const float* params);
+/* input normalisation x' = (x - mean) * scale, 16 values each */
+int dc_sched_set_norm(dc_sched* s, const float* mean, const float* scale);
+/* Y[n][2] = network(X[n][16]) */
+int dc_sched_predict(dc_sched* s, const float* X, uint64_t n, float* Y);
+/* Gradient (fp32, dc_sched_param_count values) and loss of the mean squared
+ * error over the (sample, output) pairs with M != 0; parameters unchanged. */
+int dc_sched_grad(dc_sched* s, const float* X, const float* T, const uint8_t* M, uint64_t n, float* grad, float* loss);
+/* `epochs` full-batch Adam steps on the same loss. */
+int dc_sched_train(dc_sched* s, const float* X, const float* T, const uint8_t* M, uint64_t n, int epochs, float lr,
+                   float* final_loss);
+/* Attach (or with NULL detach) a scheduler to a graph for DC_MAINT_AUTO. */
+int dc_graph_set_scheduler(dc_graph* g, dc_sched* s);
+/* Feature / timing log of maintained batches (training data). */
+int dc_maint_log_enable(dc_graph* g, int on);
+int dc_maint_log_get(dc_graph* g, float* features, int32_t* methods, float* times_ms, uint64_t capacity, uint64_t* n);
+
 /* getKmaxEdgeBatches with KEDGE_BATCHING (main.cu:1441-1488): partitions an
  * insert batch into sub-batches whose roots (endpoint with the larger kmax,
  * target on ties) share one kmax and are pairwise distinct, buckets in
