@@ -1,6 +1,7 @@
 // C ABI of the engine: graph handles, decomposition and result access.
 // Each function names the reference entry point it stands in for; the
 // declarations with full documentation are in include/dcore_b200.h.
+#include <atomic>
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -106,9 +107,10 @@ extern "C" int dc_graph_create(uint32_t V, uint64_t E, const uint32_t* src, cons
     if (int rc = new_handle(opts, &h)) return rc;
     uint32_t *d_src = nullptr, *d_dst = nullptr;
     size_t bytes = (E ? E : 1) * sizeof(uint32_t);
-    if (cudaMalloc(&d_src, bytes) != cudaSuccess || cudaMalloc(&d_dst, bytes) != cudaSuccess) {
+    if (cudaMallocAsync(&d_src, bytes, h->stream) != cudaSuccess ||
+        cudaMallocAsync(&d_dst, bytes, h->stream) != cudaSuccess) {
         cudaGetLastError();
-        if (d_src) cudaFree(d_src);
+        if (d_src) cudaFreeAsync(d_src, h->stream);
         dc_graph_free(h);
         return set_error(DC_ERR_NOMEM, "dc_graph_create: cannot stage %llu edges on the device", (unsigned long long)E);
     }
@@ -119,9 +121,9 @@ extern "C" int dc_graph_create(uint32_t V, uint64_t E, const uint32_t* src, cons
             rc = set_error(DC_ERR_CUDA, "dc_graph_create: edge upload failed");
     }
     if (rc == DC_OK) rc = build_from_device_edges(h, V, E, d_src, d_dst);
+    cudaFreeAsync(d_src, h->stream);
+    cudaFreeAsync(d_dst, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
-    cudaFree(d_src);
-    cudaFree(d_dst);
     if (rc == DC_OK && e != cudaSuccess) rc = set_error(DC_ERR_CUDA, "graph build: %s", cudaGetErrorString(e));
     if (rc != DC_OK) {
         dc_graph_free(h);
@@ -187,10 +189,11 @@ extern "C" int dc_graph_free(dc_graph* h) {
     if (!h) return DC_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     dc_set_trace(h, 0, nullptr, nullptr);
-    free_graph_arrays(h->g);
-    free_decomp(h->d);
+    free_graph_arrays(h->g, h->stream);
+    free_decomp(h->d, h->stream);
     free_scratch(h);
-    if (h->ctl) cudaFree(h->ctl);
+    if (h->ctl) cudaFreeAsync(h->ctl, h->stream);
+    if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -202,6 +205,12 @@ extern "C" int dc_graph_info(const dc_graph* h, uint32_t* V, uint64_t* E) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");
     if (V) *V = h->g.V;
     if (E) *E = h->g.E;
+    return DC_OK;
+}
+
+extern "C" int dc_graph_device_bytes(const dc_graph* h, uint64_t* bytes) {
+    if (!h || !bytes) return set_error(DC_ERR_INVALID, "null argument");
+    *bytes = device_footprint(h);
     return DC_OK;
 }
 
@@ -364,9 +373,9 @@ extern "C" int dc_get_lmax_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* o
     chunk_rows = std::min<uint64_t>(chunk_rows, n);
     int32_t* stage[2] = {nullptr, nullptr};
     for (int i = 0; i < 2; ++i)
-        if (cudaMalloc(&stage[i], 4 * chunk_rows * V) != cudaSuccess) {
+        if (cudaMallocAsync(&stage[i], 4 * chunk_rows * V, h->stream) != cudaSuccess) {
             cudaGetLastError();
-            if (stage[0]) cudaFree(stage[0]);
+            if (stage[0]) cudaFreeAsync(stage[0], h->stream);
             return set_error(DC_ERR_NOMEM, "row staging buffer allocation failed");
         }
     int rc = DC_OK;
@@ -377,9 +386,9 @@ extern "C" int dc_get_lmax_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* o
         if (rc == DC_OK && cudaMemcpyAsync(out + r * V, stage[b], 4 * m * V, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
             rc = set_error(DC_ERR_CUDA, "row download failed");
     }
+    cudaFreeAsync(stage[0], h->stream);
+    cudaFreeAsync(stage[1], h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
-    cudaFree(stage[0]);
-    cudaFree(stage[1]);
     if (rc == DC_OK && e != cudaSuccess) rc = set_error(DC_ERR_CUDA, "row download: %s", cudaGetErrorString(e));
     return rc;
 }
@@ -390,10 +399,10 @@ extern "C" int dc_materialize_rows(dc_graph* h) {
     if (h->d.rows_valid) return DC_OK;
     uint64_t elems = (uint64_t)(h->d.kmax + 1) * h->g.V;
     if (h->d.rows_cap < elems) {
-        if (h->d.rows) cudaFree(h->d.rows);
+        if (h->d.rows) cudaFreeAsync(h->d.rows, h->stream);
         h->d.rows = nullptr;
         h->d.rows_cap = 0;
-        if (cudaMalloc(&h->d.rows, 4 * (elems ? elems : 1)) != cudaSuccess) {
+        if (cudaMallocAsync(&h->d.rows, 4 * (elems ? elems : 1), h->stream) != cudaSuccess) {
             cudaGetLastError();
             return set_error(DC_ERR_NOMEM, "dense rows (%llu values) do not fit in device memory",
                              (unsigned long long)elems);
@@ -408,7 +417,8 @@ extern "C" int dc_materialize_rows(dc_graph* h) {
 
 extern "C" int dc_release_rows(dc_graph* h) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");
-    if (h->d.rows) cudaFree(h->d.rows);
+    if (h->d.rows) cudaFreeAsync(h->d.rows, h->stream);
+    cudaStreamSynchronize(h->stream);
     h->d.rows = nullptr;
     h->d.rows_cap = 0;
     h->d.rows_valid = false;
@@ -481,12 +491,12 @@ extern "C" int dc_host_free(void* p) {
 }
 
 namespace dc {
-extern unsigned long long g_launches;
+extern std::atomic<unsigned long long> g_launches;
 }
 
 extern "C" int dc_launch_count(unsigned long long* n) {
     if (!n) return set_error(DC_ERR_INVALID, "null argument");
-    *n = dc::g_launches;
+    *n = dc::g_launches.load();
     return DC_OK;
 }
 

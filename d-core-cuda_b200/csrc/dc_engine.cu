@@ -12,6 +12,7 @@
 // device work queue for cascades, no host round trip per level), and rows
 // k >= 1 derived from row k-1 by h-index refinement instead of one fresh
 // peel per row (see k_transitions).
+#include <atomic>
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -23,7 +24,7 @@
 namespace dc {
 
 // Kernel launches issued by the engine since load (host counter).
-unsigned long long g_launches = 0;
+std::atomic<unsigned long long> g_launches{0};
 
 #define DC_CUDA(call)                                                                        \
     do {                                                                                     \
@@ -40,11 +41,15 @@ static constexpr int kWarpsPerBlock = kThreads / 32;
 // small helpers
 // ---------------------------------------------------------------------------
 
+// Device buffers of a handle come from the device's stream-ordered pool on
+// the handle's stream: no implicit device-wide synchronisation, so handles on
+// different streams (the serving loop runs many) keep their kernels
+// overlapping while they allocate and free.
 template <typename T>
-static int dmalloc(T** p, uint64_t n) {
+static int dmalloc(cudaStream_t st, T** p, uint64_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    cudaError_t e = cudaMallocAsync((void**)p, n * sizeof(T), st);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
@@ -54,8 +59,8 @@ static int dmalloc(T** p, uint64_t n) {
     return DC_OK;
 }
 template <typename T>
-static void dfree(T*& p) {
-    if (p) cudaFree((void*)p);
+static void dfree(cudaStream_t st, T*& p) {
+    if (p) cudaFreeAsync((void*)p, st);
     p = nullptr;
 }
 
@@ -1174,28 +1179,34 @@ int init_handle(dc_graph* h) {
     h->geom.sms = prop.multiProcessorCount;
     h->geom.threads = kThreads;
     DC_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-    if (dmalloc(&h->ctl, 1)) return DC_ERR_NOMEM;
+    // Freed blocks stay in the device's default pool for reuse instead of
+    // going back to the driver at every synchronisation.
+    cudaMemPool_t pool;
+    DC_CUDA(cudaDeviceGetDefaultMemPool(&pool, h->device));
+    uint64_t keep = ~0ull;
+    DC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    if (dmalloc(h->stream, &h->ctl, 1)) return DC_ERR_NOMEM;
     for (auto& e : h->ev) DC_CUDA(cudaEventCreate(&e));
     return DC_OK;
 }
 
-void free_graph_arrays(DevGraph& g) {
-    dfree(g.out_off);
-    dfree(g.out_len);
-    dfree(g.out_nbr);
-    dfree(g.in_off);
-    dfree(g.in_len);
-    dfree(g.in_nbr);
+void free_graph_arrays(DevGraph& g, cudaStream_t st) {
+    dfree(st, g.out_off);
+    dfree(st, g.out_len);
+    dfree(st, g.out_nbr);
+    dfree(st, g.in_off);
+    dfree(st, g.in_len);
+    dfree(st, g.in_nbr);
     g.out_cap = g.in_cap = 0;
 }
 
-void free_decomp(Decomp& d) {
-    dfree(d.kmax_v);
-    dfree(d.row0);
-    dfree(d.sky_off);
-    dfree(d.sky_k);
-    dfree(d.sky_l);
-    dfree(d.rows);
+void free_decomp(Decomp& d, cudaStream_t st) {
+    dfree(st, d.kmax_v);
+    dfree(st, d.row0);
+    dfree(st, d.sky_off);
+    dfree(st, d.sky_k);
+    dfree(st, d.sky_l);
+    dfree(st, d.rows);
     d.rows_cap = 0;
     d.corner_cap = 0;
     d.valid = false;
@@ -1205,37 +1216,36 @@ void free_decomp(Decomp& d) {
 void free_scratch(dc_graph* h) {
     Scratch* s = h->scratch;
     if (!s) return;
-    dfree(s->key);
-    dfree(s->cdeg);
-    dfree(s->cur);
-    dfree(s->row0);
-    dfree(s->mark);
-    dfree(s->stamp);
-    dfree(s->logidx);
-    dfree(s->rem0);
-    dfree(s->rem1);
-    dfree(s->order);
-    dfree(s->ck);
-    dfree(s->ring);
-    dfree(s->log_v);
-    dfree(s->log_k);
-    dfree(s->log_l);
-    dfree(s->tmp64);
-    dfree(s->partial);
-    dfree(s->cursor);
-    if (s->tmp_edges) cudaFree(s->tmp_edges);
-    dfree(s->key2);
-    dfree(s->cdeg2);
-    dfree(s->rem2);
-    dfree(s->rem3);
-    dfree(s->cnt_out);
-    dfree(s->tring);
-    dfree(s->w_out_len);
-    dfree(s->w_in_len);
-    dfree(s->w_out_nbr);
-    dfree(s->w_in_nbr);
-    dfree(s->kmax_old);
-    dfree(s->row0_old);
+    dfree(h->stream, s->key);
+    dfree(h->stream, s->cdeg);
+    dfree(h->stream, s->cur);
+    dfree(h->stream, s->row0);
+    dfree(h->stream, s->mark);
+    dfree(h->stream, s->stamp);
+    dfree(h->stream, s->logidx);
+    dfree(h->stream, s->rem0);
+    dfree(h->stream, s->rem1);
+    dfree(h->stream, s->order);
+    dfree(h->stream, s->ck);
+    dfree(h->stream, s->ring);
+    dfree(h->stream, s->log_v);
+    dfree(h->stream, s->log_k);
+    dfree(h->stream, s->log_l);
+    dfree(h->stream, s->tmp64);
+    dfree(h->stream, s->partial);
+    dfree(h->stream, s->cursor);
+    dfree(h->stream, s->key2);
+    dfree(h->stream, s->cdeg2);
+    dfree(h->stream, s->rem2);
+    dfree(h->stream, s->rem3);
+    dfree(h->stream, s->cnt_out);
+    dfree(h->stream, s->tring);
+    dfree(h->stream, s->w_out_len);
+    dfree(h->stream, s->w_in_len);
+    dfree(h->stream, s->w_out_nbr);
+    dfree(h->stream, s->w_in_nbr);
+    dfree(h->stream, s->kmax_old);
+    dfree(h->stream, s->row0_old);
     delete s;
     h->scratch = nullptr;
 }
@@ -1245,25 +1255,43 @@ int ensure_scratch(dc_graph* h, uint32_t V) {
     Scratch* s = h->scratch;
     if (s->cap_V >= V && s->key) return DC_OK;
     // release V-sized buffers and reallocate
-    dfree(s->key); dfree(s->cdeg); dfree(s->cur); dfree(s->row0); dfree(s->mark); dfree(s->stamp);
-    dfree(s->logidx); dfree(s->rem0); dfree(s->rem1); dfree(s->order); dfree(s->ring); dfree(s->tmp64);
-    dfree(s->partial); dfree(s->cursor);
-    dfree(s->key2); dfree(s->cdeg2); dfree(s->rem2); dfree(s->rem3); dfree(s->cnt_out);
+    dfree(h->stream, s->key); dfree(h->stream, s->cdeg); dfree(h->stream, s->cur); dfree(h->stream, s->row0); dfree(h->stream, s->mark); dfree(h->stream, s->stamp);
+    dfree(h->stream, s->logidx); dfree(h->stream, s->rem0); dfree(h->stream, s->rem1); dfree(h->stream, s->order); dfree(h->stream, s->ring); dfree(h->stream, s->tmp64);
+    dfree(h->stream, s->partial); dfree(h->stream, s->cursor);
+    dfree(h->stream, s->key2); dfree(h->stream, s->cdeg2); dfree(h->stream, s->rem2); dfree(h->stream, s->rem3); dfree(h->stream, s->cnt_out);
     uint64_t n = (uint64_t)V + 1;
-    if (dmalloc(&s->key, n) || dmalloc(&s->cdeg, n) || dmalloc(&s->cur, n) || dmalloc(&s->row0, n) ||
-        dmalloc(&s->mark, n) || dmalloc(&s->stamp, n) || dmalloc(&s->logidx, n) || dmalloc(&s->rem0, n) ||
-        dmalloc(&s->rem1, n) || dmalloc(&s->order, n) || dmalloc(&s->tmp64, n + 1) ||
-        dmalloc(&s->partial, (uint64_t)h->geom.sms * 64 + 64) || dmalloc(&s->cursor, n + 1) ||
-        dmalloc(&s->key2, n) || dmalloc(&s->cdeg2, n) || dmalloc(&s->rem2, n) || dmalloc(&s->rem3, n) ||
-        dmalloc(&s->cnt_out, n))
+    if (dmalloc(h->stream, &s->key, n) || dmalloc(h->stream, &s->cdeg, n) || dmalloc(h->stream, &s->cur, n) || dmalloc(h->stream, &s->row0, n) ||
+        dmalloc(h->stream, &s->mark, n) || dmalloc(h->stream, &s->stamp, n) || dmalloc(h->stream, &s->logidx, n) || dmalloc(h->stream, &s->rem0, n) ||
+        dmalloc(h->stream, &s->rem1, n) || dmalloc(h->stream, &s->order, n) || dmalloc(h->stream, &s->tmp64, n + 1) ||
+        dmalloc(h->stream, &s->partial, (uint64_t)h->geom.sms * 64 + 64) || dmalloc(h->stream, &s->cursor, n + 1) ||
+        dmalloc(h->stream, &s->key2, n) || dmalloc(h->stream, &s->cdeg2, n) || dmalloc(h->stream, &s->rem2, n) || dmalloc(h->stream, &s->rem3, n) ||
+        dmalloc(h->stream, &s->cnt_out, n))
         return DC_ERR_NOMEM;
     uint64_t need = (uint64_t)V + (uint64_t)h->geom.sms * 64 * 32 + 64;
     uint64_t rc = 1024;
     while (rc < need) rc <<= 1;
-    if (dmalloc(&s->ring, rc)) return DC_ERR_NOMEM;
+    if (dmalloc(h->stream, &s->ring, rc)) return DC_ERR_NOMEM;
     s->ring_mask = (uint32_t)(rc - 1);
     s->cap_V = V;
     return DC_OK;
+}
+
+uint64_t device_footprint(const dc_graph* h) {
+    const DevGraph& g = h->g;
+    const Decomp& d = h->d;
+    uint64_t V1 = (uint64_t)g.V + 1;
+    uint64_t b = sizeof(EngineCtl);
+    if (g.out_off) b += 2 * 4 * (2 * V1) + 4 * (g.out_cap + g.in_cap);
+    if (d.kmax_v) b += 4 * (3 * V1) + 8 * d.corner_cap;
+    b += 4 * d.rows_cap;
+    if (const Scratch* s = h->scratch) {
+        uint64_t n = (uint64_t)s->cap_V + 1;
+        if (s->key) b += 4 * (16 * n + 1) + 8 * (n + 1) + 8 * ((uint64_t)h->geom.sms * 64 + 64) + 4ull * (s->ring_mask + 1ull);
+        b += 4ull * s->ck_cap + 12 * s->log_cap + 8 * s->tring_cap;
+        b += 4 * (s->w_out_cap + s->w_in_cap);
+        if (s->kmax_old) b += 8 * n;
+    }
+    return b;
 }
 
 // Exclusive scan of n u64 values in s->tmp64 (tmp64[n] receives the total).
@@ -1300,7 +1328,7 @@ static int finish_build(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_s
             return set_error(DC_ERR_CAPACITY, "adjacency with slack exceeds 2^32 entries (u32 offsets)");
         uint32_t** off = side == 0 ? &g.out_off : &g.in_off;
         uint32_t** nbr = side == 0 ? &g.out_nbr : &g.in_nbr;
-        if (dmalloc(off, (uint64_t)V + 1) || dmalloc(nbr, total)) return DC_ERR_NOMEM;
+        if (dmalloc(h->stream, off, (uint64_t)V + 1) || dmalloc(h->stream, nbr, total)) return DC_ERR_NOMEM;
         ++g_launches;
         k_off_to_u32<<<grid_for(h, (uint64_t)V + 1), kThreads, 0, h->stream>>>(V, (unsigned long long*)s->tmp64, *off);
         if (side == 0) g.out_cap = total;
@@ -1320,11 +1348,11 @@ static int finish_build(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_s
 }
 
 int build_from_device_edges(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_src, const uint32_t* d_dst) {
-    free_graph_arrays(h->g);
-    free_decomp(h->d);
+    free_graph_arrays(h->g, h->stream);
+    free_decomp(h->d, h->stream);
     if (int rc = ensure_scratch(h, V)) return rc;
     DevGraph& g = h->g;
-    if (dmalloc(&g.out_len, (uint64_t)V + 1) || dmalloc(&g.in_len, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+    if (dmalloc(h->stream, &g.out_len, (uint64_t)V + 1) || dmalloc(h->stream, &g.in_len, (uint64_t)V + 1)) return DC_ERR_NOMEM;
     DC_CUDA(cudaMemsetAsync(g.out_len, 0, sizeof(int32_t) * ((uint64_t)V + 1), h->stream));
     DC_CUDA(cudaMemsetAsync(g.in_len, 0, sizeof(int32_t) * ((uint64_t)V + 1), h->stream));
     DC_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
@@ -1370,15 +1398,15 @@ int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_d
     (void)in_nbr;
     // The reference binary stores both directions; the out-lists define the
     // edge multiset, so the device rebuilds both sides from them.
-    free_graph_arrays(h->g);
-    free_decomp(h->d);
+    free_graph_arrays(h->g, h->stream);
+    free_decomp(h->d, h->stream);
     if (int rc = ensure_scratch(h, V)) return rc;
     uint32_t *d_off = nullptr, *d_nbr = nullptr, *d_src = nullptr, *d_dst = nullptr;
     int32_t* d_deg = nullptr;
     int rc = DC_OK;
-    if ((rc = dmalloc(&d_off, (uint64_t)V + 1)) || (rc = dmalloc(&d_nbr, nbr_len)) || (rc = dmalloc(&d_deg, V)) ||
-        (rc = dmalloc(&d_src, E)) || (rc = dmalloc(&d_dst, E))) {
-        dfree(d_off); dfree(d_nbr); dfree(d_deg); dfree(d_src); dfree(d_dst);
+    if ((rc = dmalloc(h->stream, &d_off, (uint64_t)V + 1)) || (rc = dmalloc(h->stream, &d_nbr, nbr_len)) || (rc = dmalloc(h->stream, &d_deg, V)) ||
+        (rc = dmalloc(h->stream, &d_src, E)) || (rc = dmalloc(h->stream, &d_dst, E))) {
+        dfree(h->stream, d_off); dfree(h->stream, d_nbr); dfree(h->stream, d_deg); dfree(h->stream, d_src); dfree(h->stream, d_dst);
         return rc;
     }
     Scratch* s = h->scratch;
@@ -1394,7 +1422,7 @@ int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_d
     }
     eo[V] = acc;
     if (acc != E) {
-        dfree(d_off); dfree(d_nbr); dfree(d_deg); dfree(d_src); dfree(d_dst);
+        dfree(h->stream, d_off); dfree(h->stream, d_nbr); dfree(h->stream, d_deg); dfree(h->stream, d_src); dfree(h->stream, d_dst);
         return set_error(DC_ERR_INVALID, "binary graph: out-degrees sum to %llu, header says %llu", acc,
                          (unsigned long long)E);
     }
@@ -1404,17 +1432,17 @@ int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_d
     k_csr_to_edges<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, h->stream>>>(
         V, d_off, d_deg, (const unsigned long long*)s->tmp64, d_nbr, d_src, d_dst, 0);
     cudaError_t e = cudaStreamSynchronize(h->stream);
-    dfree(d_off);
-    dfree(d_nbr);
-    dfree(d_deg);
+    dfree(h->stream, d_off);
+    dfree(h->stream, d_nbr);
+    dfree(h->stream, d_deg);
     if (e != cudaSuccess) {
-        dfree(d_src); dfree(d_dst);
+        dfree(h->stream, d_src); dfree(h->stream, d_dst);
         return set_error(DC_ERR_CUDA, "binary graph upload failed: %s", cudaGetErrorString(e));
     }
     rc = build_from_device_edges(h, V, E, d_src, d_dst);
     cudaStreamSynchronize(h->stream);
-    dfree(d_src);
-    dfree(d_dst);
+    dfree(h->stream, d_src);
+    dfree(h->stream, d_dst);
     return rc;
 }
 
@@ -1423,9 +1451,9 @@ int ensure_tring(dc_graph* h, uint64_t need) {
     uint64_t cap = 1024;
     while (cap < need) cap <<= 1;
     if (s->tring_cap >= cap && s->tring) return DC_OK;
-    dfree(s->tring);
+    dfree(h->stream, s->tring);
     s->tring_cap = 0;
-    if (dmalloc(&s->tring, cap)) return DC_ERR_NOMEM;
+    if (dmalloc(h->stream, &s->tring, cap)) return DC_ERR_NOMEM;
     s->tring_cap = cap;
     DC_CUDA(cudaMemsetAsync(s->tring, 0xFF, sizeof(unsigned long long) * cap, h->stream));
     return DC_OK;
@@ -1551,12 +1579,12 @@ int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
     if (int rc = scan_tmp64(h, V)) return rc;
     uint64_t total = (uint64_t)V + nlog;
     if (d.corner_cap < total) {
-        dfree(d.sky_k);
-        dfree(d.sky_l);
-        if (dmalloc(&d.sky_k, total) || dmalloc(&d.sky_l, total)) return DC_ERR_NOMEM;
+        dfree(h->stream, d.sky_k);
+        dfree(h->stream, d.sky_l);
+        if (dmalloc(h->stream, &d.sky_k, total) || dmalloc(h->stream, &d.sky_l, total)) return DC_ERR_NOMEM;
         d.corner_cap = total;
     }
-    if (!d.sky_off && dmalloc(&d.sky_off, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+    if (!d.sky_off && dmalloc(h->stream, &d.sky_off, (uint64_t)V + 1)) return DC_ERR_NOMEM;
     ++g_launches;
     k_sky_fill_row0<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt, s->row0, d.sky_k, d.sky_l, s->cursor);
     if (nlog)
@@ -1573,9 +1601,9 @@ int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
 static int ensure_rows(dc_graph* h, uint64_t elems) {
     Decomp& d = h->d;
     if (d.rows_cap >= elems && d.rows) return DC_OK;
-    dfree(d.rows);
+    dfree(h->stream, d.rows);
     d.rows_cap = 0;
-    if (dmalloc(&d.rows, elems)) return DC_ERR_NOMEM;
+    if (dmalloc(h->stream, &d.rows, elems)) return DC_ERR_NOMEM;
     d.rows_cap = elems;
     return DC_OK;
 }
@@ -1626,8 +1654,8 @@ static int sort_lists_by_kmax(dc_graph* h, int32_t K, int* sorted) {
             uint32_t*& tmp = side == 0 ? s->w_out_nbr : s->w_in_nbr;
             uint64_t& tcap = side == 0 ? s->w_out_cap : s->w_in_cap;
             if (tcap < cap || !tmp) {
-                dfree(tmp);
-                if (dmalloc(&tmp, cap)) return DC_ERR_NOMEM;
+                dfree(h->stream, tmp);
+                if (dmalloc(h->stream, &tmp, cap)) return DC_ERR_NOMEM;
                 tcap = cap;
             }
             int blocks = (int)std::min<unsigned>(hc[1], (unsigned)h->geom.sms * 2);
@@ -1654,8 +1682,8 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     *nlog_out = 0;
     cudaEventRecord(h->ev[2], h->stream);
     if (s->ck_cap < (uint32_t)K + 2) {
-        dfree(s->ck);
-        if (dmalloc(&s->ck, (uint64_t)K + 2)) return DC_ERR_NOMEM;
+        dfree(h->stream, s->ck);
+        if (dmalloc(h->stream, &s->ck, (uint64_t)K + 2)) return DC_ERR_NOMEM;
         s->ck_cap = K + 2;
     }
     uint32_t* hist = s->cursor;
@@ -1686,10 +1714,10 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     k_order_scatter<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist, s->order);
     uint64_t lc = bound + 1;
     if (s->log_cap < lc) {
-        dfree(s->log_v);
-        dfree(s->log_k);
-        dfree(s->log_l);
-        if (dmalloc(&s->log_v, lc) || dmalloc(&s->log_k, lc) || dmalloc(&s->log_l, lc)) return DC_ERR_NOMEM;
+        dfree(h->stream, s->log_v);
+        dfree(h->stream, s->log_k);
+        dfree(h->stream, s->log_l);
+        if (dmalloc(h->stream, &s->log_v, lc) || dmalloc(h->stream, &s->log_k, lc) || dmalloc(h->stream, &s->log_l, lc)) return DC_ERR_NOMEM;
         s->log_cap = lc;
     }
     // adjacency lists ordered by neighbour kmax (kept until the graph changes)
@@ -1750,12 +1778,12 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     d.rows_valid = false;
     if (int rc = ensure_scratch(h, V)) return rc;
     Scratch* s = h->scratch;
-    if (!d.kmax_v && dmalloc(&d.kmax_v, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+    if (!d.kmax_v && dmalloc(h->stream, &d.kmax_v, (uint64_t)V + 1)) return DC_ERR_NOMEM;
     if (V == 0) {
         d.kmax = 0;
         d.lmax = 0;
         d.n_corners = 0;
-        if (!d.sky_off && dmalloc(&d.sky_off, 1)) return DC_ERR_NOMEM;
+        if (!d.sky_off && dmalloc(h->stream, &d.sky_off, 1)) return DC_ERR_NOMEM;
         DC_CUDA(cudaMemsetAsync(d.sky_off, 0, sizeof(uint32_t), h->stream));
         d.valid = true;
         return DC_OK;
@@ -1771,7 +1799,7 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     const int32_t K = mv[0];
     d.kmax = K;
     d.lmax = mv[1];
-    if (!d.row0 && dmalloc(&d.row0, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+    if (!d.row0 && dmalloc(h->stream, &d.row0, (uint64_t)V + 1)) return DC_ERR_NOMEM;
     DC_CUDA(cudaMemcpyAsync(d.row0, s->row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
     if (method == 1) {
         // one fresh peel per row (the reference's schedule, main.cu:238-244),
@@ -1795,12 +1823,12 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
         DC_CUDA(cudaMemcpyAsync(&total, s->tmp64 + V, sizeof(total), cudaMemcpyDeviceToHost, h->stream));
         DC_CUDA(cudaStreamSynchronize(h->stream));
         if (d.corner_cap < total) {
-            dfree(d.sky_k);
-            dfree(d.sky_l);
-            if (dmalloc(&d.sky_k, total) || dmalloc(&d.sky_l, total)) return DC_ERR_NOMEM;
+            dfree(h->stream, d.sky_k);
+            dfree(h->stream, d.sky_l);
+            if (dmalloc(h->stream, &d.sky_k, total) || dmalloc(h->stream, &d.sky_l, total)) return DC_ERR_NOMEM;
             d.corner_cap = total;
         }
-        if (!d.sky_off && dmalloc(&d.sky_off, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+        if (!d.sky_off && dmalloc(h->stream, &d.sky_off, (uint64_t)V + 1)) return DC_ERR_NOMEM;
         ++g_launches;
         k_rows_corner_fill<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, d.rows, cnt, d.sky_k, d.sky_l,
                                                                         d.sky_off);

@@ -29,8 +29,6 @@ struct Scratch {
     uint64_t* tmp64 = nullptr;   // [V+1] scan scratch
     uint64_t* partial = nullptr; // [blocks] scan scratch
     uint32_t* cursor = nullptr;  // [V+1]
-    void* tmp_edges = nullptr;   // staging for uploaded edge arrays
-    uint64_t tmp_edges_bytes = 0;
     // second peel instance
     int32_t* key2 = nullptr;
     int32_t* cdeg2 = nullptr;
@@ -55,8 +53,10 @@ struct Scratch {
 int ensure_scratch(dc_graph* h, uint32_t V);
 void free_scratch(dc_graph* h);
 int init_handle(dc_graph* h);
-void free_graph_arrays(DevGraph& g);
-void free_decomp(Decomp& d);
+void free_graph_arrays(DevGraph& g, cudaStream_t st);
+void free_decomp(Decomp& d, cudaStream_t st);
+// Device bytes currently held by the handle (graph, decomposition, scratch).
+uint64_t device_footprint(const dc_graph* h);
 
 // Builds the slack CSR/CSC of h from device edge arrays (src, dst of length E).
 int build_from_device_edges(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_src, const uint32_t* d_dst);

@@ -22,6 +22,7 @@
 //   3. rows 1..R are recomputed row to row from the new row 0, where R bounds
 //      every row an updated edge or a changed kmax can reach; rows above R
 //      keep their skyline corners.
+#include <atomic>
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -33,7 +34,7 @@
 
 namespace dc {
 
-extern unsigned long long g_launches;
+extern std::atomic<unsigned long long> g_launches;
 
 #define MT_CUDA(call)                                                                        \
     do {                                                                                     \
@@ -46,11 +47,13 @@ extern unsigned long long g_launches;
 static constexpr int kMThreads = 256;
 static constexpr int kMWarps = kMThreads / 32;
 
+// Stream-ordered pool allocations on the handle's stream (no implicit
+// device-wide synchronisation between handles).
 template <typename T>
-static int mt_malloc(T** p, uint64_t n) {
+static int mt_malloc(cudaStream_t st, T** p, uint64_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
-    if (cudaMalloc((void**)p, n * sizeof(T)) != cudaSuccess) {
+    if (cudaMallocAsync((void**)p, n * sizeof(T), st) != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
         return set_error(DC_ERR_NOMEM, "device allocation of %llu bytes failed", (unsigned long long)(n * sizeof(T)));
@@ -58,8 +61,8 @@ static int mt_malloc(T** p, uint64_t n) {
     return DC_OK;
 }
 template <typename T>
-static void mt_free(T*& p) {
-    if (p) cudaFree((void*)p);
+static void mt_free(cudaStream_t st, T*& p) {
+    if (p) cudaFreeAsync((void*)p, st);
     p = nullptr;
 }
 
@@ -642,7 +645,7 @@ static int net_batch(uint32_t V, const uint32_t* pairs, const uint8_t* is_del, u
 
 template <typename T>
 static int upload(dc_graph* h, T** d, const std::vector<T>& hv) {
-    if (mt_malloc(d, hv.size())) return DC_ERR_NOMEM;
+    if (mt_malloc(h->stream, d, hv.size())) return DC_ERR_NOMEM;
     if (!hv.empty()) MT_CUDA(cudaMemcpyAsync(*d, hv.data(), sizeof(T) * hv.size(), cudaMemcpyHostToDevice, h->stream));
     return DC_OK;
 }
@@ -671,8 +674,8 @@ static int batch_features(dc_graph* h, const NetBatch& nb, float* f) {
     if (n) {
         uint32_t *du = nullptr, *dv = nullptr;
         if (upload(h, &du, u) || upload(h, &dv, v)) {
-            mt_free(du);
-            mt_free(dv);
+            mt_free(h->stream, du);
+            mt_free(h->stream, dv);
             return DC_ERR_NOMEM;
         }
         float* dacc = (float*)h->scratch->tmp64;
@@ -684,8 +687,8 @@ static int batch_features(dc_graph* h, const NetBatch& nb, float* f) {
         MT_CUDA(cudaMemcpyAsync(acc, dacc, 16, cudaMemcpyDeviceToHost, h->stream));
         MT_CUDA(cudaMemcpyAsync(iacc, diacc, 8, cudaMemcpyDeviceToHost, h->stream));
         MT_CUDA(cudaStreamSynchronize(h->stream));
-        mt_free(du);
-        mt_free(dv);
+        mt_free(h->stream, du);
+        mt_free(h->stream, dv);
     }
     const double nn = n ? (double)n : 1.0, K1 = d.kmax + 1.0, L1 = d.lmax + 1.0;
     f[0] = (float)std::log2(1.0 + nb.n_ins);
@@ -735,7 +738,7 @@ static int apply_deletions(dc_graph* h, const NetBatch& nb) {
     uint32_t *du = nullptr, *dv = nullptr;
     int32_t* dn = nullptr;
     if ((rc = upload(h, &du, nb.del_u)) || (rc = upload(h, &dv, nb.del_v)) || (rc = upload(h, &dn, nb.del_n))) {
-        mt_free(du); mt_free(dv); mt_free(dn);
+        mt_free(h->stream, du); mt_free(h->stream, dv); mt_free(h->stream, dn);
         return rc;
     }
     MT_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
@@ -744,9 +747,9 @@ static int apply_deletions(dc_graph* h, const NetBatch& nb) {
         (uint32_t)nb.del_u.size(), du, dv, dn, g.out_off, g.out_len, g.out_nbr, h->ctl);
     EngineCtl hc;
     rc = check_ctl(h, &hc, "dc_maintain: deletion check");
-    mt_free(du);
-    mt_free(dv);
-    mt_free(dn);
+    mt_free(h->stream, du);
+    mt_free(h->stream, dv);
+    mt_free(h->stream, dn);
     if (rc != DC_OK) {
         if (hc.error & DC_DEV_ERR_NOTFOUND)
             return set_error(DC_ERR_NOT_FOUND, "dc_maintain: a deleted edge is not in the graph (batch not applied)");
@@ -758,7 +761,7 @@ static int apply_deletions(dc_graph* h, const NetBatch& nb) {
         else group_by(nb.del_v, nb.del_u, nb.del_n, gvert, goff, gnbr);
         uint32_t *d_gv = nullptr, *d_go = nullptr, *d_gn = nullptr;
         if ((rc = upload(h, &d_gv, gvert)) || (rc = upload(h, &d_go, goff)) || (rc = upload(h, &d_gn, gnbr))) {
-            mt_free(d_gv); mt_free(d_go); mt_free(d_gn);
+            mt_free(h->stream, d_gv); mt_free(h->stream, d_go); mt_free(h->stream, d_gn);
             return rc;
         }
         ++g_launches;
@@ -766,9 +769,9 @@ static int apply_deletions(dc_graph* h, const NetBatch& nb) {
             (uint32_t)gvert.size(), d_gv, d_go, d_gn, side == 0 ? g.out_off : g.in_off,
             side == 0 ? g.out_len : g.in_len, side == 0 ? g.out_nbr : g.in_nbr, h->ctl);
         cudaError_t e = cudaStreamSynchronize(h->stream);
-        mt_free(d_gv);
-        mt_free(d_go);
-        mt_free(d_gn);
+        mt_free(h->stream, d_gv);
+        mt_free(h->stream, d_go);
+        mt_free(h->stream, d_gn);
         if (e != cudaSuccess) return set_error(DC_ERR_CUDA, "deletion apply: %s", cudaGetErrorString(e));
     }
     rc = check_ctl(h, &hc, "dc_maintain: deletion apply");
@@ -785,14 +788,14 @@ static int rebuild_store(dc_graph* h, const uint32_t* d_iu, const uint32_t* d_iv
     const uint32_t V = g.V;
     uint64_t E = g.E + n_ins;
     uint32_t *src = nullptr, *dst = nullptr;
-    if (mt_malloc(&src, E) || mt_malloc(&dst, E)) {
-        mt_free(src);
+    if (mt_malloc(h->stream, &src, E) || mt_malloc(h->stream, &dst, E)) {
+        mt_free(h->stream, src);
         return DC_ERR_NOMEM;
     }
     ++g_launches;
     k_len_to_u64<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, g.out_len, (unsigned long long*)s->tmp64);
     if (int rc = scan_tmp64(h, V)) {
-        mt_free(src); mt_free(dst);
+        mt_free(h->stream, src); mt_free(h->stream, dst);
         return rc;
     }
     ++g_launches;
@@ -808,10 +811,10 @@ static int rebuild_store(dc_graph* h, const uint32_t* d_iu, const uint32_t* d_iv
     h->gap_div = gd ? std::min<uint32_t>(gd, 8) : 8;
     int rc = build_from_device_edges(h, V, E, src, dst);
     cudaStreamSynchronize(h->stream);
-    free_decomp(h->d);
+    free_decomp(h->d, h->stream);
     h->d = keep;
-    mt_free(src);
-    mt_free(dst);
+    mt_free(h->stream, src);
+    mt_free(h->stream, dst);
     return rc;
 }
 
@@ -826,7 +829,7 @@ static int apply_insertions(dc_graph* h, const NetBatch& nb, uint32_t** d_iu_out
     uint32_t *iu = nullptr, *iv = nullptr;
     int rc = DC_OK;
     if ((rc = upload(h, &iu, nb.ins_u)) || (rc = upload(h, &iv, nb.ins_v))) {
-        mt_free(iu); mt_free(iv);
+        mt_free(h->stream, iu); mt_free(h->stream, iv);
         return rc;
     }
     const uint32_t n = (uint32_t)nb.ins_u.size();
@@ -851,7 +854,7 @@ static int apply_insertions(dc_graph* h, const NetBatch& nb, uint32_t** d_iu_out
         g.E += n;
     }
     if (rc != DC_OK) {
-        mt_free(iu); mt_free(iv);
+        mt_free(h->stream, iu); mt_free(h->stream, iv);
         return rc;
     }
     g.sorted_kmax = false;
@@ -927,7 +930,7 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
     st->method = method;
     cudaEvent_t* ev = h->ev;
     cudaEventRecord(ev[0], h->stream);
-    if (!s->kmax_old && (mt_malloc(&s->kmax_old, (uint64_t)V + 1) || mt_malloc(&s->row0_old, (uint64_t)V + 1)))
+    if (!s->kmax_old && (mt_malloc(h->stream, &s->kmax_old, (uint64_t)V + 1) || mt_malloc(h->stream, &s->row0_old, (uint64_t)V + 1)))
         return DC_ERR_NOMEM;
     // values before the batch (for the row bound) and row 0 in scratch
     MT_CUDA(cudaMemcpyAsync(s->kmax_old, d.kmax_v, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
@@ -1027,7 +1030,7 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
             }
             uint32_t* m_off = nullptr;
             int32_t *m_k = nullptr, *m_l = nullptr;
-            if (rc == DC_OK && (mt_malloc(&m_off, (uint64_t)V + 1) || mt_malloc(&m_k, total) || mt_malloc(&m_l, total))) {
+            if (rc == DC_OK && (mt_malloc(h->stream, &m_off, (uint64_t)V + 1) || mt_malloc(h->stream, &m_k, total) || mt_malloc(h->stream, &m_l, total))) {
                 rc = DC_ERR_NOMEM;
             }
             if (rc == DC_OK) {
@@ -1035,21 +1038,21 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
                 k_merge_fill<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, R, d.kmax_v, d.sky_off, d.sky_k, d.sky_l,
                                                                        o_off, o_k, o_l, cnt, m_k, m_l, m_off);
                 cudaStreamSynchronize(h->stream);
-                mt_free(d.sky_off);
-                mt_free(d.sky_k);
-                mt_free(d.sky_l);
+                mt_free(h->stream, d.sky_off);
+                mt_free(h->stream, d.sky_k);
+                mt_free(h->stream, d.sky_l);
                 d.sky_off = m_off;
                 d.sky_k = m_k;
                 d.sky_l = m_l;
                 d.corner_cap = total;
                 d.n_corners = total;
             } else {
-                mt_free(m_off); mt_free(m_k); mt_free(m_l);
+                mt_free(h->stream, m_off); mt_free(h->stream, m_k); mt_free(h->stream, m_l);
             }
         }
-        mt_free(o_off);
-        mt_free(o_k);
-        mt_free(o_l);
+        mt_free(h->stream, o_off);
+        mt_free(h->stream, o_k);
+        mt_free(h->stream, o_l);
         if (rc != DC_OK) {
             d.valid = false;
             goto out;
@@ -1088,10 +1091,10 @@ timing:
         h->maint_log.push_back(r);
     }
 out:
-    mt_free(d_du);
-    mt_free(d_dv);
-    mt_free(d_iu);
-    mt_free(d_iv);
+    mt_free(h->stream, d_du);
+    mt_free(h->stream, d_dv);
+    mt_free(h->stream, d_iu);
+    mt_free(h->stream, d_iv);
     if (rc != DC_OK) d.valid = false;
     return rc;
 }

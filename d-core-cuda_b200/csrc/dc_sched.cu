@@ -12,10 +12,12 @@
 // as bf16, products accumulated in fp32.  Training keeps fp32 master
 // weights, accumulates fp32 gradients and applies Adam; the bf16 copy used
 // by forward and backward is refreshed after every step.
+#include <atomic>
 #include <cuda_bf16.h>
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "dc_engine.cuh"
@@ -23,7 +25,7 @@
 
 namespace dc {
 
-extern unsigned long long g_launches;
+extern std::atomic<unsigned long long> g_launches;
 
 constexpr int kIn = 16, kH = 64, kOut = 2;
 constexpr int kOffW1 = 0;                   // [kH][kIn]
@@ -192,6 +194,7 @@ struct dc_sched {
     float* loss = nullptr;
     int step = 0;
     std::vector<float> feat_mean, feat_scale;  // input normalisation (identity by default)
+    std::mutex mu;  // graphs on several threads may share one scheduler
 };
 
 using namespace dc;
@@ -273,6 +276,7 @@ extern "C" int dc_sched_create(uint64_t seed, dc_sched** out) {
 
 extern "C" int dc_sched_set_params(dc_sched* s, const float* p) {
     if (!s || !p) return set_error(DC_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
     SC_CUDA(cudaMemcpyAsync(s->master, p, 4 * kNParams, cudaMemcpyHostToDevice, s->stream));
     ++g_launches;
     k_to_bf16<<<8, 256, 0, s->stream>>>(s->master, s->w);
@@ -282,6 +286,7 @@ extern "C" int dc_sched_set_params(dc_sched* s, const float* p) {
 
 extern "C" int dc_sched_get_params(dc_sched* s, float* p) {
     if (!s || !p) return set_error(DC_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
     SC_CUDA(cudaMemcpyAsync(p, s->master, 4 * kNParams, cudaMemcpyDeviceToHost, s->stream));
     SC_CUDA(cudaStreamSynchronize(s->stream));
     return DC_OK;
@@ -290,6 +295,7 @@ extern "C" int dc_sched_get_params(dc_sched* s, float* p) {
 // Input normalisation x' = (x - mean) * scale applied before the network.
 extern "C" int dc_sched_set_norm(dc_sched* s, const float* mean, const float* scale) {
     if (!s || !mean || !scale) return set_error(DC_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
     s->feat_mean.assign(mean, mean + kIn);
     s->feat_scale.assign(scale, scale + kIn);
     return DC_OK;
@@ -299,7 +305,7 @@ static int sched_upload(dc_sched* s, const float* X, uint64_t n, float** dX) {
     std::vector<float> xn((size_t)n * kIn);
     for (uint64_t i = 0; i < n; ++i)
         for (int j = 0; j < kIn; ++j) xn[i * kIn + j] = (X[i * kIn + j] - s->feat_mean[j]) * s->feat_scale[j];
-    if (cudaMalloc(dX, 4 * (n ? n : 1) * kIn) != cudaSuccess) {
+    if (cudaMallocAsync(dX, 4 * (n ? n : 1) * kIn, s->stream) != cudaSuccess) {
         cudaGetLastError();
         return set_error(DC_ERR_NOMEM, "scheduler input allocation failed");
     }
@@ -311,20 +317,21 @@ static int sched_upload(dc_sched* s, const float* X, uint64_t n, float** dX) {
 extern "C" int dc_sched_predict(dc_sched* s, const float* X, uint64_t n, float* Y) {
     if (!s || (n && (!X || !Y))) return set_error(DC_ERR_INVALID, "null argument");
     if (n == 0) return DC_OK;
+    std::lock_guard<std::mutex> lk(s->mu);
     float *dX = nullptr, *dY = nullptr;
     if (int rc = sched_upload(s, X, n, &dX)) return rc;
-    if (cudaMalloc(&dY, 4 * n * kOut) != cudaSuccess) {
+    if (cudaMallocAsync(&dY, 4 * n * kOut, s->stream) != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(dX);
+        cudaFreeAsync(dX, s->stream);
         return set_error(DC_ERR_NOMEM, "scheduler output allocation failed");
     }
     int blocks = (int)std::min<uint64_t>((n + 7) / 8, 1024);
     ++g_launches;
     k_mlp_forward<<<blocks, kSchedThreads, 0, s->stream>>>(dX, (uint32_t)n, s->w, dY);
     cudaError_t e = cudaMemcpyAsync(Y, dY, 4 * n * kOut, cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(dX, s->stream);
+    cudaFreeAsync(dY, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-    cudaFree(dX);
-    cudaFree(dY);
     if (e != cudaSuccess) return set_error(DC_ERR_CUDA, "dc_sched_predict: %s", cudaGetErrorString(e));
     return DC_OK;
 }
@@ -343,20 +350,24 @@ static int sched_grad_dev(dc_sched* s, const float* dX, const float* dT, const u
 }
 
 struct SchedBatch {
+    cudaStream_t st;
     float* X = nullptr;
     float* T = nullptr;
     uint8_t* M = nullptr;
     uint64_t n_on = 0;
+    explicit SchedBatch(cudaStream_t s) : st(s) {}
     ~SchedBatch() {
-        cudaFree(X);
-        cudaFree(T);
-        cudaFree(M);
+        if (X) cudaFreeAsync(X, st);
+        if (T) cudaFreeAsync(T, st);
+        if (M) cudaFreeAsync(M, st);
+        cudaStreamSynchronize(st);
     }
 };
 
 static int sched_batch(dc_sched* s, const float* X, const float* T, const uint8_t* M, uint64_t n, SchedBatch& b) {
     if (int rc = sched_upload(s, X, n, &b.X)) return rc;
-    if (cudaMalloc(&b.T, 4 * n * kOut) != cudaSuccess || cudaMalloc(&b.M, n * kOut) != cudaSuccess) {
+    if (cudaMallocAsync(&b.T, 4 * n * kOut, s->stream) != cudaSuccess ||
+        cudaMallocAsync(&b.M, n * kOut, s->stream) != cudaSuccess) {
         cudaGetLastError();
         return set_error(DC_ERR_NOMEM, "scheduler target allocation failed");
     }
@@ -369,7 +380,8 @@ static int sched_batch(dc_sched* s, const float* X, const float* T, const uint8_
 extern "C" int dc_sched_grad(dc_sched* s, const float* X, const float* T, const uint8_t* M, uint64_t n, float* grad,
                              float* loss) {
     if (!s || !X || !T || !M || !grad || n == 0) return set_error(DC_ERR_INVALID, "bad argument");
-    SchedBatch b;
+    std::lock_guard<std::mutex> lk(s->mu);
+    SchedBatch b(s->stream);
     if (int rc = sched_batch(s, X, T, M, n, b)) return rc;
     if (int rc = sched_grad_dev(s, b.X, b.T, b.M, n, b.n_on)) return rc;
     SC_CUDA(cudaMemcpyAsync(grad, s->g, 4 * kNParams, cudaMemcpyDeviceToHost, s->stream));
@@ -385,7 +397,8 @@ extern "C" int dc_sched_grad(dc_sched* s, const float* X, const float* T, const 
 extern "C" int dc_sched_train(dc_sched* s, const float* X, const float* T, const uint8_t* M, uint64_t n, int epochs,
                               float lr, float* final_loss) {
     if (!s || !X || !T || !M || n == 0 || epochs < 0) return set_error(DC_ERR_INVALID, "bad argument");
-    SchedBatch b;
+    std::lock_guard<std::mutex> lk(s->mu);
+    SchedBatch b(s->stream);
     if (int rc = sched_batch(s, X, T, M, n, b)) return rc;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     for (int ep = 0; ep < epochs; ++ep) {

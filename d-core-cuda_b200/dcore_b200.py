@@ -62,6 +62,14 @@ class MaintStats(ctypes.Structure):
 
 MAINT_AUTO, MAINT_LOCAL, MAINT_REPEEL = 0, 1, 2
 
+
+class ServerInfo(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_uint64), ("used_bytes", ctypes.c_uint64), ("peak_bytes", ctypes.c_uint64),
+                ("admissions", ctypes.c_uint64), ("evictions", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("measured_bytes", ctypes.c_uint64),
+                ("graphs", ctypes.c_uint32),
+                ("resident", ctypes.c_uint32)]
+
 # name -> argtypes; every function returns int status unless listed in _VOID / _STR
 SIGNATURES = {
     "dc_gen_er": [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p, u32p],
@@ -119,6 +127,16 @@ SIGNATURES = {
     "dc_maint_log_enable": [vp, ctypes.c_int],
     "dc_maint_log_get": [vp, ctypes.POINTER(ctypes.c_float), i32p, ctypes.POINTER(ctypes.c_float), ctypes.c_uint64,
                          u64p],
+    "dc_graph_device_bytes": [vp, u64p],
+    "dc_server_create": [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)],
+    "dc_server_add_graph": [vp, ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, u32p],
+    "dc_server_submit": [vp, ctypes.c_uint32, u32p, u8p, ctypes.c_uint64, u64p],
+    "dc_server_drain": [vp, ctypes.c_uint64],
+    "dc_server_completions": [vp, u64p, u32p, ctypes.POINTER(ctypes.c_double), u32p, u64p, i32p, ctypes.c_uint64,
+                              u64p],
+    "dc_server_info_get": [vp, ctypes.POINTER(ServerInfo)],
+    "dc_server_graph_result": [vp, ctypes.c_uint32, i32p, i32p, ctypes.c_uint64, i32p],
+    "dc_server_free": [vp],
     "dc_kmax_noalloc": [ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp, vp, i32p, vp],
     "dc_launch_count": [u64p],
     "dc_last_error": [],
@@ -377,6 +395,11 @@ class Graph:
         _check(lib().dc_graph_write_binary(self._h, path.encode(), gap))
 
     # ---- decomposition
+    def device_bytes(self):
+        n = ctypes.c_uint64(0)
+        _check(lib().dc_graph_device_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
     def decompose(self, method=METHOD_INCREMENTAL):
         km = ctypes.c_int32(0)
         lm = ctypes.c_int32(0)
@@ -550,6 +573,90 @@ class Scheduler:
         _check(lib().dc_sched_train(self._h, _p(X, f32p), _p(T, f32p), _p(M, u8p), len(X), epochs, lr,
                                     ctypes.byref(loss)))
         return loss.value
+
+
+class Server:
+    """Serving loop over many device-resident graphs (dc_server_*): requests
+    are queued per graph, coalesced into one maintenance batch per graph when
+    a worker picks it, and run on per-graph streams under an HBM budget."""
+
+    def __init__(self, hbm_budget_bytes, max_concurrent=4, method=MAINT_AUTO, device=0):
+        h = vp()
+        _check(lib().dc_server_create(int(hbm_budget_bytes), max_concurrent, method, device, ctypes.byref(h)))
+        self._h = h
+
+    def free(self):
+        if getattr(self, "_h", None):
+            lib().dc_server_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    def add_graph(self, V, src, dst):
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        gid = ctypes.c_uint32(0)
+        _check(lib().dc_server_add_graph(self._h, V, len(src), _p(src, u32p), _p(dst, u32p), ctypes.byref(gid)))
+        return gid.value
+
+    def submit(self, graph_id, src, dst, is_delete=None):
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        pairs = np.empty(2 * len(src), np.uint32)
+        pairs[0::2] = src
+        pairs[1::2] = dst
+        dl = None if is_delete is None else np.ascontiguousarray(is_delete, np.uint8)
+        rid = ctypes.c_uint64(0)
+        _check(lib().dc_server_submit(self._h, graph_id, _p(pairs, u32p), None if dl is None else _p(dl, u8p),
+                                      len(src), ctypes.byref(rid)))
+        return rid.value
+
+    def drain(self, timeout_ms=600000):
+        _check(lib().dc_server_drain(self._h, timeout_ms))
+
+    def completions(self):
+        """Completed requests since the last call as a dict of arrays."""
+        n = ctypes.c_uint64(0)
+        _check(lib().dc_server_completions(self._h, None, None, None, None, None, None, 0, ctypes.byref(n)))
+        m = n.value
+        out = {"id": np.zeros(m, np.uint64), "graph": np.zeros(m, np.uint32), "latency_ms": np.zeros(m, np.float64),
+               "batch_requests": np.zeros(m, np.uint32), "batch_updates": np.zeros(m, np.uint64),
+               "status": np.zeros(m, np.int32)}
+        if m:
+            _check(lib().dc_server_completions(
+                self._h, _p(out["id"], u64p), _p(out["graph"], u32p),
+                out["latency_ms"].ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _p(out["batch_requests"], u32p),
+                _p(out["batch_updates"], u64p), _p(out["status"], i32p), m, ctypes.byref(n)))
+            for k in out:
+                out[k] = out[k][:n.value]
+        return out
+
+    def info(self):
+        st = ServerInfo()
+        _check(lib().dc_server_info_get(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerInfo._fields_}
+
+    def result(self, graph_id, V, rows=True):
+        """(kmaxes, rows or None) of a graph after all its queued requests."""
+        km = np.zeros(V, np.int32)
+        kmax = ctypes.c_int32(0)
+        _check(lib().dc_server_graph_result(self._h, graph_id, _p(km, i32p), None, 0, ctypes.byref(kmax)))
+        if not rows:
+            return km, None
+        R = np.zeros((kmax.value + 1) * V, np.int32)
+        _check(lib().dc_server_graph_result(self._h, graph_id, _p(km, i32p), _p(R, i32p), R.size,
+                                            ctypes.byref(kmax)))
+        return km, R.reshape(kmax.value + 1, V)
 
 
 def exported_symbols():

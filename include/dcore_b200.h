@@ -137,6 +137,10 @@ int dc_graph_degrees(dc_graph* g, int32_t* in_deg, int32_t* out_deg);
 int dc_graph_get_edges(dc_graph* g, uint32_t* src, uint32_t* dst, uint64_t capacity, uint64_t* n_edges);
 /* Graph::writeBinary of the current device graph. */
 int dc_graph_write_binary(dc_graph* g, const char* path, uint32_t gap);
+/* Device bytes the handle holds now (adjacency with slack, decomposition,
+ * engine scratch).  No counterpart in the reference; the serving loop charges
+ * it against its HBM budget. */
+int dc_graph_device_bytes(const dc_graph* g, uint64_t* bytes);
 
 /* ---- decomposition ------------------------------------------------------- */
 
@@ -263,6 +267,54 @@ int dc_kmax_edge_batches(uint32_t V, const int32_t* kmaxes, uint64_t B, const ui
  * capture on that device.  stream is a cudaStream_t (NULL: default stream). */
 int dc_kmax_noalloc(uint32_t V, uint64_t E, const uint32_t* d_in_off, const uint32_t* d_out_off,
                     const uint32_t* d_out_nbr, int32_t* d_kmax, int32_t* kmax_max, void* stream);
+
+/* ---- serving loop ------------------------------------------------------ */
+/* Many device-resident graphs, each receiving a stream of edge-update
+ * requests.  No counterpart in the reference (its driver, main.cu:1784-2218,
+ * loads one graph and runs one operation).  max_concurrent worker threads each
+ * take the graph with the oldest pending request, coalesce ALL of that
+ * graph's pending requests into one dc_maintain batch (continuous batching;
+ * the result equals applying them one by one in submission order) and run it
+ * on the graph's own stream, so batches of different graphs overlap on the
+ * GPU.  A graph is built and decomposed on the device when first needed; the
+ * each resident graph is charged an upper bound of its device footprint
+ * (maintenance transients included, room for E/8 more edges), and the
+ * charges are kept within hbm_budget_bytes by evicting the least recently
+ * used idle graph (its edges move to host memory; it is rebuilt on its next
+ * request).  A graph larger than the whole budget is admitted alone; a batch
+ * that outgrows its charge while every other resident graph is busy runs
+ * over budget.  Reading rows back (dc_server_graph_result) stages up to
+ * 2 x min(256 MB, rows) outside the budget.  method: DC_MAINT_*. */
+typedef struct dc_server dc_server;
+typedef struct dc_server_info {
+    uint64_t budget_bytes, used_bytes, peak_bytes;
+    uint64_t admissions, evictions, batches, submitted, completed;
+    uint64_t measured_bytes; /* dc_graph_device_bytes summed over resident graphs */
+    uint32_t graphs, resident;
+} dc_server_info;
+int dc_server_create(uint64_t hbm_budget_bytes, int max_concurrent, int method, int device, dc_server** out);
+/* Registers a graph (copied to host memory; built on the device on demand). */
+int dc_server_add_graph(dc_server* s, uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst,
+                        uint32_t* graph_id);
+/* Queues b updates (pairs[2i], pairs[2i+1]; is_delete may be NULL = all
+ * inserts); returns at once.  *request_id numbers requests from 1. */
+int dc_server_submit(dc_server* s, uint32_t graph_id, const uint32_t* pairs, const uint8_t* is_delete, uint64_t b,
+                     uint64_t* request_id);
+/* Waits until every submitted request has completed (DC_ERR_TIMEOUT after
+ * timeout_ms). */
+int dc_server_drain(dc_server* s, uint64_t timeout_ms);
+/* Completed requests since the last call, in completion order: id, graph,
+ * latency (submission to end of its batch), requests and updates in its
+ * batch, status.  With ids NULL only *n (the number waiting) is reported. */
+int dc_server_completions(dc_server* s, uint64_t* ids, uint32_t* graphs, double* latency_ms,
+                          uint32_t* batch_requests, uint64_t* batch_updates, int32_t* status, uint64_t capacity,
+                          uint64_t* n);
+int dc_server_info_get(dc_server* s, dc_server_info* info);
+/* Decomposition of one graph after all its queued requests: kmax[V] and,
+ * when rows is not NULL, dense rows 0..kmax (rows_capacity >= (kmax+1)*V). */
+int dc_server_graph_result(dc_server* s, uint32_t graph_id, int32_t* kmaxes, int32_t* rows, uint64_t rows_capacity,
+                           int32_t* kmax);
+int dc_server_free(dc_server* s);
 
 /* ---- diagnostics ------------------------------------------------------- */
 /* Per-step timing of the persistent kernels: after each kernel, fn is called

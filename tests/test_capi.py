@@ -78,3 +78,11 @@ def test_no_device_fails_loudly(dc):
     with pytest.raises(dc.DCoreError) as e:
         dc.Graph.from_edges(3, np.array([0, 1], np.uint32), np.array([1, 2], np.uint32))
     assert e.value.code == -9
+
+
+def test_server_without_device_fails_loudly(dc):
+    if dc.device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(dc.DCoreError) as e:
+        dc.Server(1 << 30)
+    assert e.value.code == -9
