@@ -51,7 +51,20 @@ WORKLOADS = {
     "maint-rmat22": dict(gen="rmat", scale=22, ef=16, seed=1, ops=1_000_000, maint=True,
                          sizes=[(1, 20), (100, 20), (10_000, 20), (1_000_000, 1)],
                          desc="R-MAT scale 22, edge factor 16 + 1e6-op update stream (50% insert / 50% delete)"),
+    # serving loop: 64 device-resident graphs, open-loop Poisson arrivals
+    "serve-64": dict(serve=True, n_graphs=64, scales=(16, 22), efs=(8, 32), seed=1, budget_gb=150.0,
+                     rate=100.0, requests=1000, sat_rate=2000.0, sat_requests=4000, max_request=10_000,
+                     insert_frac=0.6, workers=4,
+                     desc="64 R-MAT graphs, scale U{16..22}, edge factor U{8..32}; Poisson arrivals of requests "
+                          "of log-uniform 1..1e4 updates (60% insert / 40% delete) on uniformly chosen graphs; "
+                          "150 GB HBM admission budget; continuous batching"),
+    # learned scheduler against the rule of thumb on R-MAT 23
+    "sched-rmat23": dict(sched=True, scale=23, ef=16, seed=1, train_scales=(20, 21, 22, 23), train_batches=40,
+                         train_max=65_536, eval_batches=60, eval_max=1_000_000, hot_frac=0.1,
+                         desc="R-MAT scale 23, edge factor 16; batches of log-uniform 1..1e6 updates "
+                              "(50% insert / 50% delete), 10% of batches on the top-1% out-degree vertices"),
 }
+METRIC_SERVE = "updates/s serving loop"
 METRIC_MAINT = "updates/s batched D-core maintenance"
 METRIC = "edges/s full D-core decomposition"
 
@@ -132,6 +145,24 @@ def kernel_traffic(kernel, workload):
     return d.get(workload, {}).get(kernel)
 
 
+def decomposition_bytes(V, s, d, kmaxes):
+    """Algorithmic bytes of a full decomposition as a per-row peel moves them
+    (the reference's dcore(), main.cu:197-262): the kmax pass B_K = 12 E + 16 V
+    (out-adjacency ids, in-degree read-modify-write, offsets, degree init,
+    result and state) and per row k B_k = 8 D_k + 16 I_k + 24 V_k + 4 (V - V_k)
+    with V_k = |{v : kmax(v) >= k}|, D_k = total degree of those vertices,
+    I_k = edges with both endpoints among them (ids + neighbour-kmax filter,
+    two 4+4 B degree updates per internal edge, per-core-vertex offsets,
+    degrees, state and result, zero rows for the rest)."""
+    K = int(kmaxes.max()) if len(kmaxes) else 0
+    deg = np.bincount(s, minlength=V) + np.bincount(d, minlength=V)
+    rev = lambda a: np.cumsum(a[::-1])[::-1]
+    Vk = rev(np.bincount(kmaxes, minlength=K + 1).astype(np.float64))
+    Dk = rev(np.bincount(kmaxes, weights=deg, minlength=K + 1))
+    Ik = rev(np.bincount(np.minimum(kmaxes[s], kmaxes[d]), minlength=K + 1).astype(np.float64))
+    return {"B_K": 12.0 * len(s) + 16.0 * V, "B_row": 8 * Dk + 16 * Ik + 24 * Vk + 4 * (V - Vk)}
+
+
 def cpu_baseline(w, V, s, d, budget_s=20.0):
     """Oracle port on the host cores: kmax pass plus a stratified sample of
     rows, extrapolated to the full decomposition."""
@@ -162,6 +193,9 @@ def run_reference(args, w, rank, world):
     if rank != 0:
         return
     import dcore_b200 as dc
+    if w.get("serve") or w.get("sched"):
+        run_reference_recompute(args, w, dc)
+        return
     V, s, d = make_graph(dc, w, 0)
     vals = []
     base = None
@@ -185,6 +219,52 @@ def run_reference(args, w, rank, world):
             "config": {"workload": args.workload, "graph": w["desc"], "V": V, "E": int(len(s))},
             "cpu_baseline": dict(base, value=value),
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_recompute(args, w, dc):
+    """CPU path for the serving and scheduler workloads: the reference keeps a
+    decomposition current by recomputing it (checkDCore, main.cu:264-293), so
+    every batch costs one decomposition of its graph on the host cores."""
+    rng = np.random.default_rng(w["seed"] + 31)
+    vals, base = [], None
+    if w.get("serve"):
+        scales, efs, phases = serve_plan(w, 0, args.requests, args.rate)
+        t_arr, gid, size, _ = phases[1]
+        nominal = (2.0 ** scales) * efs
+        mid = int(np.argsort(nominal)[len(nominal) // 2])
+        V, s, d = dc.gen_rmat(int(scales[mid]), int(efs[mid]), w["seed"] * 1000 + mid)
+        dedup = len(s) / nominal[mid]
+        for i in range(args.warmup + args.steps):
+            b = cpu_baseline(w, V, s, d, budget_s=args.cpu_seconds)
+            if i >= args.warmup:
+                vals.append(b["value"])
+                base = b
+        rate = float(np.mean(vals))
+        seconds = float(np.sum(nominal[gid] * dedup / rate))  # one recomputation per request
+        value = float(size.sum()) / seconds
+        metric = METRIC_SERVE
+        sample = (base["sample"] + f"; measured on graph {mid} (scale {scales[mid]}, edge factor {efs[mid]}), "
+                  f"every request costs one recomputation of its graph at that edges/s")
+        config = {"workload": args.workload, "graphs": w["desc"], "requests": int(len(t_arr))}
+    else:
+        V, s, d = dc.gen_rmat(w["scale"], w["ef"], w["seed"])
+        for i in range(args.warmup + args.steps):
+            b = cpu_baseline(w, V, s, d, budget_s=args.cpu_seconds)
+            if i >= args.warmup:
+                vals.append(b["value"])
+                base = b
+        rate = float(np.mean(vals))
+        ev_sizes = _log_uniform(np.random.default_rng(w["seed"] + 77), w["eval_batches"], w["eval_max"])
+        value = float(ev_sizes.mean()) * rate / len(s)
+        metric = METRIC_MAINT
+        sample = base["sample"] + "; every batch costs one recomputation of the graph"
+        config = {"workload": args.workload, "graph": w["desc"], "V": V, "E": int(len(s))}
+    line = {"metric": metric, "value": value, "unit": "updates/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic", "impl": "reference", "config": config,
+            "cpu_baseline": dict(base, value=value, unit="updates/s", sample=sample),
+            "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -235,6 +315,274 @@ def run_maintenance(args, w, rank, world, local):
     g.free()
 
 
+def _final_edges(s, d, u, v, dl):
+    """Edge list after a valid update stream (multiplicities 0/1)."""
+    keys = np.concatenate([(s.astype(np.uint64) << 32) | d, (u.astype(np.uint64) << 32) | v])
+    w = np.concatenate([np.ones(len(s), np.int64), np.where(dl == 1, -1, 1).astype(np.int64)])
+    uk, inv = np.unique(keys, return_inverse=True)
+    cnt = np.zeros(len(uk), np.int64)
+    np.add.at(cnt, inv, w)
+    fk = uk[cnt > 0]
+    return (fk >> 32).astype(np.uint32), (fk & 0xFFFFFFFF).astype(np.uint32)
+
+
+def _log_uniform(rng, n, hi):
+    return np.minimum(hi, np.exp(rng.uniform(0, np.log(hi), n)).astype(np.int64) + 1)
+
+
+def serve_plan(w, rank, requests=None, rate=None):
+    """Graph sizes and the two request phases: (arrival times, graph, size)
+    at the latency rate, then at the saturation rate."""
+    rng = np.random.default_rng(w["seed"] * 7919 + rank)
+    n = w["n_graphs"]
+    scales = rng.integers(w["scales"][0], w["scales"][1] + 1, n)
+    efs = rng.integers(w["efs"][0], w["efs"][1] + 1, n)
+    phases = []
+    for R, lam in ((requests or w["requests"], rate or w["rate"]), (w["sat_requests"], w["sat_rate"])):
+        t_arr = np.cumsum(rng.exponential(1.0 / lam, R))
+        gid = rng.integers(0, n, R)
+        size = _log_uniform(rng, R, w["max_request"])
+        phases.append((t_arr, gid, size, lam))
+    return scales, efs, phases
+
+
+def _serve_phase(dc, srv, graphs, ids, pos, t_arr, gid, size, local):
+    info0 = srv.info()
+    launches0 = dc.launch_count()
+    sampler = ClockSampler(local)
+    sampler.start()
+    t0 = time.perf_counter()
+    for r in range(len(t_arr)):
+        delay = t0 + t_arr[r] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        g, k, p = int(gid[r]), int(size[r]), int(pos[gid[r]])
+        _, _, _, u, v, dl = graphs[g]
+        srv.submit(ids[g], u[p:p + k], v[p:p + k], dl[p:p + k])
+        pos[g] = p + k
+    srv.drain()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    comp = srv.completions()
+    info = srv.info()
+    if (comp["status"] != 0).any():
+        raise RuntimeError(f"{int((comp['status'] != 0).sum())} requests failed")
+    lat = comp["latency_ms"]
+    nb = int(info["batches"] - info0["batches"])
+    return {"requests": int(len(t_arr)), "updates": int(size.sum()), "wall_s": wall,
+            "updates_per_s": float(size.sum()) / wall, "offered_updates_per_s": float(size.sum()) / float(t_arr[-1]),
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
+                           "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "batches": nb, "mean_requests_per_batch": len(t_arr) / max(1, nb),
+            "gpu_launches": int(dc.launch_count() - launches0), "clocks": clocks}
+
+
+def run_serve(args, w, rank, world, local):
+    """Serving loop over many device-resident graphs.  Requests arrive
+    open-loop at Poisson times in two phases: below capacity (latency:
+    submission to the end of the batch holding the request, p50/p99) and at
+    saturation (throughput: updates of all requests / (last completion - first
+    submission)).  A sample of graphs is checked afterwards against a fresh
+    decomposition of its final edge set."""
+    from concurrent.futures import ThreadPoolExecutor
+    import torch
+    import dcore_b200 as dc
+    torch.cuda.set_device(local)
+    scales, efs, phases = serve_plan(w, rank, args.requests, args.rate)
+    n = w["n_graphs"]
+    need = sum(np.bincount(gid, weights=size, minlength=n) for _, gid, size, _ in phases).astype(np.int64)
+
+    def gen(i):
+        V, s, d = dc.gen_rmat(int(scales[i]), int(efs[i]), w["seed"] * 1000 + 17 * rank + i)
+        u, v, dl = dc.gen_updates(V, s, d, int(need[i]), w["insert_frac"], w["seed"] * 1000 + 500 + i)
+        return V, s, d, u, v, dl
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max(1, min(16, os.cpu_count() or 1))) as ex:
+        graphs = list(ex.map(gen, range(n)))
+    t_gen = time.perf_counter() - t0
+    E_tot = int(sum(len(g[1]) for g in graphs))
+    workers = args.workers or w["workers"]
+    srv = dc.Server(int(w["budget_gb"] * 1e9), max_concurrent=workers, method=args.maint_method, device=local)
+    ids = [srv.add_graph(g[0], g[1], g[2]) for g in graphs]
+    t0 = time.perf_counter()
+    for i in ids:  # admit and decompose every graph before the timed phases
+        srv.result(i, graphs[i][0], rows=False)
+    t_admit = time.perf_counter() - t0
+    pos = np.zeros(n, np.int64)
+    lat_phase = _serve_phase(dc, srv, graphs, ids, pos, *phases[0][:3], local)
+    sat_phase = _serve_phase(dc, srv, graphs, ids, pos, *phases[1][:3], local)
+    info = srv.info()
+    # exactness on a sample: the three smallest graphs and the largest one of
+    # scale <= 19 (dense rows of the largest graphs run to tens of GB)
+    order = np.argsort([len(g[1]) for g in graphs])
+    mid = [int(i) for i in order if scales[i] <= 19][-1:]
+    checked = []
+    for i in list(order[:3]) + mid:
+        V, s, d, u, v, dl = graphs[i]
+        km, rows = srv.result(ids[i], V)
+        fs, fd = _final_edges(s, d, u, v, dl)
+        with dc.Graph.from_edges(V, fs, fd, device=local) as g:
+            g.decompose()
+            if not (np.array_equal(g.kmaxes(), km) and np.array_equal(g.rows(), rows)):
+                raise RuntimeError(f"graph {i}: served result differs from a fresh decomposition")
+        checked.append(int(i))
+    srv.free()
+    value = sat_phase["updates_per_s"]
+    clocks = sat_phase.pop("clocks")
+    lat_clocks = lat_phase.pop("clocks")
+    line = {"metric": METRIC_SERVE, "value": value, "unit": "updates/s", "n_gpus": world,
+            "steps": sat_phase["requests"], "warmup": 0, "ms_per_step": lat_phase["latency_ms"]["p50"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "graphs": w["desc"], "n_graphs": n, "E_total": E_tot,
+                       "scales": scales.tolist(), "edge_factors": efs.tolist(), "workers": workers,
+                       "budget_gb": w["budget_gb"], "method": {0: "scheduler", 1: "local", 2: "re-peel"}[
+                           args.maint_method],
+                       "gen_s": t_gen, "admit_s": t_admit, "exact_checked_graphs": checked,
+                       "step": "one request (submission to completion)",
+                       "value": "updates/s of the saturation phase; ms_per_step = p50 latency below capacity"},
+            "latency_phase": dict(lat_phase, offered_req_s=phases[0][3], clocks=lat_clocks),
+            "saturation_phase": dict(sat_phase, offered_req_s=phases[1][3]),
+            "hbm": {"peak_charged_gb": info["peak_bytes"] / 1e9, "measured_resident_gb": info["measured_bytes"] / 1e9,
+                    "resident": info["resident"], "evictions": info["evictions"]},
+            "e2e": {"value": value, "unit": "updates/s",
+                    "h2d_bytes_per_step": float(9 * sat_phase["updates"] / sat_phase["requests"]),
+                    "d2h_bytes_per_step": 0,
+                    "timing": "wall clock through dc_server_submit/drain with host request buffers"},
+            "gpu_launches": sat_phase["gpu_launches"], "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _same_decomposition(a, b, chunk=32):
+    """kmaxes and every dense row equal, compared a chunk of rows at a time."""
+    ka, kb = a.decomp_info()["kmax"], b.decomp_info()["kmax"]
+    if ka != kb or not np.array_equal(a.kmaxes(), b.kmaxes()):
+        return False
+    for k0 in range(0, ka + 1, chunk):
+        n = min(chunk, ka + 1 - k0)
+        if not np.array_equal(a.rows(k0, n), b.rows(k0, n)):
+            return False
+    return True
+
+
+def _stream_times(dc, g, u, v, dl, sizes, method):
+    pos, ms, methods = 0, [], []
+    for bs in sizes:
+        st = g.maintain(u[pos:pos + bs], v[pos:pos + bs], dl[pos:pos + bs], method)
+        ms.append(st["total_ms"])
+        methods.append(st["method"])
+        pos += bs
+    return np.array(ms), np.array(methods)
+
+
+def _hot_stream(dc, V, s, d, sizes, hot_frac, rng, seed):
+    od = np.bincount(s, minlength=V)
+    hot = np.argsort(-od, kind="stable")[:max(1, V // 100)].astype(np.uint32)
+    hot_batch = rng.uniform(size=len(sizes)) < hot_frac
+    op_hot = np.repeat(hot_batch.astype(np.uint8), sizes)
+    u, v, dl = dc.gen_updates_hot(V, s, d, int(np.sum(sizes)), 0.5, seed, hot, op_hot)
+    return u, v, dl, hot_batch
+
+
+def run_sched(args, w, rank, world, local):
+    """Learned scheduler against the rule of thumb.  Training: a fresh R-MAT
+    graph, a log-uniform batch stream (10% hot) applied to two copies, one
+    per method, logging features and device times; the network learns
+    log(time - row recompute) of each method.  Evaluation: a fresh R-MAT 23
+    graph and stream applied to two copies, one with the network attached,
+    one with the rule of thumb; both must end equal to a fresh
+    decomposition of the final edge set."""
+    import torch
+    import dcore_b200 as dc
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(w["seed"] + 31 * rank)
+    # ---- training log: fresh graphs of several sizes (the graph-size
+    # features must vary), each stream applied to one copy per method
+    Xs, Ts = [], []
+    t0 = time.perf_counter()
+    for j, scale in enumerate(w["train_scales"]):
+        V, s, d = dc.gen_rmat(scale, w["ef"], w["seed"] + 100 + 10 * j + rank)
+        tr_sizes = _log_uniform(rng, w["train_batches"], w["train_max"])
+        u, v, dl, _ = _hot_stream(dc, V, s, d, tr_sizes, w["hot_frac"], rng, w["seed"] + 200 + j)
+        logs = []
+        for method in (dc.MAINT_LOCAL, dc.MAINT_REPEEL):
+            with dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16) as g:
+                g.decompose()
+                g.maint_log(True)
+                _stream_times(dc, g, u, v, dl, tr_sizes, method)
+                logs.append(g.maint_log())
+        (X, _, ta), (_, _, tb) = logs
+        Xs.append(X)
+        Ts.append(np.log(np.stack([ta[:, 0] - ta[:, 2], tb[:, 0] - tb[:, 2]], 1).clip(1e-3) + 1e-2))
+    X = np.concatenate(Xs).astype(np.float32)
+    T = np.concatenate(Ts).astype(np.float32)
+    sched = dc.Scheduler(seed=w["seed"])
+    sched.set_norm(X.mean(0), 1.0 / (X.std(0) + 1e-3))
+    loss = sched.train(X, T, np.ones_like(T, np.uint8), epochs=800, lr=3e-3)
+    t_train = time.perf_counter() - t0
+    # ---- evaluation stream on R-MAT 23
+    V, s, d = dc.gen_rmat(w["scale"], w["ef"], w["seed"] + rank)
+    ev_sizes = _log_uniform(np.random.default_rng(w["seed"] + 77), w["eval_batches"], w["eval_max"])
+    u, v, dl, hot_batch = _hot_stream(dc, V, s, d, ev_sizes, w["hot_frac"], rng, w["seed"] + 300)
+    res = {}
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = dc.launch_count()
+    for name, sch in (("learned", sched), ("rule", None)):
+        g = dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16)
+        g.decompose()
+        g.set_scheduler(sch)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ms, methods = _stream_times(dc, g, u, v, dl, ev_sizes, dc.MAINT_AUTO)
+        wall = time.perf_counter() - t0
+        res[name] = {"wall_s": wall, "device_ms": float(ms.sum()), "ms": ms, "methods": methods, "graph": g}
+    launches = dc.launch_count() - launches0
+    clocks = sampler.stop()
+    fs, fd = _final_edges(s, d, u, v, dl)
+    with dc.Graph.from_edges(V, fs, fd, device=local) as fresh:
+        fresh.decompose()
+        for name in res:
+            if not _same_decomposition(res[name]["graph"], fresh):
+                raise RuntimeError(f"{name}: maintained result differs from a fresh decomposition")
+            res[name]["graph"].free()
+    L, Rr = res["learned"], res["rule"]
+    updates = int(ev_sizes.sum())
+    value = updates / L["wall_s"]
+    diff = L["methods"] != Rr["methods"]
+    line = {"metric": METRIC_MAINT, "value": value, "unit": "updates/s", "n_gpus": world,
+            "steps": int(len(ev_sizes)), "warmup": 1, "ms_per_step": float(np.median(L["ms"])),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "graph": w["desc"], "V": V, "E": int(len(s)),
+                       "updates": updates, "hot_batches": int(hot_batch.sum()),
+                       "train": {"graphs": f"R-MAT scales {list(w['train_scales'])}, edge factor {w['ef']}, "
+                                           "fresh seeds",
+                                 "batches": int(w["train_batches"]) * len(w["train_scales"]),
+                                 "max_batch": w["train_max"],
+                                 "final_loss": float(loss), "seconds": t_train},
+                       "exactness": "both runs end with kmaxes and every row equal to a fresh "
+                                    "decomposition of the final graph"},
+            "scheduler": {"learned_wall_s": L["wall_s"], "rule_wall_s": Rr["wall_s"],
+                          "gain_wall": Rr["wall_s"] / L["wall_s"],
+                          "learned_device_ms": L["device_ms"], "rule_device_ms": Rr["device_ms"],
+                          "gain_device": Rr["device_ms"] / L["device_ms"],
+                          "batches_decided_differently": int(diff.sum()),
+                          "ms_on_differing_batches": {"learned": float(L["ms"][diff].sum()),
+                                                      "rule": float(Rr["ms"][diff].sum())},
+                          "learned_methods": {"local": int((L["methods"] == 1).sum()),
+                                              "repeel": int((L["methods"] == 2).sum())},
+                          "rule_methods": {"local": int((Rr["methods"] == 1).sum()),
+                                           "repeel": int((Rr["methods"] == 2).sum())}},
+            "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": float(9 * updates / len(ev_sizes)),
+                    "d2h_bytes_per_step": 0, "timing": "wall clock of dc_maintain calls with host batches"},
+            "gpu_launches": int(launches), "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -246,6 +594,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--maint-method", type=int, default=0, help="0 scheduler, 1 local, 2 re-peel")
+    ap.add_argument("--requests", type=int, default=0, help="serve: number of requests (0: workload default)")
+    ap.add_argument("--rate", type=float, default=0.0, help="serve: arrivals per second (0: workload default)")
+    ap.add_argument("--workers", type=int, default=0, help="serve: worker threads (0: workload default)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -257,6 +608,12 @@ def main():
         return
     if w.get("maint"):
         run_maintenance(args, w, rank, world, local)
+        return
+    if w.get("serve"):
+        run_serve(args, w, rank, world, local)
+        return
+    if w.get("sched"):
+        run_sched(args, w, rank, world, local)
         return
 
     import torch
@@ -313,23 +670,30 @@ def main():
     value = world * E / (ms_per_step / 1000.0)
     K = infos[-1]["kmax"]
 
-    # ---- roofline of the dominant kernel (engine counters, CUDA events)
+    # ---- roofline of the dominant kernel (CUDA events on the engine stream)
     peak, peak_kind = peaks()
     inf = infos[-1]
     peel_ms = float(np.mean([i["kmax_ms"] for i in infos]))
     rows_ms = float(np.mean([i["rows_ms"] for i in infos]))
+    model = decomposition_bytes(V, s, d, g.kmaxes())
     kernels = {
-        # fused kmax + row-0 peel: per pass 12 B per edge (id + two-sided
-        # degree update) + 16 B per vertex, two passes
-        "k_peel2": {"ms": peel_ms, "bytes": 2 * (12.0 * E + 16.0 * V)},
-        # row-to-row refinement: 8 B per adjacency entry read (id + neighbour
-        # value) + 16 B per evaluation (value, two counters, queue state)
-        "k_trans2": {"ms": rows_ms, "bytes": 8.0 * inf.get("entries", 0) + 16.0 * inf["evals"]},
+        # fused kmax + row 0 peel
+        "k_peel2": {"ms": peel_ms, "bytes": model["B_K"] + model["B_row"][0]},
+        # rows 1..kmax
+        "k_trans2": {"ms": rows_ms, "bytes": float(np.sum(model["B_row"][1:]))},
     }
     dom = max(kernels, key=lambda k: kernels[k]["ms"])
     ach = kernels[dom]["bytes"] / (kernels[dom]["ms"] / 1000.0) / 1e9
+    b_alg = model["B_K"] + float(np.sum(model["B_row"]))
+    touched = 8.0 * inf.get("entries", 0) + 16.0 * inf["evals"]
     roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
             "peak_source": peak_kind, "traffic": kernel_traffic(dom, args.workload),
+            "model": "per-row peel bytes: B_K = 12E + 16V; B_k = 8 D_k + 16 I_k + 24 V_k + 4 (V - V_k)",
+            "decomposition": {"alg_bytes": b_alg, "ms": ms_per_step,
+                              "achieved_gbs": b_alg / (ms_per_step / 1000.0) / 1e9,
+                              "frac": b_alg / (ms_per_step / 1000.0) / 1e9 / peak},
+            "engine_touched_bytes": {"k_trans2": touched,
+                                     "gbs": touched / (rows_ms / 1000.0) / 1e9 if rows_ms else None},
             "kernels": {k: {"ms": v["ms"], "alg_bytes": v["bytes"],
                             "achieved_gbs": v["bytes"] / (v["ms"] / 1000.0) / 1e9 if v["ms"] else None}
                         for k, v in kernels.items()}}

@@ -196,8 +196,23 @@ extern "C" int dc_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, doubl
 // to a host copy of the edge set, so it is valid in sequence.
 extern "C" int dc_gen_updates(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, uint64_t n_ops,
                               double insert_frac, uint64_t seed, uint32_t* out_u, uint32_t* out_v, uint8_t* out_del) {
+    return dc_gen_updates_hot(V, E, src, dst, n_ops, insert_frac, seed, nullptr, 0, nullptr, out_u, out_v, out_del);
+}
+
+extern "C" int dc_gen_updates_hot(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, uint64_t n_ops,
+                                  double insert_frac, uint64_t seed, const uint32_t* hot, uint32_t n_hot,
+                                  const uint8_t* op_hot, uint32_t* out_u, uint32_t* out_v, uint8_t* out_del) {
     if (V < 2) return dc::set_error(DC_ERR_INVALID, "dc_gen_updates: need V >= 2");
     if (n_ops && (!out_u || !out_v || !out_del)) return dc::set_error(DC_ERR_INVALID, "dc_gen_updates: null output");
+    if (op_hot && (!hot || n_hot == 0)) return dc::set_error(DC_ERR_INVALID, "dc_gen_updates_hot: empty hot set");
+    std::vector<uint8_t> is_hot;
+    if (op_hot) {
+        is_hot.assign(V, 0);
+        for (uint32_t i = 0; i < n_hot; ++i) {
+            if (hot[i] >= V) return dc::set_error(DC_ERR_INVALID, "dc_gen_updates_hot: hot id out of range");
+            is_hot[hot[i]] = 1;
+        }
+    }
     std::vector<uint64_t> keys(E);
     for (uint64_t e = 0; e < E; ++e) {
         if (src[e] >= V || dst[e] >= V) return dc::set_error(DC_ERR_INVALID, "dc_gen_updates: id out of range");
@@ -225,9 +240,13 @@ extern "C" int dc_gen_updates(uint32_t V, uint64_t E, const uint32_t* src, const
         uint64_t live = E - n_gone + added.size();
         bool ins = rng.next() <= thr || live == 0;
         if (ins && live >= (uint64_t)V * (V - 1)) ins = false;
+        // a hot operation has its source among the hot vertices: inserts
+        // draw it from them, deletes reject present edges from other sources
+        // (up to 4096 draws, then any present edge)
+        const bool hot_op = op_hot && op_hot[i];
         if (ins) {
             for (;;) {
-                uint32_t u = rng.bounded(V), v = rng.bounded(V);
+                uint32_t u = hot_op ? hot[rng.bounded(n_hot)] : rng.bounded(V), v = rng.bounded(V);
                 if (u == v) continue;
                 uint64_t k = ((uint64_t)u << 32) | v;
                 int64_t orig;
@@ -245,9 +264,13 @@ extern "C" int dc_gen_updates(uint32_t V, uint64_t E, const uint32_t* src, const
                 break;
             }
         } else {
-            for (;;) {
+            for (int tries = 0;; ++tries) {
                 uint64_t r = rng.bounded64(E + added.size());
                 uint64_t k;
+                if (hot_op && tries < 4096) {
+                    uint64_t kk = r < E ? keys[r] : added[r - E];
+                    if (!is_hot[(uint32_t)(kk >> 32)]) continue;
+                }
                 if (r < E) {
                     if (gone[r]) continue;
                     gone[r] = 1;

@@ -655,6 +655,8 @@ int sched_choose(dc_sched* s, const float* feat);
 // Rule of thumb (the scheduler's fallback): the local update of kmax and
 // row 0 grows with the batch (its bound on how far a value can rise is the
 // number of inserted edges), the fused peel is a fixed pass over the graph.
+static constexpr uint64_t kSchedLocalMax = 1ull << 16;
+
 int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del) {
     (void)h;
     return (n_ins + n_del <= 64) ? DC_MAINT_LOCAL : DC_MAINT_REPEEL;
@@ -924,7 +926,10 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
     if (want_feat)
         if (int rc = batch_features(h, nb, feat)) return rc;
     if (method == DC_MAINT_AUTO) {
-        int m = h->sched ? sched_choose(h->sched, feat) : -1;
+        // the network decides where both methods are practical; past
+        // kSchedLocalMax net updates the local update's region covers most
+        // of the graph and the fused re-peel is taken without asking
+        int m = h->sched && nb.n_ins + nb.n_del <= kSchedLocalMax ? sched_choose(h->sched, feat) : -1;
         method = m > 0 ? m : choose_method(h, nb.n_ins, nb.n_del);
     }
     st->method = method;

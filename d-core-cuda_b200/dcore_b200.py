@@ -78,6 +78,8 @@ SIGNATURES = {
     "dc_kmax_edge_batches": [ctypes.c_uint32, i32p, ctypes.c_uint64, u32p, u32p, i64p, i64p],
     "dc_gen_updates": [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_uint64, ctypes.c_double,
                        ctypes.c_uint64, u32p, u32p, u8p],
+    "dc_gen_updates_hot": [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_uint64, ctypes.c_double,
+                           ctypes.c_uint64, u32p, ctypes.c_uint32, u8p, u32p, u32p, u8p],
     "dc_text_read_edges": [ctypes.c_char_p, ctypes.c_int, u32p, u64p, u32p, u32p, ctypes.c_uint64],
     "dc_binary_read_edges": [ctypes.c_char_p, u32p, u64p, u32p, u32p, ctypes.c_uint64],
     "dc_binary_write_edges": [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_uint32],
@@ -241,6 +243,23 @@ def gen_updates(V, src, dst, n_ops, insert_frac, seed):
     dl = np.empty(max(n_ops, 1), np.uint8)
     _check(lib().dc_gen_updates(V, len(src), _p(src, u32p), _p(dst, u32p), n_ops, insert_frac, seed, _p(u, u32p),
                                 _p(v, u32p), _p(dl, u8p)))
+    return u[:n_ops], v[:n_ops], dl[:n_ops]
+
+
+def gen_updates_hot(V, src, dst, n_ops, insert_frac, seed, hot, op_hot):
+    """gen_updates where operations marked in op_hot have their source among
+    the vertices `hot`."""
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    hot = np.ascontiguousarray(hot, np.uint32)
+    op_hot = np.ascontiguousarray(op_hot, np.uint8)
+    assert len(op_hot) == n_ops
+    u = np.empty(max(n_ops, 1), np.uint32)
+    v = np.empty(max(n_ops, 1), np.uint32)
+    dl = np.empty(max(n_ops, 1), np.uint8)
+    _check(lib().dc_gen_updates_hot(V, len(src), _p(src, u32p), _p(dst, u32p), n_ops, insert_frac, seed,
+                                    _p(hot, u32p), len(hot), _p(op_hot, u8p), _p(u, u32p), _p(v, u32p),
+                                    _p(dl, u8p)))
     return u[:n_ops], v[:n_ops], dl[:n_ops]
 
 

@@ -70,6 +70,13 @@ int dc_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double
  * Replaces getRandomInsertEdge / getRandomDeleteEdge (src/graph.cpp:327-380). */
 int dc_gen_updates(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, uint64_t n_ops,
                    double insert_frac, uint64_t seed, uint32_t* out_u, uint32_t* out_v, uint8_t* out_del);
+/* dc_gen_updates with hot operations: where op_hot[i] = 1, operation i has
+ * its source among hot[0..n_hot) (an insertion draws the source from them,
+ * a deletion picks a present edge leaving one of them).  Used for streams
+ * whose batches concentrate on the highest out-degree vertices. */
+int dc_gen_updates_hot(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, uint64_t n_ops,
+                       double insert_frac, uint64_t seed, const uint32_t* hot, uint32_t n_hot, const uint8_t* op_hot,
+                       uint32_t* out_u, uint32_t* out_v, uint8_t* out_del);
 
 /* ---- file formats (host only, no GPU needed) ---------------------------- */
 
@@ -213,8 +220,10 @@ int dc_maintain(dc_graph* g, const uint32_t* pairs, const uint8_t* is_delete, ui
 /* A BF16 MLP (16 -> 64 -> 64 -> 2, ReLU) predicting the log of the wall time
  * of DC_MAINT_LOCAL (output 0) and DC_MAINT_REPEEL (output 1) from 16
  * features of a batch (dc_maint_log_get lists them); DC_MAINT_AUTO runs the
- * method with the smaller prediction, the rule of thumb when no network is
- * attached.  Either method gives exact results.  Training and inference run
+ * method with the smaller prediction for batches of at most 65,536 net
+ * updates (larger ones always re-peel), the rule of thumb (at most 64 net
+ * updates: local) when no network is attached.  Either method gives exact
+ * results.  Training and inference run
  * in the engine's own CUDA kernels.  No reference counterpart (the reference
  * fixes its batching mode at compile time, src/common.h:18-19). */
 typedef struct dc_sched dc_sched;

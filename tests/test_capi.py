@@ -86,3 +86,44 @@ def test_server_without_device_fails_loudly(dc):
     with pytest.raises(dc.DCoreError) as e:
         dc.Server(1 << 30)
     assert e.value.code == -9
+
+
+def _replay(s, d, u, v, dl):
+    live = set(zip(s.tolist(), d.tolist()))
+    for a, b, x in zip(u.tolist(), v.tolist(), dl.tolist()):
+        assert a != b
+        if x:
+            assert (a, b) in live
+            live.remove((a, b))
+        else:
+            assert (a, b) not in live
+            live.add((a, b))
+    return live
+
+
+@pytest.mark.parametrize("frac", [0.0, 0.5, 0.6, 1.0])
+def test_update_stream_valid_in_sequence(dc, frac):
+    V, s, d = dc.gen_rmat(10, 4, 2)
+    u, v, dl = dc.gen_updates(V, s, d, 3000, frac, 7)
+    _replay(s, d, u, v, dl)
+    if 0 < frac < 1:
+        assert abs(1 - dl.mean() - frac) < 0.05
+    u2, v2, dl2 = dc.gen_updates(V, s, d, 3000, frac, 7)
+    assert np.array_equal(u, u2) and np.array_equal(v, v2) and np.array_equal(dl, dl2)
+
+
+def test_hot_update_stream(dc):
+    V, s, d = dc.gen_rmat(12, 8, 3)
+    od = np.bincount(s, minlength=V)
+    hot = np.argsort(-od, kind="stable")[:V // 100].astype(np.uint32)
+    n = 4000
+    op_hot = np.zeros(n, np.uint8)
+    op_hot[1000:1400] = 1
+    op_hot[3000:3100] = 1
+    u, v, dl = dc.gen_updates_hot(V, s, d, n, 0.6, 11, hot, op_hot)
+    _replay(s, d, u, v, dl)
+    assert np.isin(u[op_hot == 1], hot).all()
+    assert np.isin(u[op_hot == 0], hot).mean() < 0.5
+    # without hot operations it is the plain stream
+    u0, v0, dl0 = dc.gen_updates(V, s, d, 1000, 0.6, 11)
+    assert np.array_equal(u0, u[:1000]) and np.array_equal(dl0, dl[:1000])
