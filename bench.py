@@ -42,6 +42,8 @@ WORKLOADS = {
                           desc="R-MAT scale 22, edge factor 16, a=.57 b=.19 c=.19, dedup, permuted"),
     "decomp-rmat20": dict(gen="rmat", scale=20, ef=16, seed=1,
                           desc="R-MAT scale 20, edge factor 16, a=.57 b=.19 c=.19, dedup, permuted"),
+    "decomp-rmat19": dict(gen="rmat", scale=19, ef=16, seed=1,
+                          desc="R-MAT scale 19, edge factor 16, a=.57 b=.19 c=.19, dedup, permuted"),
     "decomp-er10k": dict(gen="er", n=10_000, m=100_000, seed=1, desc="directed G(n=10000, m=100000)"),
     # maintenance: R-MAT graph + stream of 50% inserts of absent edges and 50%
     # deletes of present edges, valid in sequence, in several batch sizes
@@ -143,6 +145,24 @@ def kernel_traffic(kernel, workload):
         return None
     d = json.load(open(p))
     return d.get(workload, {}).get(kernel)
+
+
+def reference_gpu(V, s, d, g):
+    """The reference's own GPU dcore() on the same graph (oracle/_ref), timed
+    around the call as the reference times it (host clock, its allocation,
+    uploads, per-row degree resets and per-row result copies included), and
+    its result compared with the engine's."""
+    from oracle import ref_gpu
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref/ref_dcore not built (reference sources absent at build time)"}
+    if V >= ref_gpu.MAX_V:
+        return {"unavailable": f"V = {V} >= 1,000,000: the reference's unchecked per-block peel buffers "
+                               "(1,000,000 entries, src/cuda_utils.cuh:10-13) can overflow; not run"}
+    kmax, lmax, kmaxes, rows, ms = ref_gpu.dcore(V, s, d)
+    same = (kmax == g.decomp_info()["kmax"] and np.array_equal(kmaxes, g.kmaxes())
+            and np.array_equal(rows, g.rows()))
+    return {"ms": ms, "edges_per_s": len(s) / (ms / 1000.0), "same_result": bool(same),
+            "timing": "host clock around dcore(), as main.cu:249-254 reports it"}
 
 
 def decomposition_bytes(V, s, d, kmaxes):
@@ -732,6 +752,7 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w, V, s, d, budget_s=args.cpu_seconds)
+    ref = reference_gpu(V, s, d, g) if rank == 0 else None
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
@@ -745,7 +766,7 @@ def main():
                 "phases_ms": {"peel": peel_ms, "rows": rows_ms,
                               "other": ms_per_step - peel_ms - rows_ms},
                 "gpu_launches": int(launches), "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
-                "clocks": clocks}
+                "reference_gpu": ref, "clocks": clocks}
         print(json.dumps(line), flush=True)
     g.free()
     if dist:
