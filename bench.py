@@ -475,6 +475,88 @@ def run_serve(args, w, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_row_sharded(args, w, rank, world, local, dist):
+    """Row sharding of ONE decomposition (strong scaling): every rank holds the
+    same graph, computes kmax and row 0, derives the same row ranges from
+    dc_row_weights and computes its range straight from row 0, writing its
+    dense rows into its own HBM (no exchange).  With --emulate-ranks N on one
+    GPU the N ranges run one after another on the device, each rank's time
+    being the shared kmax/row-0/weights time plus its own range; ranks never
+    wait on one another, so the maximum is what N GPUs would take."""
+    import torch
+    import dcore_b200 as dc
+    import dcore_dist
+    nranks = args.emulate_ranks if args.emulate_ranks > 1 else world
+    V, s, d = make_graph(dc, w, 0)  # the same graph on every rank
+    E = int(len(s))
+    g = dc.Graph.from_edges(V, s, d, device=local)
+    stream = torch.cuda.ExternalStream(g.stream())
+    bufs = {}
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    def step(ranks):
+        e0 = ev()
+        g.decompose_rows(0, 0)  # kmax + row 0, recomputed
+        wts = g.row_weights()
+        e1 = ev()
+        shards = dcore_dist.row_shards(wts, nranks)
+        per = {}
+        for r in ranks:
+            a0, b0 = shards[r]
+            t0 = ev()
+            if a0 <= b0:
+                g.decompose_rows(a0, b0)
+                n = b0 - a0 + 1
+                if r not in bufs or bufs[r].numel() < n * V:
+                    bufs[r] = torch.empty(n * V, dtype=torch.int32, device=f"cuda:{local}")
+                g.rows_to_device(a0, n, bufs[r].data_ptr())
+            t1 = ev()
+            per[r] = (t0, t1)
+        t_end = ev()
+        t_end.synchronize()
+        shared = e0.elapsed_time(e1)
+        return shared, {r: a.elapsed_time(b) for r, (a, b) in per.items()}, shards
+
+    ranks = list(range(nranks)) if args.emulate_ranks > 1 else [rank]
+    for _ in range(args.warmup):
+        step(ranks)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = dc.launch_count()
+    step_ms, shared_ms, range_ms = [], [], {r: [] for r in ranks}
+    for _ in range(args.steps):
+        sh, per, shards = step(ranks)
+        shared_ms.append(sh)
+        for r in ranks:
+            range_ms[r].append(per[r])
+        step_ms.append(sh + max(per.values()))
+    launches = dc.launch_count() - launches0
+    clocks = sampler.stop()
+    mine = float(np.mean(step_ms))
+    ms = dcore_dist.max_over_ranks(mine, dist, device=f"cuda:{local}")
+    if rank == 0:
+        line = {"metric": METRIC, "value": E / (ms / 1000.0), "unit": "edges/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                "config": {"workload": args.workload, "graph": w["desc"], "V": V, "E": E,
+                           "parallelism": f"row shards x{nranks}" + (" (emulated on one GPU)"
+                                                                     if args.emulate_ranks > 1 else ""),
+                           "output": "dense rows of each range in its rank's HBM",
+                           "shards": [list(map(int, x)) for x in shards]},
+                "per_rank_ms": {"kmax_row0_weights": float(np.mean(shared_ms)),
+                                "ranges": {str(r): float(np.mean(v)) for r, v in range_ms.items()}},
+                "gpu_launches": int(launches), "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    g.free()
+
+
 def _same_decomposition(a, b, chunk=32):
     """kmaxes and every dense row equal, compared a chunk of rows at a time."""
     ka, kb = a.decomp_info()["kmax"], b.decomp_info()["kmax"]
@@ -617,6 +699,10 @@ def main():
     ap.add_argument("--requests", type=int, default=0, help="serve: number of requests (0: workload default)")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: arrivals per second (0: workload default)")
     ap.add_argument("--workers", type=int, default=0, help="serve: worker threads (0: workload default)")
+    ap.add_argument("--shard", choices=["replicas", "rows"], default="replicas",
+                    help="decomposition with N > 1: one graph per rank, or the rows of one graph split over ranks")
+    ap.add_argument("--emulate-ranks", type=int, default=0,
+                    help="row sharding of one decomposition over N ranks, run one range after another on one GPU")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -643,6 +729,12 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.shard == "rows" or args.emulate_ranks > 1:
+        run_row_sharded(args, w, rank, world, local, dist)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     V, s, d = make_graph(dc, w, rank)
     E = int(len(s))

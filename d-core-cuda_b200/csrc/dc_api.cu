@@ -276,6 +276,26 @@ extern "C" int dc_decompose(dc_graph* h, int method, int32_t* kmax, int32_t* lma
     return DC_OK;
 }
 
+extern "C" int dc_decompose_rows(dc_graph* h, uint32_t k_first, uint32_t k_last, int32_t* kmax, int32_t* lmax) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    API_CUDA(cudaSetDevice(h->device));
+    const int32_t k0 = (int32_t)std::min<uint32_t>(k_first, 0x7FFFFFFF);
+    const int32_t k1 = (int32_t)std::min<uint32_t>(k_last, 0x7FFFFFFF);
+    if (int rc = decompose_range(h, k0, k1)) return rc;
+    if (kmax) *kmax = h->d.kmax;
+    if (lmax) *lmax = h->d.lmax;
+    return DC_OK;
+}
+
+extern "C" int dc_row_weights(dc_graph* h, uint64_t* weights, uint64_t capacity) {
+    if (!h || !weights) return set_error(DC_ERR_INVALID, "null argument");
+    if (!h->d.peel_valid) return set_error(DC_ERR_STATE, "no kmax on this graph (dc_decompose_rows first)");
+    if (capacity < (uint64_t)h->d.kmax + 1)
+        return set_error(DC_ERR_CAPACITY, "dc_row_weights: need kmax + 1 = %d values", h->d.kmax + 1);
+    API_CUDA(cudaSetDevice(h->device));
+    return row_weights(h, weights);
+}
+
 extern "C" int dc_maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_delete, uint64_t b, int method,
                            dc_maint_stats* stats) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");
@@ -346,6 +366,9 @@ extern "C" int dc_get_lmax_rows_device(dc_graph* h, uint32_t k0, uint32_t n, int
     if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
     if ((uint64_t)k0 + n > (uint64_t)h->d.kmax + 1)
         return set_error(DC_ERR_INVALID, "rows [%u, %llu) outside 0..kmax=%d", k0, (unsigned long long)k0 + n, h->d.kmax);
+    if (!h->d.holds(k0, n))
+        return set_error(DC_ERR_STATE, "rows [%u, %llu) not held: the decomposition holds row 0 and rows %d..%d",
+                         k0, (unsigned long long)k0 + n, h->d.row_lo, h->d.row_hi);
     if (h->d.rows_valid) {
         if (n)
             API_CUDA(cudaMemcpyAsync(d_out, h->d.rows + (uint64_t)k0 * h->g.V, 4ull * n * h->g.V,
@@ -361,6 +384,9 @@ extern "C" int dc_get_lmax_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* o
     if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
     if ((uint64_t)k0 + n > (uint64_t)h->d.kmax + 1)
         return set_error(DC_ERR_INVALID, "rows [%u, %llu) outside 0..kmax=%d", k0, (unsigned long long)k0 + n, h->d.kmax);
+    if (!h->d.holds(k0, n))
+        return set_error(DC_ERR_STATE, "rows [%u, %llu) not held: the decomposition holds row 0 and rows %d..%d",
+                         k0, (unsigned long long)k0 + n, h->d.row_lo, h->d.row_hi);
     const uint64_t V = h->g.V;
     if (n == 0 || V == 0) return DC_OK;
     if (h->d.rows_valid) {
@@ -396,6 +422,9 @@ extern "C" int dc_get_lmax_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* o
 extern "C" int dc_materialize_rows(dc_graph* h) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");
     if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    if (!h->d.full())
+        return set_error(DC_ERR_STATE, "the decomposition holds row 0 and rows %d..%d only (dc_decompose_rows)",
+                         h->d.row_lo, h->d.row_hi);
     if (h->d.rows_valid) return DC_OK;
     uint64_t elems = (uint64_t)(h->d.kmax + 1) * h->g.V;
     if (h->d.rows_cap < elems) {
@@ -429,6 +458,9 @@ extern "C" int dc_get_skyline(dc_graph* h, uint32_t* off, int32_t* ks, int32_t* 
                               uint64_t* n_corners) {
     if (!h || !n_corners) return set_error(DC_ERR_INVALID, "null argument");
     if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    if (!h->d.full())
+        return set_error(DC_ERR_STATE, "the decomposition holds row 0 and rows %d..%d only (dc_decompose_rows)",
+                         h->d.row_lo, h->d.row_hi);
     *n_corners = h->d.n_corners;
     if (!off || !ks || !ls) return DC_OK;
     if (capacity < h->d.n_corners) return set_error(DC_ERR_CAPACITY, "dc_get_skyline: capacity too small");
@@ -446,6 +478,9 @@ extern "C" int dc_get_skyline(dc_graph* h, uint32_t* off, int32_t* ks, int32_t* 
 extern "C" int dc_write_decomp(dc_graph* h, const char* path) {
     if (!h || !path) return set_error(DC_ERR_INVALID, "null argument");
     if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    if (!h->d.full())
+        return set_error(DC_ERR_STATE, "the decomposition holds row 0 and rows %d..%d only (dc_decompose_rows)",
+                         h->d.row_lo, h->d.row_hi);
     const uint64_t V = h->g.V;
     std::vector<int32_t> km(V ? V : 1), rows((uint64_t)(h->d.kmax + 1) * V + 1);
     if (int rc = dc_get_kmaxes(h, km.data())) return rc;
@@ -457,6 +492,9 @@ extern "C" int dc_write_decomp(dc_graph* h, const char* path) {
 extern "C" int dc_write_decomp_cpu(dc_graph* h, const char* path) {
     if (!h || !path) return set_error(DC_ERR_INVALID, "null argument");
     if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    if (!h->d.full())
+        return set_error(DC_ERR_STATE, "the decomposition holds row 0 and rows %d..%d only (dc_decompose_rows)",
+                         h->d.row_lo, h->d.row_hi);
     const uint64_t V = h->g.V;
     std::vector<int32_t> km(V ? V : 1), rows((uint64_t)(h->d.kmax + 1) * V + 1);
     if (int rc = dc_get_kmaxes(h, km.data())) return rc;

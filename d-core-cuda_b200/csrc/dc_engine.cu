@@ -460,6 +460,7 @@ struct Trans2Params {
     uint32_t* in_nbr;
     const int32_t* kmax;
     int32_t K;
+    int32_t K0;     // first row to compute; cur holds row 0 (K0 > 1 jumps straight to row K0)
     int32_t Kstop;  // last row to compute (rows above stay untouched)
     int sorted;     // lists ordered by neighbour kmax, descending
     const uint32_t* order;
@@ -481,10 +482,11 @@ struct Trans2Params {
 struct TransHook {
     unsigned nworkers;
     int K;
+    int K0;
     __device__ void operator()(EngineCtl* c) const {
         // next row: after a row that needed no work, jump to the first row
         // whose leaving set or seed set can be non-empty (next_min)
-        if (c->step < 0) c->level = 1;
+        if (c->step < 0) c->level = K0;
         else if (c->t_tail == c->trace_tail0) c->level = max(c->level + 1, c->next_min);
         else c->level = c->level + 1;
         c->next_min = K + 1;
@@ -624,7 +626,7 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
     __shared__ int s_hi[kWarpsPerBlock][kWin];
     int* ho = s_ho[wib];
     int* hi_ = s_hi[wib];
-    TransHook hook{gridDim.x, p.Kstop};
+    TransHook hook{gridDim.x, p.Kstop, p.K0};
     unsigned long long my_evals = 0, my_drops = 0, my_entries = 0;
     unsigned ticket = kNoTicket;
     __shared__ unsigned s_prod;
@@ -1003,6 +1005,26 @@ __global__ void k_sort_big(const uint32_t* off, const int32_t* len, uint32_t* nb
 __global__ void k_kmax_hist(uint32_t V, const int32_t* kmax, uint32_t* hist) {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
         atomicAdd(&hist[kmax[v]], 1u);
+}
+
+// w[k] += in + out degree of every vertex with kmax == k (shared-memory
+// bins when the range fits, else global atomics)
+__global__ void k_kmax_degree_hist(uint32_t V, const int32_t* kmax, const int32_t* in_len, const int32_t* out_len,
+                                   int32_t K, unsigned long long* w) {
+    extern __shared__ unsigned long long sw[];
+    const bool shared = K + 1 <= 4096;
+    if (shared)
+        for (int i = threadIdx.x; i <= K; i += blockDim.x) sw[i] = 0;
+    __syncthreads();
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        unsigned long long dgr = (unsigned long long)(in_len[v] + out_len[v]);
+        if (shared) atomicAdd(&sw[kmax[v]], dgr);
+        else atomicAdd(&w[kmax[v]], dgr);
+    }
+    __syncthreads();
+    if (shared)
+        for (int i = threadIdx.x; i <= K; i += blockDim.x)
+            if (sw[i]) atomicAdd(&w[i], sw[i]);
 }
 
 // cursor[k] = first position of bucket k in descending-kmax order
@@ -1674,7 +1696,7 @@ static int sort_lists_by_kmax(dc_graph* h, int32_t K, int* sorted) {
 // row-to-row kernel.  Corners of rows 1..Kstop are left in the scratch log
 // (*nlog entries).  allow_sort: order adjacency lists by neighbour kmax
 // first (otherwise lists are read whole).
-int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out) {
+int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out, int32_t K0) {
     DevGraph& g = h->g;
     Decomp& d = h->d;
     Scratch* s = h->scratch;
@@ -1737,6 +1759,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     tp.in_off = g.in_off; tp.in_len = g.in_len; tp.in_nbr = g.in_nbr;
     tp.kmax = d.kmax_v;
     tp.K = K;
+    tp.K0 = std::max(1, K0);
     tp.Kstop = Kstop;
     tp.sorted = sorted;
     tp.order = s->order;
@@ -1756,7 +1779,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     tp.ctl = h->ctl;
     uint64_t nlog = 0;
     cudaEventRecord(h->ev[3], h->stream);
-    if (Kstop >= 1) {
+    if (Kstop >= tp.K0) {
         void* args[] = {&tp};
         EngineCtl hc;
         if (int rc = run_persistent(h, (const void*)k_trans2, args, "transitions", &hc)) return rc;
@@ -1779,12 +1802,16 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     if (int rc = ensure_scratch(h, V)) return rc;
     Scratch* s = h->scratch;
     if (!d.kmax_v && dmalloc(h->stream, &d.kmax_v, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+    d.peel_valid = false;
     if (V == 0) {
         d.kmax = 0;
         d.lmax = 0;
         d.n_corners = 0;
         if (!d.sky_off && dmalloc(h->stream, &d.sky_off, 1)) return DC_ERR_NOMEM;
         DC_CUDA(cudaMemsetAsync(d.sky_off, 0, sizeof(uint32_t), h->stream));
+        d.row_lo = 1;
+        d.row_hi = 0;
+        d.peel_valid = true;
         d.valid = true;
         return DC_OK;
     }
@@ -1801,6 +1828,9 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     d.lmax = mv[1];
     if (!d.row0 && dmalloc(h->stream, &d.row0, (uint64_t)V + 1)) return DC_ERR_NOMEM;
     DC_CUDA(cudaMemcpyAsync(d.row0, s->row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+    d.peel_valid = true;
+    d.row_lo = 1;
+    d.row_hi = K;
     if (method == 1) {
         // one fresh peel per row (the reference's schedule, main.cu:238-244),
         // two rows per launch
@@ -1876,5 +1906,84 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     h->times.expand_ms = ms;
     return DC_OK;
 }
+
+int row_weights(dc_graph* h, uint64_t* out) {
+    const DevGraph& g = h->g;
+    const Decomp& d = h->d;
+    const int32_t K = d.kmax;
+    unsigned long long* w = nullptr;
+    if (dmalloc(h->stream, &w, (uint64_t)K + 1)) return DC_ERR_NOMEM;
+    DC_CUDA(cudaMemsetAsync(w, 0, 8ull * (K + 1), h->stream));
+    if (g.V) {
+        ++g_launches;
+        size_t shm = K + 1 <= 4096 ? 8ull * (K + 1) : 0;
+        k_kmax_degree_hist<<<grid_for(h, g.V), kThreads, shm, h->stream>>>(g.V, d.kmax_v, g.in_len, g.out_len, K, w);
+    }
+    std::vector<uint64_t> hw((size_t)K + 1);
+    DC_CUDA(cudaMemcpyAsync(hw.data(), w, 8ull * (K + 1), cudaMemcpyDeviceToHost, h->stream));
+    dfree(h->stream, w);
+    DC_CUDA(cudaStreamSynchronize(h->stream));
+    uint64_t run = 0;
+    for (int32_t k = K; k >= 0; --k) {
+        run += hw[k];
+        out[k] = run;
+    }
+    return DC_OK;
+}
+
+int decompose_range(dc_graph* h, int32_t k_first, int32_t k_last) {
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    const uint32_t V = g.V;
+    if (k_first <= 0 || !d.peel_valid || !d.kmax_v || !d.row0) {
+        // kmax and row 0 (fused peel)
+        if (int rc = ensure_scratch(h, V)) return rc;
+        Scratch* s = h->scratch;
+        if (!d.kmax_v && dmalloc(h->stream, &d.kmax_v, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+        if (V == 0) return decompose(h, 0, 0);
+        d.valid = false;
+        d.rows_valid = false;
+        cudaEventRecord(h->ev[0], h->stream);
+        int32_t mv[2] = {0, 0};
+        PeelInst I[2] = {make_inst(h, 0, nullptr, 0, d.kmax_v, 0), make_inst(h, 1, nullptr, 0, s->row0, 1)};
+        if (int rc = run_peel2(h, 2, I, mv)) return rc;
+        cudaEventRecord(h->ev[1], h->stream);
+        d.kmax = mv[0];
+        d.lmax = mv[1];
+        if (!d.row0 && dmalloc(h->stream, &d.row0, (uint64_t)V + 1)) return DC_ERR_NOMEM;
+        DC_CUDA(cudaMemcpyAsync(d.row0, s->row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+        DC_CUDA(cudaStreamSynchronize(h->stream));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+        h->times.kmax_ms = ms;
+        d.peel_valid = true;
+    } else {
+        h->times.kmax_ms = 0;
+    }
+    if (int rc = ensure_scratch(h, V)) return rc;
+    Scratch* s = h->scratch;
+    const int32_t K = d.kmax;
+    const int32_t k0 = std::max(1, k_first), k1 = std::min(k_last, K);
+    d.rows_valid = false;
+    // the row kernel starts from row 0 in scratch
+    DC_CUDA(cudaMemcpyAsync(s->row0, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+    uint64_t nlog = 0;
+    if (int rc = rows_from_row0(h, K, k1, true, &nlog, k0)) return rc;
+    if (int rc = build_skyline_from_log(h, nlog)) return rc;
+    cudaEventRecord(h->ev[5], h->stream);
+    DC_CUDA(cudaStreamSynchronize(h->stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
+    h->times.trans_ms = ms;
+    cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]);
+    h->times.sky_ms = ms;
+    h->times.row0_ms = 0;
+    h->times.expand_ms = 0;
+    d.row_lo = k0;
+    d.row_hi = k1;
+    d.valid = true;
+    return DC_OK;
+}
+
 
 }  // namespace dc

@@ -72,8 +72,18 @@ int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del);
 
 // Full decomposition; method 0 = incremental rows, 1 = per-row peel.
 int decompose(dc_graph* h, int method, int materialize_rows);
-// Rows 1..Kstop from row 0 and kmax; corners left in the scratch log.
-int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out);
+// Rows K0..Kstop from row 0 (in the scratch row0) and kmax; corners left in
+// the scratch log.  K0 > 1 jumps from row 0 straight to row K0: the first
+// step is the fixpoint of row K0 below row 0, so the corners it logs at K0
+// are relative to row 0 and rows 1..K0-1 of the resulting skyline are not
+// meaningful.
+int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out, int32_t K0 = 1);
+// kmax and row 0 (fused peel) when k_first <= 0 or not current, then rows
+// max(k_first, 1)..min(k_last, kmax) only; the decomposition then holds row 0
+// and that range.
+int decompose_range(dc_graph* h, int32_t k_first, int32_t k_last);
+// out[k] = total in + out degree of C_k (vertices with kmax >= k), k = 0..kmax.
+int row_weights(dc_graph* h, uint64_t* out);
 // Dense rows [k0, k0+n) into dst (device pointer, row-major, V per row).
 int expand_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* d_dst);
 

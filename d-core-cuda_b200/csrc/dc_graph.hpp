@@ -61,6 +61,15 @@ struct Decomp {
     int32_t* rows = nullptr;  // dense rows when materialised
     uint64_t rows_cap = 0;    // elements allocated
     bool rows_valid = false;
+    bool peel_valid = false;  // kmax_v and row0 match the current graph
+    int32_t row_lo = 1, row_hi = -1;  // rows held besides row 0 (all: 1..kmax)
+    bool full() const { return valid && row_lo <= 1 && row_hi >= kmax; }
+    // every row of [k0, k0 + n) is held (row 0 always is)
+    bool holds(uint64_t k0, uint64_t n) const {
+        if (n == 0) return true;
+        const int64_t first = (int64_t)(k0 == 0 ? 1 : k0), last = (int64_t)(k0 + n - 1);
+        return last < first || (first >= row_lo && last <= row_hi);
+    }
 };
 
 struct MaintLogRec {

@@ -915,7 +915,7 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
     if (method < DC_MAINT_AUTO || method > DC_MAINT_REPEEL) return set_error(DC_ERR_INVALID, "dc_maintain: bad method %d", method);
     if (int rc = ensure_scratch(h, V)) return rc;
     Scratch* s = h->scratch;
-    if (!d.valid)
+    if (!d.full())
         if (int rc = decompose(h, 0, 0)) return rc;
     NetBatch nb;
     if (int rc = net_batch(V, pairs, is_del, b, nb)) return rc;
@@ -1100,7 +1100,13 @@ out:
     mt_free(h->stream, d_dv);
     mt_free(h->stream, d_iu);
     mt_free(h->stream, d_iv);
-    if (rc != DC_OK) d.valid = false;
+    if (rc != DC_OK) {
+        d.valid = false;
+        d.peel_valid = false;
+    } else {
+        d.row_lo = 1;
+        d.row_hi = d.kmax;
+    }
     return rc;
 }
 

@@ -98,6 +98,8 @@ SIGNATURES = {
     "dc_graph_get_edges": [vp, u32p, u32p, ctypes.c_uint64, u64p],
     "dc_graph_write_binary": [vp, ctypes.c_char_p, ctypes.c_uint32],
     "dc_decompose": [vp, ctypes.c_int, i32p, i32p],
+    "dc_decompose_rows": [vp, ctypes.c_uint32, ctypes.c_uint32, i32p, i32p],
+    "dc_row_weights": [vp, u64p, ctypes.c_uint64],
     "dc_maintain": [vp, u32p, u8p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(MaintStats)],
     "dc_decomp_info_get": [vp, ctypes.POINTER(DecompInfo)],
     "dc_get_kmaxes": [vp, i32p],
@@ -424,6 +426,23 @@ class Graph:
         lm = ctypes.c_int32(0)
         _check(lib().dc_decompose(self._h, method, ctypes.byref(km), ctypes.byref(lm)))
         return km.value, lm.value
+
+    def decompose_rows(self, k_first, k_last):
+        """kmax, row 0 and rows max(k_first, 1)..k_last only (row sharding);
+        k_first = 0 recomputes kmax and row 0 even when current; an empty
+        range computes (or keeps) kmax and row 0 alone."""
+        km = ctypes.c_int32(0)
+        lm = ctypes.c_int32(0)
+        k_last = max(k_last, 0)
+        _check(lib().dc_decompose_rows(self._h, k_first, k_last, ctypes.byref(km), ctypes.byref(lm)))
+        return km.value, lm.value
+
+    def row_weights(self):
+        """weights[k] = total degree of the vertices with kmax >= k."""
+        K = self.decomp_info()["kmax"]
+        w = np.zeros(K + 1, np.uint64)
+        _check(lib().dc_row_weights(self._h, _p(w, u64p), K + 1))
+        return w
 
     def maintain(self, src, dst, is_delete=None, method=MAINT_AUTO):
         """maintenanceFast: applies the update batch; returns the stats dict."""

@@ -158,6 +158,21 @@ int dc_graph_device_bytes(const dc_graph* g, uint64_t* bytes);
  * every vertex and all rows lmax[k][v], k = 0..kmax, kept on the device.
  * Reports the global kmax and lmax.  Both methods give identical results. */
 int dc_decompose(dc_graph* g, int method, int32_t* kmax, int32_t* lmax);
+/* A slice of the decomposition, for sharding rows over GPUs that each hold
+ * the whole graph (each row k depends only on the graph and on kmax): kmax
+ * and row 0 (computed when k_first = 0 or when not current), then rows
+ * max(k_first, 1)..k_last only, clamped to kmax (an empty range: kmax and
+ * row 0 alone).  Rows of the
+ * range are derived from row 0 directly, so ranges are independent.
+ * Afterwards row 0 and the range can be read (dc_get_lmax_rows); reading
+ * other rows, the skyline or writing files fails with DC_ERR_STATE until a
+ * full dc_decompose.  No reference counterpart (dcore computes all rows,
+ * main.cu:236-243). */
+int dc_decompose_rows(dc_graph* g, uint32_t k_first, uint32_t k_last, int32_t* kmax, int32_t* lmax);
+/* Work weights for row sharding: weights[k] = total in + out degree of the
+ * vertices with kmax >= k (k = 0..kmax; capacity >= kmax + 1).  Needs kmax
+ * (dc_decompose or dc_decompose_rows). */
+int dc_row_weights(dc_graph* g, uint64_t* weights, uint64_t capacity);
 
 typedef struct dc_decomp_info {
     int32_t kmax, lmax;
