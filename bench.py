@@ -701,6 +701,8 @@ def main():
     ap.add_argument("--workers", type=int, default=0, help="serve: worker threads (0: workload default)")
     ap.add_argument("--shard", choices=["replicas", "rows"], default="replicas",
                     help="decomposition with N > 1: one graph per rank, or the rows of one graph split over ranks")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="decomposition: keep the default launch shapes instead of running dc_autotune first")
     ap.add_argument("--emulate-ranks", type=int, default=0,
                     help="row sharding of one decomposition over N ranks, run one range after another on one GPU")
     args = ap.parse_args()
@@ -740,6 +742,7 @@ def main():
     E = int(len(s))
     g = dc.Graph.from_edges(V, s, d, device=local)
     stream = torch.cuda.ExternalStream(g.stream())
+    tuning, tune_ms = (g.autotune() if args.autotune else (g.tuning(), None))
 
     def step():
         g.decompose(dc.METHOD_INCREMENTAL)
@@ -854,7 +857,9 @@ def main():
                            "lmax": inf["lmax"], "method": "incremental rows", "output": "dense rows in HBM",
                            "l2": "inputs larger than L2 (graph %.0f MB, rows %.0f MB)" % (
                                8.0 * E / 2**20, 4.0 * (K + 1) * V / 2**20),
-                           "parallelism": f"replicas x{world}"},
+                           "parallelism": f"replicas x{world}",
+                           "tuning": dict(tuning, source="autotuner (dc_autotune) before the timed steps"
+                                          if args.autotune else "defaults")},
                 "phases_ms": {"peel": peel_ms, "rows": rows_ms,
                               "other": ms_per_step - peel_ms - rows_ms},
                 "gpu_launches": int(launches), "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,

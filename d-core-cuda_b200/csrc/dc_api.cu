@@ -507,6 +507,86 @@ extern "C" int dc_set_launch(dc_graph* h, int blocks_per_sm) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");
     if (blocks_per_sm < 0 || blocks_per_sm > 8) return set_error(DC_ERR_INVALID, "blocks_per_sm must be 0..8");
     h->blocks_per_sm = blocks_per_sm;
+    h->peel_bps = 0;
+    h->rows_bps = 0;
+    return DC_OK;
+}
+
+extern "C" int dc_get_tuning(dc_graph* h, dc_tuning* t) {
+    if (!h || !t) return set_error(DC_ERR_INVALID, "null argument");
+    const int dflt = h->blocks_per_sm > 0 ? h->blocks_per_sm : 1;
+    t->peel_blocks_per_sm = h->peel_bps > 0 ? h->peel_bps : dflt;
+    t->rows_blocks_per_sm = h->rows_bps > 0 ? h->rows_bps : dflt;
+    t->peel_chunk = (int32_t)h->peel_chunk;
+    t->reserved = 0;
+    return DC_OK;
+}
+
+extern "C" int dc_set_tuning(dc_graph* h, const dc_tuning* t) {
+    if (!h || !t) return set_error(DC_ERR_INVALID, "null argument");
+    if (t->peel_blocks_per_sm < 1 || t->peel_blocks_per_sm > 8 || t->rows_blocks_per_sm < 1 ||
+        t->rows_blocks_per_sm > 8)
+        return set_error(DC_ERR_INVALID, "dc_set_tuning: blocks per SM must be 1..8");
+    if (t->peel_chunk < 16 || t->peel_chunk > 4096 || (t->peel_chunk & (t->peel_chunk - 1)))
+        return set_error(DC_ERR_INVALID, "dc_set_tuning: peel_chunk must be a power of two in 16..4096");
+    h->peel_bps = t->peel_blocks_per_sm;
+    h->rows_bps = t->rows_blocks_per_sm;
+    h->peel_chunk = (unsigned)t->peel_chunk;
+    return DC_OK;
+}
+
+// Coordinate search: the fused peel's grid and chunk size timed on the peel
+// alone, then the row kernel's grid timed on the rows alone (kmax and row 0
+// reused); every candidate runs twice and keeps its faster time.  The
+// fastest setting stays on the handle, which ends with a full
+// decomposition.
+extern "C" int dc_autotune(dc_graph* h, dc_tuning* best, float* best_ms) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    API_CUDA(cudaSetDevice(h->device));
+    dc_tuning cur;
+    dc_get_tuning(h, &cur);
+    if (int rc = decompose_range(h, 0, 0)) return rc;  // warm-up
+    float peel_best = 1e30f;
+    dc_tuning pick = cur;
+    for (int bps = 1; bps <= 4; ++bps)
+        for (int chunk = 32; chunk <= 256; chunk *= 2) {
+            dc_tuning t = pick;
+            t.peel_blocks_per_sm = bps;
+            t.peel_chunk = chunk;
+            dc_set_tuning(h, &t);
+            float ms = 1e30f;
+            for (int r = 0; r < 2; ++r) {
+                if (int rc = decompose_range(h, 0, 0)) return rc;
+                ms = std::min(ms, h->times.kmax_ms);
+            }
+            if (ms < peel_best) {
+                peel_best = ms;
+                pick.peel_blocks_per_sm = bps;
+                pick.peel_chunk = chunk;
+            }
+        }
+    dc_set_tuning(h, &pick);
+    if (int rc = decompose_range(h, 0, 0)) return rc;
+    float rows_best = 1e30f;
+    const int32_t K = h->d.kmax;
+    for (int bps = 1; bps <= 4; ++bps) {
+        dc_tuning t = pick;
+        t.rows_blocks_per_sm = bps;
+        dc_set_tuning(h, &t);
+        float ms = 1e30f;
+        for (int r = 0; r < 2; ++r) {
+            if (int rc = decompose_range(h, 1, K)) return rc;
+            ms = std::min(ms, h->times.trans_ms);
+        }
+        if (ms < rows_best) {
+            rows_best = ms;
+            pick.rows_blocks_per_sm = bps;
+        }
+    }
+    dc_set_tuning(h, &pick);
+    if (int rc = decompose(h, 0, 0)) return rc;
+    if (best) *best = pick;
+    if (best_ms) *best_ms = peel_best + rows_best;
     return DC_OK;
 }
 

@@ -1481,20 +1481,21 @@ int ensure_tring(dc_graph* h, uint64_t need) {
     return DC_OK;
 }
 
-static int persistent_grid(dc_graph* h, const void* fn, int* blocks) {
+static int persistent_grid(dc_graph* h, const void* fn, int bps, int* blocks) {
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0);
     if (e != cudaSuccess || per_sm < 1)
         return set_error(DC_ERR_CUDA, "occupancy query failed (%s)", cudaGetErrorString(e));
-    per_sm = std::min(per_sm, h->blocks_per_sm > 0 ? h->blocks_per_sm : 1);
+    if (bps <= 0) bps = h->blocks_per_sm > 0 ? h->blocks_per_sm : 1;
+    per_sm = std::min(per_sm, bps);
     *blocks = per_sm * h->geom.sms;
     return DC_OK;
 }
 
 // Launches a persistent kernel, waits, and converts its device status.
-int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out) {
+int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out, int bps) {
     int blocks = 0;
-    if (int rc = persistent_grid(h, fn, &blocks)) return rc;
+    if (int rc = persistent_grid(h, fn, bps, &blocks)) return rc;
     {
         EngineCtl& init = h->ctl_init;
         memset(&init, 0, sizeof(init));
@@ -1547,18 +1548,17 @@ PeelInst make_inst(dc_graph* h, int which, const int32_t* member, int32_t k, int
     return I;
 }
 
-static constexpr unsigned kPeelChunk = 64;
-
 // Runs one or two peels in one persistent launch; maxv[i] = largest value.
 int run_peel2(dc_graph* h, int ninst, const PeelInst* inst, int32_t* maxv) {
     Scratch* s = h->scratch;
     DevGraph& g = h->g;
-    uint64_t need = 2ull * g.V + 2ull * (g.out_cap + g.in_cap) / kPeelChunk + (uint64_t)h->geom.sms * 64 + 4096;
+    const unsigned chunk = h->peel_chunk ? h->peel_chunk : 64;
+    uint64_t need = 2ull * g.V + 2ull * (g.out_cap + g.in_cap) / chunk + (uint64_t)h->geom.sms * 64 + 4096;
     if (int rc = ensure_tring(h, need)) return rc;
     Peel2Params p;
     p.V = g.V;
     p.ninst = ninst;
-    p.chunk = kPeelChunk;
+    p.chunk = chunk;
     p.in[0] = inst[0];
     p.in[1] = ninst > 1 ? inst[1] : inst[0];
     p.q.slots = s->tring;
@@ -1566,7 +1566,7 @@ int run_peel2(dc_graph* h, int ninst, const PeelInst* inst, int32_t* maxv) {
     p.ctl = h->ctl;
     void* args[] = {&p};
     EngineCtl hc;
-    if (int rc = run_persistent(h, (const void*)k_peel2, args, "peel", &hc)) return rc;
+    if (int rc = run_persistent(h, (const void*)k_peel2, args, "peel", &hc, h->peel_bps)) return rc;
     for (int i = 0; i < ninst; ++i) maxv[i] = hc.maxv[i];
     return DC_OK;
 }
@@ -1782,7 +1782,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     if (Kstop >= tp.K0) {
         void* args[] = {&tp};
         EngineCtl hc;
-        if (int rc = run_persistent(h, (const void*)k_trans2, args, "transitions", &hc)) return rc;
+        if (int rc = run_persistent(h, (const void*)k_trans2, args, "transitions", &hc, h->rows_bps)) return rc;
         nlog = hc.log_count;
         h->stat_evals = hc.evals;
         h->stat_drops = hc.drops;

@@ -106,6 +106,9 @@ struct dc_graph {
     uint32_t gap_div = 0;      // extra slack = len / gap_div (0 = none)
     int method = 0;            // 0 = incremental rows, 1 = per-row peel
     int blocks_per_sm = 0;     // persistent-kernel blocks per SM (0 = default)
+    int peel_bps = 0;          // the fused peel's blocks per SM (0 = blocks_per_sm)
+    int rows_bps = 0;          // the row kernel's blocks per SM (0 = blocks_per_sm)
+    unsigned peel_chunk = 64;  // adjacency entries per peel work item
     uint64_t stat_evals = 0, stat_drops = 0, stat_entries = 0;
     dc::EngineCtl ctl_init{};
     // optional per-step trace of persistent kernels (diagnostics)

@@ -63,6 +63,11 @@ class MaintStats(ctypes.Structure):
 MAINT_AUTO, MAINT_LOCAL, MAINT_REPEEL = 0, 1, 2
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("peel_blocks_per_sm", ctypes.c_int32), ("rows_blocks_per_sm", ctypes.c_int32),
+                ("peel_chunk", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
 class ServerInfo(ctypes.Structure):
     _fields_ = [("budget_bytes", ctypes.c_uint64), ("used_bytes", ctypes.c_uint64), ("peak_bytes", ctypes.c_uint64),
                 ("admissions", ctypes.c_uint64), ("evictions", ctypes.c_uint64), ("batches", ctypes.c_uint64),
@@ -116,6 +121,9 @@ SIGNATURES = {
     "dc_graph_stream": [vp, ctypes.POINTER(vp)],
     "dc_set_trace": [vp, ctypes.c_uint32, vp, vp],
     "dc_set_launch": [vp, ctypes.c_int],
+    "dc_get_tuning": [vp, ctypes.POINTER(Tuning)],
+    "dc_set_tuning": [vp, ctypes.POINTER(Tuning)],
+    "dc_autotune": [vp, ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_float)],
     "dc_sched_create": [ctypes.c_uint64, ctypes.POINTER(vp)],
     "dc_sched_free": [vp],
     "dc_sched_param_count": [],
@@ -536,6 +544,23 @@ class Graph:
             callback(phase.decode(), arr)
         self._trace_cb = CB(_cb)
         _check(lib().dc_set_trace(self._h, max_steps, ctypes.cast(self._trace_cb, vp), None))
+
+    def tuning(self):
+        t = Tuning()
+        _check(lib().dc_get_tuning(self._h, ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in Tuning._fields_ if f != "reserved"}
+
+    def set_tuning(self, peel_blocks_per_sm=1, rows_blocks_per_sm=1, peel_chunk=64):
+        t = Tuning(peel_blocks_per_sm, rows_blocks_per_sm, peel_chunk, 0)
+        _check(lib().dc_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self):
+        """Picks the fastest launch shapes for this graph (dc_autotune);
+        returns (setting, its peel + rows device ms)."""
+        t = Tuning()
+        ms = ctypes.c_float(0)
+        _check(lib().dc_autotune(self._h, ctypes.byref(t), ctypes.byref(ms)))
+        return {f: getattr(t, f) for f, _ in Tuning._fields_ if f != "reserved"}, ms.value
 
     def set_launch(self, blocks_per_sm):
         _check(lib().dc_set_launch(self._h, blocks_per_sm))

@@ -352,6 +352,25 @@ int dc_set_trace(dc_graph* g, uint32_t max_steps, dc_trace_fn fn, void* user);
 /* Persistent-kernel blocks per SM (0 = default). */
 int dc_set_launch(dc_graph* g, int blocks_per_sm);
 
+/* Launch shapes of the persistent kernels: blocks per SM of the fused peel
+ * and of the row kernel, and adjacency entries per peel work item.  No
+ * counterpart in the reference (its launches are fixed at <<<256, 1024>>>,
+ * src/common.h:32-33).  Any setting gives identical results. */
+typedef struct dc_tuning {
+    int32_t peel_blocks_per_sm; /* 1..8 (capped by occupancy) */
+    int32_t rows_blocks_per_sm; /* 1..8 (capped by occupancy) */
+    int32_t peel_chunk;         /* power of two, 16..4096 */
+    int32_t reserved;
+} dc_tuning;
+int dc_get_tuning(dc_graph* g, dc_tuning* t);
+int dc_set_tuning(dc_graph* g, const dc_tuning* t);
+/* Autotuner: times the decomposition of this graph under candidate launch
+ * shapes (peel grid and chunk on the peel alone, then the row kernel's grid
+ * on the rows alone, each candidate twice), keeps the fastest on the handle
+ * and ends with a full decomposition.  *best / *best_ms (may be NULL): the
+ * chosen setting and its peel + rows device time. */
+int dc_autotune(dc_graph* g, dc_tuning* best, float* best_ms);
+
 /* Engine kernel launches since the library was loaded. */
 int dc_launch_count(unsigned long long* n);
 
