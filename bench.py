@@ -297,6 +297,7 @@ def run_maintenance(args, w, rank, world, local):
     V, s, d = make_graph(dc, w, rank)
     u, v, dl = dc.gen_updates(V, s, d, w["ops"], 0.5, w["seed"] + 1000 + rank)
     g = dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16)
+    g.set_row_repair(args.row_repair)
     g.decompose(dc.METHOD_INCREMENTAL)
     sampler = ClockSampler(local)
     launches0 = dc.launch_count()
@@ -309,15 +310,18 @@ def run_maintenance(args, w, rank, world, local):
             continue
         lat = []
         methods = []
+        local_rows = 0
         for _ in range(nb):
             st = g.maintain(u[pos:pos + bs], v[pos:pos + bs], dl[pos:pos + bs], args.maint_method)
             lat.append(st["total_ms"])
             methods.append(st["method"])
+            local_rows += st["rows_local"]
             pos += bs
         lat = np.array(lat)
         per_size[str(bs)] = {"batches": nb, "updates_per_s": bs * nb / (lat.sum() / 1000.0),
                              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                             "methods": {"local": methods.count(1), "repeel": methods.count(2)}}
+                             "methods": {"local": methods.count(1), "repeel": methods.count(2)},
+                             "rows_repaired_in_place": local_rows}
     clocks = sampler.stop()
     launches = dc.launch_count() - launches0
     head = per_size.get("10000") or per_size[max(per_size, key=lambda k: int(k))]
@@ -328,7 +332,8 @@ def run_maintenance(args, w, rank, world, local):
             "config": {"workload": args.workload, "graph": w["desc"], "V": V, "E": int(len(s)),
                        "headline": "batches of 10,000 updates", "per_batch_size": per_size,
                        "exactness": "each batch leaves kmaxes and rows equal to a full recomputation",
-                       "method": {0: "scheduler", 1: "local", 2: "re-peel"}[args.maint_method]},
+                       "method": {0: "scheduler", 1: "local", 2: "re-peel"}[args.maint_method],
+                       "row_repair": bool(args.row_repair)},
             "gpu_launches": int(launches), "clocks": clocks}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -701,6 +706,8 @@ def main():
     ap.add_argument("--workers", type=int, default=0, help="serve: worker threads (0: workload default)")
     ap.add_argument("--shard", choices=["replicas", "rows"], default="replicas",
                     help="decomposition with N > 1: one graph per rank, or the rows of one graph split over ranks")
+    ap.add_argument("--no-row-repair", dest="row_repair", action="store_false",
+                    help="maintenance: recompute rows 1..R for deletions instead of repairing them in place")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="decomposition: keep the default launch shapes instead of running dc_autotune first")
     ap.add_argument("--emulate-ranks", type=int, default=0,

@@ -303,6 +303,12 @@ extern "C" int dc_maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is
     return maintain(h, pairs, is_delete, b, method, stats);
 }
 
+extern "C" int dc_set_row_repair(dc_graph* h, int on) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    h->row_repair = on ? 1 : 0;
+    return DC_OK;
+}
+
 extern "C" int dc_graph_set_scheduler(dc_graph* h, dc_sched* s) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");
     h->sched = s;

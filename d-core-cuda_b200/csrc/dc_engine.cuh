@@ -67,6 +67,12 @@ int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_d
 
 // Batch maintenance (dc_maint.cu).
 int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t b, int method, dc_maint_stats* st);
+// Rows 1..R repaired in place after a deletion-only batch (dc_repair.cu);
+// *applied = false when the caller must recompute them instead.
+int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_dv, uint32_t n_del, bool* applied);
+// Deletions per batch below which maintenance splits a mixed batch to repair
+// its rows in place.
+uint32_t row_repair_max_deletions();
 // Maintenance method for a batch (rule of thumb or the learned scheduler).
 int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del);
 

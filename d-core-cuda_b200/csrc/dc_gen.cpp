@@ -226,7 +226,11 @@ extern "C" int dc_gen_updates_hot(uint32_t V, uint64_t E, const uint32_t* src, c
     std::unordered_map<uint64_t, uint64_t> added_pos;
     added_pos.reserve(n_ops);
     dc::Xoshiro256ss rng(dc::derive_seed(seed, 0x555044ull));
-    const uint64_t thr = (uint64_t)(insert_frac * 18446744073709551615.0);
+    // insert when the next 64-bit draw is <= thr (insert_frac of the range);
+    // 1.0 and above: always, 0 and below: never (but for an empty graph)
+    const uint64_t thr = insert_frac >= 1.0   ? ~0ull
+                         : insert_frac <= 0.0 ? 0ull
+                                              : (uint64_t)(insert_frac * 18446744073709551616.0);
     auto present = [&](uint64_t k, int64_t* orig) -> bool {
         auto it = std::lower_bound(keys.begin(), keys.end(), k);
         *orig = -1;

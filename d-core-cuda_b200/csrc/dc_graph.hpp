@@ -109,6 +109,7 @@ struct dc_graph {
     int peel_bps = 0;          // the fused peel's blocks per SM (0 = blocks_per_sm)
     int rows_bps = 0;          // the row kernel's blocks per SM (0 = blocks_per_sm)
     unsigned peel_chunk = 64;  // adjacency entries per peel work item
+    int row_repair = 1;        // deletions: repair rows locally instead of recomputing
     uint64_t stat_evals = 0, stat_drops = 0, stat_entries = 0;
     dc::EngineCtl ctl_init{};
     // optional per-step trace of persistent kernels (diagnostics)

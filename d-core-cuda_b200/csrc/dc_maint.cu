@@ -919,6 +919,34 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
         if (int rc = decompose(h, 0, 0)) return rc;
     NetBatch nb;
     if (int rc = net_batch(V, pairs, is_del, b, nb)) return rc;
+    if (h->row_repair && !nb.del_u.empty() && !nb.ins_u.empty() && nb.del_u.size() <= row_repair_max_deletions()) {
+        // deletions first (their rows are repaired in place), then the
+        // insertions: the net effect per edge makes the two commute
+        std::vector<uint32_t> pd(2 * nb.del_u.size()), pi(2 * nb.ins_u.size());
+        for (size_t i = 0; i < nb.del_u.size(); ++i) {
+            pd[2 * i] = nb.del_u[i];
+            pd[2 * i + 1] = nb.del_v[i];
+        }
+        for (size_t i = 0; i < nb.ins_u.size(); ++i) {
+            pi[2 * i] = nb.ins_u[i];
+            pi[2 * i + 1] = nb.ins_v[i];
+        }
+        std::vector<uint8_t> ones(nb.del_u.size(), 1);
+        dc_maint_stats a, c;
+        if (int rc = maintain(h, pd.data(), ones.data(), nb.del_u.size(), method, &a)) return rc;
+        if (int rc = maintain(h, pi.data(), nullptr, nb.ins_u.size(), method, &c)) return rc;
+        *st = c;
+        st->deleted = a.deleted;
+        st->rows_recomputed = std::max(a.rows_recomputed, c.rows_recomputed);
+        st->rebuilt = a.rebuilt | c.rebuilt;
+        st->rows_local = a.rows_local;
+        st->region = a.region + c.region;
+        st->apply_ms = a.apply_ms + c.apply_ms;
+        st->core_ms = a.core_ms + c.core_ms;
+        st->rows_ms = a.rows_ms + c.rows_ms;
+        st->total_ms = a.total_ms + c.total_ms;
+        return DC_OK;
+    }
     st->deleted = nb.n_del;
     st->inserted = nb.n_ins;
     float feat[16];
@@ -1009,6 +1037,21 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
             st->kmax = d.kmax;
             st->lmax = d.lmax;
             goto timing;
+        }
+        // ---- deletions only: repair rows 1..R in place
+        if (h->row_repair && nb.ins_u.empty() && !nb.del_u.empty()) {
+            bool applied = false;
+            if ((rc = rows_repair(h, R, d_du, d_dv, (uint32_t)nb.del_u.size(), &applied))) goto out;
+            if (applied) {
+                st->rows_local = 1;
+                d.kmax = Knew;
+                d.lmax = res[2];
+                d.rows_valid = false;
+                d.valid = true;
+                st->kmax = d.kmax;
+                st->lmax = d.lmax;
+                goto timing;
+            }
         }
         // ---- rows 0..R from the new row 0, rows above R from the old skyline
         MT_CUDA(cudaMemcpyAsync(s->row0, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));

@@ -1,0 +1,679 @@
+// Local row repair after edge deletions.
+//
+// Deleting edges (and the vertices that leave C_k because their kmax fell)
+// can only lower row values: new row k is the greatest fixpoint of the row-k
+// operator of the updated graph that lies below old row k.  Each block takes
+// whole rows k = 1..R from a counter and repairs one row at a time, starting
+// from the old row (read from the old skyline) and touching only the vertices
+// the deletions reach:
+//
+//   seeds    the endpoints of deleted edges that are still in C_k, and the
+//            neighbours that a vertex leaving C_k was supporting
+//   evaluate l(x) = max L <= cur(x) with #{out-nbrs w in C_k, l(w) >= L} >= L
+//            and #{in-nbrs u in C_k, l(u) >= L} >= k, by windowed histograms
+//            over x's lists, neighbour values from the block's overrides or
+//            the old skyline
+//   drop     write the lower value, queue the neighbours whose support it
+//            was (values in (new, old])
+//
+// Overrides and the work queue live in shared memory (one open-addressed
+// table per block); a row that touches more vertices than the table holds
+// aborts the repair and the caller recomputes the rows instead.  The changed
+// (v, k, value) triples go to a log from which the new skyline is merged with
+// the old one.
+//
+// The row semantics are those of the reference's per-row pass
+// (KListInplace, main.cu:171-195, driven by dcore, main.cu:236-243); the
+// reference itself re-peels rows after maintenance (maintenanceFast,
+// main.cu:1735-1743) and its exact l-list maintenance is disabled code
+// (main.cu:929-1242).
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <vector>
+
+#include "dc_engine.cuh"
+#include "dc_internal.h"
+
+namespace dc {
+
+extern std::atomic<unsigned long long> g_launches;
+
+namespace {
+
+constexpr int kRThreads = 256;
+constexpr int kRWarps = kRThreads / 32;
+constexpr int kHashBits = 13;
+constexpr int kHash = 1 << kHashBits;  // vertices a block can touch in one row
+constexpr unsigned kHashLimit = kHash * 3 / 4;  // more than this aborts the repair
+constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
+constexpr int kUnset = 0x7FFFFFFF;   // no override: the old value applies
+constexpr uint32_t kEmptySlot = 0xFFFFFFFFu;
+constexpr int kRWin = 64;
+
+struct RepairParams {
+    uint32_t V;
+    const uint32_t* out_off;
+    const int32_t* out_len;
+    const uint32_t* out_nbr;
+    const uint32_t* in_off;
+    const int32_t* in_len;
+    const uint32_t* in_nbr;
+    const int32_t* kmax_new;
+    const int32_t* kmax_old;
+    const uint32_t* sky_off;  // old skyline
+    const int32_t* sky_k;
+    const int32_t* sky_l;
+    const uint32_t* del_u;  // deleted edges u -> v
+    const uint32_t* del_v;
+    uint32_t n_del;
+    const uint32_t* leave;  // vertices whose kmax fell
+    uint32_t n_leave;
+    int32_t R;
+    uint32_t* log_v;
+    int32_t* log_k;
+    int32_t* log_l;
+    unsigned long long log_cap;
+    EngineCtl* ctl;  // level = row counter, log_count, error
+};
+
+struct RowState {
+    uint32_t key[kHash];
+    int cur[kHash];
+    unsigned st[kHash];  // 0 idle, 1 queued or being evaluated, 2 re-run requested
+    uint32_t ring[kHash];
+    unsigned qhead, qtail, used;
+    int out;    // queued + running items
+    int abort;  // table full, or a wait ran out
+    int k;
+    int hist[kRWarps][2][kRWin];
+};
+
+__device__ __forceinline__ int vld(const int* p) { return *(const volatile int*)p; }
+__device__ __forceinline__ unsigned vldu(const unsigned* p) { return *(const volatile unsigned*)p; }
+
+// Old row-k value of v: the last corner at or below k (binary search).
+__device__ __forceinline__ int sky_at(const RepairParams& p, uint32_t v, int k) {
+    uint32_t a = p.sky_off[v], b = p.sky_off[v + 1];
+    int val = 0;
+    while (a < b) {
+        uint32_t m = (a + b) >> 1;
+        if (p.sky_k[m] <= k) {
+            val = p.sky_l[m];
+            a = m + 1;
+        } else {
+            b = m;
+        }
+    }
+    return val;
+}
+
+__device__ __forceinline__ unsigned hslot0(uint32_t v) { return (v * 2654435761u) >> (32 - kHashBits); }
+
+// Table slot of v (inserting it when asked); -1 when absent / table full.
+__device__ int h_slot(RowState& S, uint32_t v, bool insert) {
+    unsigned i = hslot0(v) & (kHash - 1);
+    for (int probe = 0; probe < kHash; ++probe) {
+        uint32_t key = vldu(&S.key[i]);
+        if (key == v) return (int)i;
+        if (key == kEmptyKey) {
+            if (!insert) return -1;
+            uint32_t prev = atomicCAS(&S.key[i], kEmptyKey, v);
+            if (prev == kEmptyKey) {
+                if (atomicAdd(&S.used, 1u) >= kHashLimit) atomicExch(&S.abort, 1);
+                return (int)i;
+            }
+            if (prev == v) return (int)i;
+        }
+        i = (i + 1) & (kHash - 1);
+    }
+    atomicExch(&S.abort, 1);
+    return -1;
+}
+
+// Row-k value of w: -1 outside C_k, else the override or the old value.
+__device__ __forceinline__ int rv(const RepairParams& p, RowState& S, uint32_t w, int k) {
+    if (p.kmax_new[w] < k) return -1;
+    int i = h_slot(S, w, false);
+    if (i >= 0) {
+        int c = vld(&S.cur[i]);
+        if (c != kUnset) return c;
+    }
+    return sky_at(p, w, k);
+}
+
+__device__ __forceinline__ void enqueue(RowState& S, unsigned slot) {
+    atomicAdd(&S.out, 1);
+    unsigned pos = atomicAdd(&S.qtail, 1u);
+    __threadfence_block();
+    *(volatile uint32_t*)&S.ring[pos & (kHash - 1)] = slot;
+}
+
+// Any thread: asks for an evaluation of w at this row.
+__device__ __forceinline__ void push(RowState& S, uint32_t w) {
+    int slot = h_slot(S, w, true);
+    if (slot < 0) return;
+    unsigned old = atomicCAS(&S.st[slot], 0u, 1u);
+    if (old == 0u) enqueue(S, (unsigned)slot);
+    else if (old == 1u) atomicCAS(&S.st[slot], 1u, 2u);
+}
+
+// Converged warp: one histogram pass over a list for the window [lo, hi];
+// values above hi land in the top bin on the first window only.
+__device__ __forceinline__ void r_hist(const RepairParams& p, RowState& S, const uint32_t* a, int n, int k, int lo,
+                                       int hi, bool first, int* bins) {
+    const unsigned lane = threadIdx.x & 31u;
+    int top = 0;
+    for (int e = (int)lane; e < n; e += 32) {
+        int x = rv(p, S, a[e], k);
+        if (x > hi) top += first;
+        else if (x == hi) ++top;
+        else if (x >= lo) atomicAdd(&bins[x - lo], 1);
+    }
+#pragma unroll
+    for (int s = 16; s; s >>= 1) top += __shfl_xor_sync(0xFFFFFFFFu, top, s);
+    if (lane == 0 && top) atomicAdd(&bins[hi - lo], top);
+}
+
+// Converged warp, after x dropped from cap to nv (value already written):
+// queues the neighbours in a list whose value lies in (nv, cap] and returns
+// how many neighbours hold at least nv, read after the write.  The recount
+// closes the race in which x and a neighbour drop at the same time and each
+// read the other's old value: whichever reads second sees the other's write.
+__device__ __forceinline__ int r_release(const RepairParams& p, RowState& S, const uint32_t* a, int n, int k, int nv,
+                                         int cap) {
+    int support = 0;
+    for (int e = (int)(threadIdx.x & 31u); e < n && !vld(&S.abort); e += 32) {
+        uint32_t w = a[e];
+        int x = rv(p, S, w, k);
+        support += x >= nv;
+        if (x > nv && x <= cap) push(S, w);
+    }
+#pragma unroll
+    for (int s = 16; s; s >>= 1) support += __shfl_xor_sync(0xFFFFFFFFu, support, s);
+    return support;
+}
+
+// Converged warp: takes a queued slot; false when the row is finished or
+// abandoned.
+__device__ bool r_take(const RepairParams& p, RowState& S, unsigned* slot) {
+    const unsigned lane = threadIdx.x & 31u;
+    int state = 0;
+    unsigned got = 0;
+    if (lane == 0) {
+        unsigned t = atomicAdd(&S.qhead, 1u);
+        volatile uint32_t* cell = (volatile uint32_t*)&S.ring[t & (kHash - 1)];
+        unsigned long long t0 = 0;
+        for (unsigned spins = 0;; ++spins) {
+            uint32_t it = *cell;
+            if (it != kEmptySlot) {
+                *cell = kEmptySlot;
+                got = it;
+                state = 1;
+                break;
+            }
+            if (vld(&S.out) == 0 || vld(&S.abort) || ld_vol(&p.ctl->error)) {
+                state = 2;
+                break;
+            }
+            if (spins == 64) t0 = gtimer();
+            if (spins > 64 && (spins & 63) == 0 && gtimer() - t0 > kWaitNs) {
+                set_dev_error(p.ctl, DC_DEV_ERR_TIMEOUT, 40);
+                atomicExch(&S.abort, 1);
+                state = 2;
+                break;
+            }
+            if (spins > 16) __nanosleep(64);
+        }
+    }
+    state = __shfl_sync(0xFFFFFFFFu, state, 0);
+    *slot = __shfl_sync(0xFFFFFFFFu, got, 0);
+    __threadfence_block();
+    return state == 1;
+}
+
+__global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    RowState& S = *reinterpret_cast<RowState*>(s_raw);
+    const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    int* ho = S.hist[wib][0];
+    int* hi_ = S.hist[wib][1];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) S.k = ld_vol(&p.ctl->error) ? p.R + 1 : atomicAdd(&p.ctl->level, 1) + 1;
+        for (int i = threadIdx.x; i < kHash; i += kRThreads) {
+            S.key[i] = kEmptyKey;
+            S.cur[i] = kUnset;
+            S.st[i] = 0;
+            S.ring[i] = kEmptySlot;
+        }
+        if (threadIdx.x == 0) {
+            S.qhead = S.qtail = S.used = 0;
+            S.out = 1;  // held by the seeding phase
+            S.abort = 0;
+        }
+        __syncthreads();
+        const int k = S.k;
+        if (k > p.R) break;
+        // ---- seeds: endpoints of deleted edges still in C_k
+        for (uint32_t i = threadIdx.x; i < p.n_del && !vld(&S.abort); i += kRThreads) {
+            uint32_t u = p.del_u[i], v = p.del_v[i];
+            if (p.kmax_new[u] >= k) push(S, u);
+            if (p.kmax_new[v] >= k) push(S, v);
+        }
+        // ---- vertices leaving C_k: the neighbours they supported
+        for (uint32_t i = wib; i < p.n_leave; i += kRWarps) {
+            if (__any_sync(0xFFFFFFFFu, vld(&S.abort))) break;
+            uint32_t x = p.leave[i];
+            if (!(p.kmax_old[x] >= k && p.kmax_new[x] < k)) continue;
+            int ox = sky_at(p, x, k);
+            const uint32_t* a = p.out_nbr + p.out_off[x];
+            int n = p.out_len[x];
+            for (int e = (int)lane; e < n && !vld(&S.abort); e += 32) {
+                uint32_t z = a[e];
+                int vz = rv(p, S, z, k);
+                if (vz >= 1 && vz <= ox) push(S, z);
+            }
+            a = p.in_nbr + p.in_off[x];
+            n = p.in_len[x];
+            for (int e = (int)lane; e < n && !vld(&S.abort); e += 32) {
+                uint32_t y = a[e];
+                int vy = rv(p, S, y, k);
+                if (vy >= 1 && vy <= ox) push(S, y);
+            }
+        }
+        for (int sweep = 0;; ++sweep) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicSub(&S.out, 1);
+        __syncthreads();
+        // ---- drain
+        unsigned slot;
+        while (r_take(p, S, &slot)) {
+            const uint32_t x = vldu(&S.key[slot]);
+            int cap = vld(&S.cur[slot]);
+            if (cap == kUnset) cap = sky_at(p, x, k);
+            int nv = cap;
+            if (cap >= 1 && p.kmax_new[x] >= k) {
+                const uint32_t* ao = p.out_nbr + p.out_off[x];
+                const uint32_t* ai = p.in_nbr + p.in_off[x];
+                const int no = p.out_len[x], ni = p.in_len[x];
+                int carry_o = 0, carry_i = 0, hi = cap;
+                bool first = true;
+                for (;;) {
+                    const int lo = max(0, hi - (kRWin - 1));
+                    ho[lane] = 0;
+                    ho[lane + 32] = 0;
+                    hi_[lane] = 0;
+                    hi_[lane + 32] = 0;
+                    __syncwarp();
+                    r_hist(p, S, ao, no, k, lo, hi, first, ho);
+                    r_hist(p, S, ai, ni, k, lo, hi, first, hi_);
+                    __syncwarp();
+                    int found = -1;
+                    if (lane == 0) {
+                        for (int L = hi; L >= lo; --L) {
+                            carry_o += ho[L - lo];
+                            carry_i += hi_[L - lo];
+                            if (carry_o >= L && carry_i >= k) {
+                                found = L;
+                                break;
+                            }
+                        }
+                    }
+                    found = __shfl_sync(0xFFFFFFFFu, found, 0);
+                    carry_o = __shfl_sync(0xFFFFFFFFu, carry_o, 0);
+                    carry_i = __shfl_sync(0xFFFFFFFFu, carry_i, 0);
+                    __syncwarp();
+                    if (found >= 0) {
+                        nv = found;
+                        break;
+                    }
+                    if (lo == 0) {  // a member keeps at least 0
+                        nv = 0;
+                        break;
+                    }
+                    hi = lo - 1;
+                    first = false;
+                }
+                if (nv < cap) {
+                    if (lane == 0) atomicExch(&S.cur[slot], nv);
+                    __syncwarp();
+                    __threadfence_block();
+                    const int so = r_release(p, S, ao, no, k, nv, cap);
+                    const int si = r_release(p, S, ai, ni, k, nv, cap);
+                    // a neighbour fell below nv meanwhile: evaluate x again
+                    if (lane == 0 && nv >= 1 && (so < nv || si < k)) atomicCAS(&S.st[slot], 1u, 2u);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                if (atomicCAS(&S.st[slot], 1u, 0u) == 2u) {
+                    atomicExch(&S.st[slot], 1u);
+                    enqueue(S, slot);
+                }
+                __threadfence_block();
+                atomicSub(&S.out, 1);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        if (S.abort) break;
+        // ---- the row is quiet: every touched vertex must hold its value
+        // against the final values of its neighbours; queue any that does
+        // not and drain again
+        if (threadIdx.x == 0) {
+            S.qhead = S.qtail = 0;
+            S.out = 1;  // held by the sweep
+            S.k = 0;    // vertices found unstable
+        }
+        for (int i = threadIdx.x; i < kHash; i += kRThreads) S.ring[i] = kEmptySlot;
+        __syncthreads();
+        for (int i = wib; i < kHash; i += kRWarps) {
+            const uint32_t x = S.key[i];
+            if (x == kEmptyKey || p.kmax_new[x] < k) continue;
+            int val = S.cur[i];
+            if (val == kUnset) val = sky_at(p, x, k);
+            if (val < 1) continue;
+            int so = 0, si = 0;
+            const uint32_t* ao = p.out_nbr + p.out_off[x];
+            const uint32_t* ai = p.in_nbr + p.in_off[x];
+            for (int e = (int)lane; e < p.out_len[x]; e += 32) so += rv(p, S, ao[e], k) >= val;
+            for (int e = (int)lane; e < p.in_len[x]; e += 32) si += rv(p, S, ai[e], k) >= val;
+#pragma unroll
+            for (int s = 16; s; s >>= 1) {
+                so += __shfl_xor_sync(0xFFFFFFFFu, so, s);
+                si += __shfl_xor_sync(0xFFFFFFFFu, si, s);
+            }
+            if (lane == 0 && (so < val || si < k)) {
+                atomicAdd(&S.k, 1);
+                push(S, x);
+            }
+        }
+        __syncthreads();
+        const bool again = S.k != 0;
+        __syncthreads();
+        if (threadIdx.x == 0) S.k = k;
+        if (!again) {
+            __syncthreads();
+            break;
+        }
+        }
+        __syncthreads();
+        if (S.abort) {
+            if (threadIdx.x == 0) set_dev_error(p.ctl, DC_DEV_ERR_CAPACITY, 41);
+            break;
+        }
+        // ---- changed values of this row to the log
+        for (int i = threadIdx.x; i < kHash; i += kRThreads) {
+            uint32_t v = S.key[i];
+            int c = S.cur[i];
+            if (v == kEmptyKey || c == kUnset) continue;
+            if (c >= sky_at(p, v, k)) continue;
+            unsigned long long li = atomicAdd(&p.ctl->log_count, 1u);
+            if (li < p.log_cap) {
+                p.log_v[li] = v;
+                p.log_k[li] = k;
+                p.log_l[li] = c;
+            } else {
+                set_dev_error(p.ctl, DC_DEV_ERR_CAPACITY, 42);
+            }
+        }
+    }
+}
+
+}  // namespace
+
+// Largest deletion batch whose seeds fit a row's table (callers split mixed
+// batches only below it).
+uint32_t row_repair_max_deletions() { return kHashLimit / 4; }
+
+namespace {
+
+// Vertices whose kmax fell (kmax_new < kmax_old), compacted.
+__global__ void k_collect_leave(uint32_t V, const int32_t* kold, const int32_t* knew, uint32_t* out, unsigned* n) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+        if (knew[v] < kold[v]) out[atomicAdd(n, 1u)] = (uint32_t)v;
+}
+
+// Per-vertex change lists from the log: count, fill, sort by k.
+__global__ void k_chg_count(unsigned long long n, const uint32_t* lv, unsigned long long* cnt) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[lv[i]], 1ull);
+}
+__global__ void k_chg_fill(unsigned long long n, const uint32_t* lv, const int32_t* lk, const int32_t* ll,
+                           const unsigned long long* off, uint32_t* fill, int32_t* ck, int32_t* cl) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t v = lv[i];
+        uint64_t o = off[v] + atomicAdd(&fill[v], 1u);
+        ck[o] = lk[i];
+        cl[o] = ll[i];
+    }
+}
+__global__ void k_chg_sort(uint32_t V, const unsigned long long* off, int32_t* ck, int32_t* cl, uint32_t* off32) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t a = off[v], b = off[v + 1];
+        for (uint64_t i = a + 1; i < b; ++i) {
+            int kk = ck[i], ll = cl[i];
+            uint64_t j = i;
+            while (j > a && ck[j - 1] > kk) {
+                ck[j] = ck[j - 1];
+                cl[j] = cl[j - 1];
+                --j;
+            }
+            ck[j] = kk;
+            cl[j] = ll;
+        }
+        off32[v] = (uint32_t)a;
+        if (v == V - 1) off32[V] = (uint32_t)b;
+    }
+}
+
+// New skyline of v: corner (0, new row 0), then at every row k <= new kmax
+// where the old skyline has a corner, the change list has an entry, or a
+// change run ends, the new value (change or old value) when it differs from
+// the previous corner's.  FILL = false counts, true writes.
+template <bool FILL>
+__global__ void k_rep_merge(uint32_t V, const int32_t* kmax, const int32_t* row0, const uint32_t* ooff,
+                            const int32_t* ok, const int32_t* ol, const uint32_t* coff, const int32_t* ck,
+                            const int32_t* cl, unsigned long long* cnt_off, int32_t* nk, int32_t* nl,
+                            uint32_t* noff) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        const int km = kmax[v];
+        uint32_t i = ooff[v], ie = ooff[v + 1];
+        uint32_t j = coff[v], je = coff[v + 1];
+        uint64_t o = FILL ? cnt_off[v] : 0;
+        uint64_t c = 0;
+        int last = row0[v];
+        if (FILL) {
+            nk[o] = 0;
+            nl[o] = last;
+        }
+        ++c;
+        int oldv = (i < ie) ? ol[i] : 0;  // old row-0 corner
+        ++i;
+        int after = 0x7FFFFFFF;  // row after a change run
+        for (;;) {
+            int kc = 0x7FFFFFFF;
+            if (i < ie) kc = min(kc, ok[i]);
+            if (j < je) kc = min(kc, ck[j]);
+            kc = min(kc, after);
+            if (kc > km) break;
+            while (i < ie && ok[i] <= kc) oldv = ol[i++];
+            int val = oldv;
+            after = 0x7FFFFFFF;
+            if (j < je && ck[j] == kc) {
+                val = cl[j++];
+                after = kc + 1;
+            }
+            if (val != last) {
+                if (FILL) {
+                    nk[o + c] = kc;
+                    nl[o + c] = val;
+                }
+                ++c;
+                last = val;
+            }
+        }
+        if (FILL) {
+            noff[v] = (uint32_t)o;
+            if (v == V - 1) noff[V] = (uint32_t)(o + c);
+        } else {
+            cnt_off[v] = c;
+        }
+    }
+}
+
+}  // namespace
+
+static int rgrid(dc_graph* h, uint64_t n) {
+    uint64_t b = (n + kRThreads - 1) / kRThreads;
+    uint64_t cap = (uint64_t)h->geom.sms * 16;
+    return (int)std::max<uint64_t>(1, std::min(b, cap));
+}
+
+#define RP_CUDA(call)                                                                       \
+    do {                                                                                    \
+        cudaError_t _e = (call);                                                            \
+        if (_e != cudaSuccess) {                                                            \
+            cudaGetLastError();                                                             \
+            return set_error(DC_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(_e)); \
+        }                                                                                   \
+    } while (0)
+
+// Rows 1..R after a deletion-only batch (graph, kmax and row 0 already
+// updated; kmax before the batch in scratch kmax_old).  Replaces the skyline
+// and sets *applied; leaves everything untouched with *applied = false when a
+// row touched more vertices than a block's table holds or the change log ran
+// out (the caller then recomputes the rows).
+int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_dv, uint32_t n_del, bool* applied) {
+    *applied = false;
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    if (R < 1 || V == 0) return DC_OK;
+    if (2ull * n_del > kHashLimit) return DC_OK;  // the seeds alone overflow a row's table
+    unsigned* n_leave_d = (unsigned*)s->cursor;
+    RP_CUDA(cudaMemsetAsync(n_leave_d, 0, sizeof(unsigned), h->stream));
+    ++g_launches;
+    k_collect_leave<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, s->kmax_old, d.kmax_v, s->rem0, n_leave_d);
+    unsigned n_leave = 0;
+    RP_CUDA(cudaMemcpyAsync(&n_leave, n_leave_d, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    RP_CUDA(cudaStreamSynchronize(h->stream));
+    if (2ull * n_del + n_leave > kHashLimit) return DC_OK;
+    // change log: the scratch corner log (sized by the last decomposition)
+    uint64_t cap = s->log_cap;
+    if (cap < (1u << 20)) {
+        cudaFreeAsync(s->log_v, h->stream);
+        cudaFreeAsync(s->log_k, h->stream);
+        cudaFreeAsync(s->log_l, h->stream);
+        s->log_v = nullptr;
+        s->log_k = nullptr;
+        s->log_l = nullptr;
+        s->log_cap = 0;
+        cap = 1u << 20;
+        if (cudaMallocAsync((void**)&s->log_v, 4 * cap, h->stream) != cudaSuccess ||
+            cudaMallocAsync((void**)&s->log_k, 4 * cap, h->stream) != cudaSuccess ||
+            cudaMallocAsync((void**)&s->log_l, 4 * cap, h->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(DC_ERR_NOMEM, "row repair: change log allocation failed");
+        }
+        s->log_cap = cap;
+    }
+    RP_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
+    RP_CUDA(cudaStreamSynchronize(h->stream));
+    RepairParams p;
+    p.V = V;
+    p.out_off = g.out_off; p.out_len = g.out_len; p.out_nbr = g.out_nbr;
+    p.in_off = g.in_off; p.in_len = g.in_len; p.in_nbr = g.in_nbr;
+    p.kmax_new = d.kmax_v;
+    p.kmax_old = s->kmax_old;
+    p.sky_off = d.sky_off; p.sky_k = d.sky_k; p.sky_l = d.sky_l;
+    p.del_u = d_du; p.del_v = d_dv; p.n_del = n_del;
+    p.leave = s->rem0; p.n_leave = n_leave;
+    p.R = R;
+    p.log_v = s->log_v; p.log_k = s->log_k; p.log_l = s->log_l; p.log_cap = cap;
+    p.ctl = h->ctl;
+    static_assert(sizeof(RowState) <= 200 * 1024, "row table exceeds shared memory");
+    RP_CUDA(cudaFuncSetAttribute(k_row_repair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RowState)));
+    const int blocks = std::max(1, std::min<int>(R, h->geom.sms));
+    ++g_launches;
+    k_row_repair<<<blocks, kRThreads, sizeof(RowState), h->stream>>>(p);
+    RP_CUDA(cudaGetLastError());
+    EngineCtl hc;
+    RP_CUDA(cudaMemcpyAsync(&hc, h->ctl, sizeof(EngineCtl), cudaMemcpyDeviceToHost, h->stream));
+    RP_CUDA(cudaStreamSynchronize(h->stream));
+    if (hc.error & DC_DEV_ERR_TIMEOUT)
+        return set_error(DC_ERR_TIMEOUT, "row repair: bounded device wait expired (site %u)", hc.err_where);
+    if (hc.error) return DC_OK;  // capacity: the caller recomputes the rows
+    const uint64_t nlog = hc.log_count;
+    // per-vertex change lists
+    unsigned long long* cnt = (unsigned long long*)s->tmp64;
+    uint32_t *coff = nullptr, *fill = s->cursor, *noff = nullptr;
+    int32_t *ck = nullptr, *cl = nullptr, *nk = nullptr, *nl = nullptr;
+    int rc = DC_OK;
+    if (cudaMallocAsync((void**)&coff, 4ull * (V + 1), h->stream) != cudaSuccess ||
+        cudaMallocAsync((void**)&ck, 4ull * (nlog ? nlog : 1), h->stream) != cudaSuccess ||
+        cudaMallocAsync((void**)&cl, 4ull * (nlog ? nlog : 1), h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        rc = set_error(DC_ERR_NOMEM, "row repair: change list allocation failed");
+    }
+    unsigned long long total = 0;
+    if (rc == DC_OK) {
+        cudaMemsetAsync(cnt, 0, 8ull * (V + 1), h->stream);
+        cudaMemsetAsync(fill, 0, 4ull * V, h->stream);
+        g_launches += 3;
+        if (nlog) k_chg_count<<<rgrid(h, nlog), kRThreads, 0, h->stream>>>(nlog, s->log_v, cnt);
+        rc = scan_tmp64(h, V);
+    }
+    if (rc == DC_OK) {
+        if (nlog)
+            k_chg_fill<<<rgrid(h, nlog), kRThreads, 0, h->stream>>>(nlog, s->log_v, s->log_k, s->log_l, cnt, fill, ck,
+                                                                    cl);
+        k_chg_sort<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, cnt, ck, cl, coff);
+        // new skyline: count, scan, fill
+        k_rep_merge<false><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
+                                                                     coff, ck, cl, cnt, nullptr, nullptr, nullptr);
+        rc = scan_tmp64(h, V);
+    }
+    if (rc == DC_OK) {
+        if (cudaMemcpyAsync(&total, cnt + V, sizeof(total), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess) {
+            cudaGetLastError();
+            rc = set_error(DC_ERR_CUDA, "row repair: corner count download failed");
+        }
+    }
+    if (rc == DC_OK && (cudaMallocAsync((void**)&noff, 4ull * (V + 1), h->stream) != cudaSuccess ||
+                        cudaMallocAsync((void**)&nk, 4ull * (total ? total : 1), h->stream) != cudaSuccess ||
+                        cudaMallocAsync((void**)&nl, 4ull * (total ? total : 1), h->stream) != cudaSuccess)) {
+        cudaGetLastError();
+        rc = set_error(DC_ERR_NOMEM, "row repair: skyline allocation failed");
+    }
+    if (rc == DC_OK) {
+        ++g_launches;
+        k_rep_merge<true><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
+                                                                    coff, ck, cl, cnt, nk, nl, noff);
+        if (cudaGetLastError() != cudaSuccess) rc = set_error(DC_ERR_CUDA, "row repair: merge launch failed");
+    }
+    cudaFreeAsync(coff, h->stream);
+    cudaFreeAsync(ck, h->stream);
+    cudaFreeAsync(cl, h->stream);
+    if (rc != DC_OK) {
+        if (noff) cudaFreeAsync(noff, h->stream);
+        if (nk) cudaFreeAsync(nk, h->stream);
+        if (nl) cudaFreeAsync(nl, h->stream);
+        return rc;
+    }
+    cudaFreeAsync(d.sky_off, h->stream);
+    cudaFreeAsync(d.sky_k, h->stream);
+    cudaFreeAsync(d.sky_l, h->stream);
+    d.sky_off = noff;
+    d.sky_k = nk;
+    d.sky_l = nl;
+    d.n_corners = total;
+    d.corner_cap = total;
+    *applied = true;
+    return DC_OK;
+}
+
+}  // namespace dc

@@ -55,7 +55,7 @@ class DecompInfo(ctypes.Structure):
 class MaintStats(ctypes.Structure):
     _fields_ = [("inserted", ctypes.c_uint64), ("deleted", ctypes.c_uint64), ("kmax", ctypes.c_int32),
                 ("lmax", ctypes.c_int32), ("rows_recomputed", ctypes.c_int32), ("method", ctypes.c_int32),
-                ("rebuilt", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("region", ctypes.c_uint64),
+                ("rebuilt", ctypes.c_uint32), ("rows_local", ctypes.c_uint32), ("region", ctypes.c_uint64),
                 ("apply_ms", ctypes.c_float), ("core_ms", ctypes.c_float), ("rows_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float)]
 
@@ -105,6 +105,7 @@ SIGNATURES = {
     "dc_decompose": [vp, ctypes.c_int, i32p, i32p],
     "dc_decompose_rows": [vp, ctypes.c_uint32, ctypes.c_uint32, i32p, i32p],
     "dc_row_weights": [vp, u64p, ctypes.c_uint64],
+    "dc_set_row_repair": [vp, ctypes.c_int],
     "dc_maintain": [vp, u32p, u8p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(MaintStats)],
     "dc_decomp_info_get": [vp, ctypes.POINTER(DecompInfo)],
     "dc_get_kmaxes": [vp, i32p],
@@ -465,7 +466,10 @@ class Graph:
         st = MaintStats()
         _check(lib().dc_maintain(self._h, _p(pairs, u32p), None if dl is None else _p(dl, u8p), len(src), method,
                                  ctypes.byref(st)))
-        return {f: getattr(st, f) for f, _ in MaintStats._fields_ if f != "pad"}
+        return {f: getattr(st, f) for f, _ in MaintStats._fields_}
+
+    def set_row_repair(self, on):
+        _check(lib().dc_set_row_repair(self._h, 1 if on else 0))
 
     def set_scheduler(self, sched):
         _check(lib().dc_graph_set_scheduler(self._h, sched.handle if sched is not None else None))

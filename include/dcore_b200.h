@@ -214,7 +214,7 @@ typedef struct dc_maint_stats {
     int32_t rows_recomputed;    /* rows 0..R recomputed (R + 1); rows above kept      */
     int32_t method;             /* DC_MAINT_LOCAL or DC_MAINT_REPEEL                  */
     uint32_t rebuilt;           /* 1 when the adjacency store grew (slack exhausted)  */
-    uint32_t pad;
+    uint32_t rows_local;        /* 1 when rows were repaired locally (deletions only) */
     uint64_t region;            /* vertices visited by the local kmax / row-0 update  */
     float apply_ms, core_ms, rows_ms, total_ms;
 } dc_maint_stats;
@@ -230,6 +230,14 @@ typedef struct dc_maint_stats {
  * decomposed first.  stats may be NULL. */
 int dc_maintain(dc_graph* g, const uint32_t* pairs, const uint8_t* is_delete, uint64_t b, int method,
                 dc_maint_stats* stats);
+/* Row maintenance mode (default 1).  1: the deletions of a batch are applied
+ * first and rows 1..R are repaired in place from their old values, touching
+ * only the vertices the deletions reach (a row that touches too many falls
+ * back to recomputation); the insertions follow as a second batch whose rows
+ * are recomputed from the new row 0.  0: every batch recomputes rows 1..R
+ * from the new row 0.  Results are identical.  No counterpart in the
+ * reference (it re-peels rows k <= M+1, main.cu:1735-1743). */
+int dc_set_row_repair(dc_graph* g, int on);
 
 /* ---- learned maintenance scheduler -------------------------------------- */
 /* A BF16 MLP (16 -> 64 -> 64 -> 2, ReLU) predicting the log of the wall time

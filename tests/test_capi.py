@@ -108,6 +108,10 @@ def test_update_stream_valid_in_sequence(dc, frac):
     _replay(s, d, u, v, dl)
     if 0 < frac < 1:
         assert abs(1 - dl.mean() - frac) < 0.05
+    if frac == 1.0:
+        assert not dl.any()  # inserts only
+    if frac == 0.0:
+        assert dl.all()  # deletes only
     u2, v2, dl2 = dc.gen_updates(V, s, d, 3000, frac, 7)
     assert np.array_equal(u, u2) and np.array_equal(v, v2) and np.array_equal(dl, dl2)
 

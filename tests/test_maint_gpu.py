@@ -41,13 +41,15 @@ def _check(orc, g, V, cnt):
     assert bad.size == 0, f"{len(bad)} mismatches, first (k, v) = {bad[:5].tolist()}"
 
 
+@pytest.mark.parametrize("repair", [True, False])
 @pytest.mark.parametrize("method", METHODS)
 @pytest.mark.parametrize("scale,seed", [(11, 5), (13, 6)])
-def test_mixed_stream_matches_recompute(dc, orc, gpu, method, scale, seed):
+def test_mixed_stream_matches_recompute(dc, orc, gpu, method, scale, seed, repair):
     V, s, d = dc.gen_rmat(scale, 8, seed)
     u, v, dl = dc.gen_updates(V, s, d, 700, 0.5, seed + 100)
     cnt = Counter(zip(s.tolist(), d.tolist()))
     with dc.Graph.from_edges(V, s, d) as g:
+        g.set_row_repair(repair)
         g.decompose()
         i = 0
         for bs in [1, 1, 2, 5, 20, 100, 571]:
@@ -157,3 +159,45 @@ def test_maintain_before_decompose_and_auto(dc, orc, gpu):
         assert st["method"] in (1, 2)
         _apply(cnt, u, v, dl)
         _check(orc, g, V, cnt)
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("scale,ef,seed", [(12, 16, 21), (14, 8, 22)])
+def test_deletion_stream_local_row_repair(dc, orc, gpu, method, scale, ef, seed):
+    # deletions only: rows are repaired in place from their old values
+    V, s, d = dc.gen_rmat(scale, ef, seed)
+    sizes = [1, 1, 2, 3, 10, 50, 200, 1000]
+    u, v, dl = dc.gen_updates(V, s, d, sum(sizes), 0.0, seed + 7)
+    assert dl.all()
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    local = 0
+    with dc.Graph.from_edges(V, s, d) as g:
+        g.decompose()
+        i = 0
+        for bs in sizes:
+            st = g.maintain(u[i:i + bs], v[i:i + bs], dl[i:i + bs], method)
+            local += st["rows_local"]
+            _apply(cnt, u[i:i + bs], v[i:i + bs], dl[i:i + bs])
+            _check(orc, g, V, cnt)
+            i += bs
+    assert local >= len(sizes) // 2  # the in-place path ran
+
+
+@pytest.mark.parametrize("seed", range(1, 13))
+def test_randomized_deletion_heavy_streams(dc, orc, gpu, seed):
+    # random graphs, batch sizes and methods, mostly deletions: every batch
+    # leaves kmaxes and every row equal to a recomputation
+    rng = np.random.default_rng(seed)
+    V, s, d = dc.gen_rmat(int(rng.integers(10, 14)), int(rng.choice([8, 16])), seed)
+    sizes = [int(x) for x in rng.integers(1, 700, 3)]
+    u, v, dl = dc.gen_updates(V, s, d, sum(sizes), float(rng.choice([0.0, 0.3])), seed + 50)
+    method = int(rng.choice(METHODS))
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    with dc.Graph.from_edges(V, s, d) as g:
+        g.decompose()
+        i = 0
+        for bs in sizes:
+            g.maintain(u[i:i + bs], v[i:i + bs], dl[i:i + bs], method)
+            _apply(cnt, u[i:i + bs], v[i:i + bs], dl[i:i + bs])
+            _check(orc, g, V, cnt)
+            i += bs
