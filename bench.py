@@ -55,7 +55,7 @@ WORKLOADS = {
                          desc="R-MAT scale 22, edge factor 16 + 1e6-op update stream (50% insert / 50% delete)"),
     # serving loop: 64 device-resident graphs, open-loop Poisson arrivals
     "serve-64": dict(serve=True, n_graphs=64, scales=(16, 22), efs=(8, 32), seed=1, budget_gb=150.0,
-                     rate=100.0, requests=1000, sat_rate=2000.0, sat_requests=4000, max_request=10_000,
+                     rate=25.0, requests=500, sat_rate=2000.0, sat_requests=4000, max_request=10_000,
                      insert_frac=0.6, workers=4,
                      desc="64 R-MAT graphs, scale U{16..22}, edge factor U{8..32}; Poisson arrivals of requests "
                           "of log-uniform 1..1e4 updates (60% insert / 40% delete) on uniformly chosen graphs; "

@@ -1883,6 +1883,7 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     // ---- method 0: rows 1..K derived row to row
     uint64_t nlog = 0;
     if (int rc = rows_from_row0(h, K, K, true, &nlog)) return rc;
+    h->full_entries = h->stat_entries;
     if (int rc = build_skyline_from_log(h, nlog)) return rc;
     cudaEventRecord(h->ev[5], h->stream);
     d.valid = true;

@@ -73,6 +73,9 @@ int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_
 // Deletions per batch below which maintenance splits a mixed batch to repair
 // its rows in place.
 uint32_t row_repair_max_deletions();
+// Whether a row repair after deleting these (device) edges is expected to
+// beat recomputing the rows (uses the graph before the deletions).
+bool row_repair_worthwhile(dc_graph* h, const uint32_t* d_u, const uint32_t* d_v, uint32_t n);
 // Maintenance method for a batch (rule of thumb or the learned scheduler).
 int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del);
 

@@ -919,7 +919,15 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
         if (int rc = decompose(h, 0, 0)) return rc;
     NetBatch nb;
     if (int rc = net_batch(V, pairs, is_del, b, nb)) return rc;
-    if (h->row_repair && !nb.del_u.empty() && !nb.ins_u.empty() && nb.del_u.size() <= row_repair_max_deletions()) {
+    bool repair_del = false;  // rows of the deletions repaired in place
+    if (h->row_repair && !nb.del_u.empty() && nb.del_u.size() <= row_repair_max_deletions() && d.kmax_v) {
+        uint32_t *eu = nullptr, *ev = nullptr;
+        if (upload(h, &eu, nb.del_u) == DC_OK && upload(h, &ev, nb.del_v) == DC_OK)
+            repair_del = h->row_repair == 2 || row_repair_worthwhile(h, eu, ev, (uint32_t)nb.del_u.size());
+        mt_free(h->stream, eu);
+        mt_free(h->stream, ev);
+    }
+    if (repair_del && !nb.ins_u.empty()) {
         // deletions first (their rows are repaired in place), then the
         // insertions: the net effect per edge makes the two commute
         std::vector<uint32_t> pd(2 * nb.del_u.size()), pi(2 * nb.ins_u.size());
@@ -1039,7 +1047,7 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
             goto timing;
         }
         // ---- deletions only: repair rows 1..R in place
-        if (h->row_repair && nb.ins_u.empty() && !nb.del_u.empty()) {
+        if (repair_del && nb.ins_u.empty()) {
             bool applied = false;
             if ((rc = rows_repair(h, R, d_du, d_dv, (uint32_t)nb.del_u.size(), &applied))) goto out;
             if (applied) {

@@ -358,6 +358,11 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
         }
         __syncthreads();
         if (S.abort) break;
+        if (sweep == 32) {  // bounded: a row that keeps failing is recomputed
+            if (threadIdx.x == 0) S.abort = 1;
+            __syncthreads();
+            break;
+        }
         // ---- the row is quiet: every touched vertex must hold its value
         // against the final values of its neighbours; queue any that does
         // not and drain again
@@ -421,13 +426,20 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
     }
 }
 
-}  // namespace
-
-// Largest deletion batch whose seeds fit a row's table (callers split mixed
-// batches only below it).
-uint32_t row_repair_max_deletions() { return kHashLimit / 4; }
-
-namespace {
+// Work of a repair: sum over the endpoints x of the deleted edges of
+// deg(x) * kmax(x), the list entries a row-by-row repair scans at least once.
+__global__ void k_repair_work(uint32_t n, const uint32_t* u, const uint32_t* v, const int32_t* kmax,
+                              const int32_t* in_len, const int32_t* out_len, unsigned long long* acc) {
+    unsigned long long w = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t a = u[i], b = v[i];
+        w += (unsigned long long)(in_len[a] + out_len[a]) * (unsigned long long)max(kmax[a], 0);
+        w += (unsigned long long)(in_len[b] + out_len[b]) * (unsigned long long)max(kmax[b], 0);
+    }
+#pragma unroll
+    for (int s = 16; s; s >>= 1) w += __shfl_xor_sync(0xFFFFFFFFu, w, s);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(acc, w);
+}
 
 // Vertices whose kmax fell (kmax_new < kmax_old), compacted.
 __global__ void k_collect_leave(uint32_t V, const int32_t* kold, const int32_t* knew, uint32_t* out, unsigned* n) {
@@ -525,10 +537,35 @@ __global__ void k_rep_merge(uint32_t V, const int32_t* kmax, const int32_t* row0
 
 }  // namespace
 
+
 static int rgrid(dc_graph* h, uint64_t n) {
     uint64_t b = (n + kRThreads - 1) / kRThreads;
     uint64_t cap = (uint64_t)h->geom.sms * 16;
     return (int)std::max<uint64_t>(1, std::min(b, cap));
+}
+
+// Largest deletion batch whose seeds fit a row's table (callers split mixed
+// batches only below it).
+uint32_t row_repair_max_deletions() { return kHashLimit / 4; }
+
+// Whether repairing the rows after deleting these edges (device arrays) is
+// expected to beat recomputing them: the entries the repair scans, times the
+// passes it makes over each (histogram, release, re-check), against the
+// entries the last full row derivation scanned.
+bool row_repair_worthwhile(dc_graph* h, const uint32_t* d_u, const uint32_t* d_v, uint32_t n) {
+    if (n == 0 || 2ull * n > kHashLimit || h->full_entries == 0 || !h->d.kmax_v) return false;
+    unsigned long long* acc = (unsigned long long*)h->scratch->tmp64;
+    if (cudaMemsetAsync(acc, 0, sizeof(unsigned long long), h->stream) != cudaSuccess) return false;
+    ++g_launches;
+    k_repair_work<<<rgrid(h, n), kRThreads, 0, h->stream>>>(n, d_u, d_v, h->d.kmax_v, h->g.in_len, h->g.out_len,
+                                                              acc);
+    unsigned long long w = 0;
+    if (cudaMemcpyAsync(&w, acc, sizeof(w), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return 8ull * w < h->full_entries;
 }
 
 #define RP_CUDA(call)                                                                       \

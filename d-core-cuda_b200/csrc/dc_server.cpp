@@ -80,6 +80,7 @@ struct dc_server {
     uint64_t admissions = 0, evictions = 0, batches = 0;
     int method = DC_MAINT_AUTO;
     int device = 0;
+    int row_repair = 1;
     uint64_t sms = 148;
     bool stop = false;
     dc_graph_opts opts;
@@ -159,6 +160,7 @@ int admit(dc_server* s, GraphSlot& g, std::unique_lock<std::mutex>& lk) {
     lk.unlock();
     dc_graph* h = nullptr;
     int rc = dc_graph_create(g.V, src.size(), src.data(), dst.data(), &s->opts, &h);
+    if (rc == DC_OK) rc = dc_set_row_repair(h, s->row_repair);
     if (rc == DC_OK) rc = dc_decompose(h, DC_METHOD_INCREMENTAL, nullptr, nullptr);
     uint64_t bytes = 0;
     if (rc == DC_OK) dc_graph_device_bytes(h, &bytes);
@@ -405,6 +407,13 @@ extern "C" int dc_server_graph_result(dc_server* s, uint32_t graph_id, int32_t* 
     s->cv_done.notify_all();
     s->cv_work.notify_all();
     return rc;
+}
+
+extern "C" int dc_server_set_row_repair(dc_server* s, int on) {
+    if (!s) return set_error(DC_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->row_repair = on ? 1 : 0;
+    return DC_OK;
 }
 
 extern "C" int dc_server_free(dc_server* s) {

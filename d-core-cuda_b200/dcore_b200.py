@@ -150,6 +150,7 @@ SIGNATURES = {
     "dc_server_info_get": [vp, ctypes.POINTER(ServerInfo)],
     "dc_server_graph_result": [vp, ctypes.c_uint32, i32p, i32p, ctypes.c_uint64, i32p],
     "dc_server_free": [vp],
+    "dc_server_set_row_repair": [vp, ctypes.c_int],
     "dc_kmax_noalloc": [ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp, vp, i32p, vp],
     "dc_launch_count": [u64p],
     "dc_last_error": [],
@@ -468,8 +469,9 @@ class Graph:
                                  ctypes.byref(st)))
         return {f: getattr(st, f) for f, _ in MaintStats._fields_}
 
-    def set_row_repair(self, on):
-        _check(lib().dc_set_row_repair(self._h, 1 if on else 0))
+    def set_row_repair(self, mode):
+        """0 recompute rows, 1 repair deletions in place when worthwhile, 2 always when they fit."""
+        _check(lib().dc_set_row_repair(self._h, int(mode)))
 
     def set_scheduler(self, sched):
         _check(lib().dc_graph_set_scheduler(self._h, sched.handle if sched is not None else None))
@@ -668,6 +670,9 @@ class Server:
 
     def __exit__(self, *a):
         self.free()
+
+    def set_row_repair(self, on):
+        _check(lib().dc_server_set_row_repair(self._h, 1 if on else 0))
 
     def add_graph(self, V, src, dst):
         src = np.ascontiguousarray(src, np.uint32)

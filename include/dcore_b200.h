@@ -230,13 +230,16 @@ typedef struct dc_maint_stats {
  * decomposed first.  stats may be NULL. */
 int dc_maintain(dc_graph* g, const uint32_t* pairs, const uint8_t* is_delete, uint64_t b, int method,
                 dc_maint_stats* stats);
-/* Row maintenance mode (default 1).  1: the deletions of a batch are applied
- * first and rows 1..R are repaired in place from their old values, touching
- * only the vertices the deletions reach (a row that touches too many falls
- * back to recomputation); the insertions follow as a second batch whose rows
- * are recomputed from the new row 0.  0: every batch recomputes rows 1..R
- * from the new row 0.  Results are identical.  No counterpart in the
- * reference (it re-peels rows k <= M+1, main.cu:1735-1743). */
+/* Row maintenance mode (default 1).  Repair: the deletions of a batch are
+ * applied first and rows 1..R are repaired in place from their old values,
+ * touching only the vertices the deletions reach (a row that touches too many
+ * falls back to recomputation); the insertions follow as a second batch whose
+ * rows are recomputed from the new row 0.  1: repair when the batch's
+ * deletions are few and the lists they touch are short enough that the
+ * repair is expected to beat recomputation; 2: repair whenever the deletions
+ * fit; 0: every batch recomputes rows 1..R from the new row 0.  Results are
+ * identical.  No counterpart in the reference (it re-peels rows k <= M+1,
+ * main.cu:1735-1743). */
 int dc_set_row_repair(dc_graph* g, int on);
 
 /* ---- learned maintenance scheduler -------------------------------------- */
@@ -347,6 +350,9 @@ int dc_server_info_get(dc_server* s, dc_server_info* info);
 int dc_server_graph_result(dc_server* s, uint32_t graph_id, int32_t* kmaxes, int32_t* rows, uint64_t rows_capacity,
                            int32_t* kmax);
 int dc_server_free(dc_server* s);
+/* Row maintenance mode (dc_set_row_repair) of the graphs this server builds
+ * from now on (default 1). */
+int dc_server_set_row_repair(dc_server* s, int on);
 
 /* ---- diagnostics ------------------------------------------------------- */
 /* Per-step timing of the persistent kernels: after each kernel, fn is called

@@ -41,7 +41,7 @@ def _check(orc, g, V, cnt):
     assert bad.size == 0, f"{len(bad)} mismatches, first (k, v) = {bad[:5].tolist()}"
 
 
-@pytest.mark.parametrize("repair", [True, False])
+@pytest.mark.parametrize("repair", [2, 1, 0])
 @pytest.mark.parametrize("method", METHODS)
 @pytest.mark.parametrize("scale,seed", [(11, 5), (13, 6)])
 def test_mixed_stream_matches_recompute(dc, orc, gpu, method, scale, seed, repair):
@@ -172,6 +172,7 @@ def test_deletion_stream_local_row_repair(dc, orc, gpu, method, scale, ef, seed)
     cnt = Counter(zip(s.tolist(), d.tolist()))
     local = 0
     with dc.Graph.from_edges(V, s, d) as g:
+        g.set_row_repair(2)  # in place whenever the deletions fit
         g.decompose()
         i = 0
         for bs in sizes:
