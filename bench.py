@@ -47,10 +47,11 @@ WORKLOADS = {
     "decomp-er10k": dict(gen="er", n=10_000, m=100_000, seed=1, desc="directed G(n=10000, m=100000)"),
     # maintenance: R-MAT graph + stream of 50% inserts of absent edges and 50%
     # deletes of present edges, valid in sequence, in several batch sizes
-    "maint-rmat24": dict(gen="rmat", scale=24, ef=16, seed=1, ops=1_000_000, maint=True,
+    # (20 batches of 1, 100 and 10,000 updates, then one of 1,000,000)
+    "maint-rmat24": dict(gen="rmat", scale=24, ef=16, seed=1, ops=1_202_020, maint=True,
                          sizes=[(1, 20), (100, 20), (10_000, 20), (1_000_000, 1)],
                          desc="R-MAT scale 24, edge factor 16 + 1e6-op update stream (50% insert / 50% delete)"),
-    "maint-rmat22": dict(gen="rmat", scale=22, ef=16, seed=1, ops=1_000_000, maint=True,
+    "maint-rmat22": dict(gen="rmat", scale=22, ef=16, seed=1, ops=1_202_020, maint=True,
                          sizes=[(1, 20), (100, 20), (10_000, 20), (1_000_000, 1)],
                          desc="R-MAT scale 22, edge factor 16 + 1e6-op update stream (50% insert / 50% delete)"),
     # serving loop: 64 device-resident graphs, open-loop Poisson arrivals
