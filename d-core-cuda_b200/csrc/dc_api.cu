@@ -555,7 +555,7 @@ extern "C" int dc_autotune(dc_graph* h, dc_tuning* best, float* best_ms) {
     if (int rc = decompose_range(h, 0, 0)) return rc;  // warm-up
     float peel_best = 1e30f;
     dc_tuning pick = cur;
-    for (int bps = 1; bps <= 4; ++bps)
+    for (int bps = 1; bps <= 6; ++bps)
         for (int chunk = 32; chunk <= 256; chunk *= 2) {
             dc_tuning t = pick;
             t.peel_blocks_per_sm = bps;
@@ -576,7 +576,7 @@ extern "C" int dc_autotune(dc_graph* h, dc_tuning* best, float* best_ms) {
     if (int rc = decompose_range(h, 0, 0)) return rc;
     float rows_best = 1e30f;
     const int32_t K = h->d.kmax;
-    for (int bps = 1; bps <= 4; ++bps) {
+    for (int bps = 1; bps <= 8; ++bps) {
         dc_tuning t = pick;
         t.rows_blocks_per_sm = bps;
         dc_set_tuning(h, &t);

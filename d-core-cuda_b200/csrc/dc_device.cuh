@@ -22,14 +22,20 @@ constexpr unsigned DC_DEV_ERR_NOTFOUND = 16u; // delete of an absent edge
 constexpr uint32_t kEmptySlot = 0xFFFFFFFFu;
 constexpr unsigned long long kWaitNs = 4000000000ull;  // 4 s per wait
 
+// The counters every warp hits (ticket head and tail, the outstanding count,
+// the barrier) and the flags idle warps poll (phase_done, error) each sit in
+// a 128-byte line of their own: on one line they all land in one L2 slice,
+// which then serialises the grid.
 struct EngineCtl {
     // grid barrier
-    unsigned bar_count;
+    alignas(128) unsigned bar_count;
     unsigned bar_gen;
-    unsigned error;
+    // polled by idle warps
+    alignas(128) unsigned error;
     unsigned err_where;
+    unsigned phase_done;    // set by whoever brings outstanding to 0
     // work queue (monotone within one phase)
-    unsigned q_head;
+    alignas(128) unsigned q_head;
     unsigned q_tail;
     unsigned q_done;
     unsigned pad0;
@@ -39,18 +45,17 @@ struct EngineCtl {
     // results / statistics
     int maxval;
     int steps;
-    unsigned log_count;
+    alignas(128) unsigned log_count;
     unsigned pad1;
     unsigned long long evals;
     unsigned long long drops;
     unsigned long long pushes;
     unsigned long long edges_scanned;
     // ticket queue (see TicketQueue)
-    unsigned t_head;        // next ticket
-    unsigned t_tail;        // next slot to reserve
-    int outstanding;        // unfinished producers + pushed, unfinished items
-    unsigned phase_done;    // set by whoever brings outstanding to 0
-    unsigned rc_cur[2];     // remaining-list sizes per peel instance
+    alignas(128) unsigned t_head;  // next ticket
+    alignas(128) unsigned t_tail;  // next slot to reserve
+    alignas(128) int outstanding;  // unfinished producers + pushed, unfinished items
+    alignas(128) unsigned rc_cur[2];  // remaining-list sizes per peel instance
     unsigned rc_next[2];
     int maxv[2];            // largest value per peel instance
     int step;               // level / transition index
@@ -390,7 +395,8 @@ __device__ __forceinline__ bool tq_take_warp(EngineCtl* c, TicketQueue q, unsign
                 state = 1;
                 break;
             }
-            if (ld_vol(&c->phase_done) || ld_vol(&c->error)) {
+            // the shared flags are polled every 4th spin once the wait is long
+            if ((spins < 16 || (spins & 3) == 0) && (ld_vol(&c->phase_done) || ld_vol(&c->error))) {
                 // abandon the ticket: the phase-ending barrier skips it
                 *ticket = kNoTicket;
                 state = 2;

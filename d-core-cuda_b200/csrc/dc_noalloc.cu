@@ -33,7 +33,7 @@ constexpr uint64_t kNaRingSlots = 1ull << 20;
 constexpr int kNaThreads = 256;
 
 // byte layout of the scratch array
-constexpr size_t kNaCtlBytes = 256;
+constexpr size_t kNaCtlBytes = 2048;
 constexpr size_t kNaKeyOff = kNaCtlBytes;
 constexpr size_t kNaRem0Off = kNaKeyOff + 4ull * kNaMaxV;
 constexpr size_t kNaRem1Off = kNaRem0Off + 4ull * kNaMaxV;

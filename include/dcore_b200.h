@@ -379,8 +379,9 @@ typedef struct dc_tuning {
 int dc_get_tuning(dc_graph* g, dc_tuning* t);
 int dc_set_tuning(dc_graph* g, const dc_tuning* t);
 /* Autotuner: times the decomposition of this graph under candidate launch
- * shapes (peel grid and chunk on the peel alone, then the row kernel's grid
- * on the rows alone, each candidate twice), keeps the fastest on the handle
+ * shapes (peel grid 1..6 blocks per SM x chunk 32..256 on the peel alone,
+ * then the row kernel's grid 1..8 blocks per SM on the rows alone, each
+ * candidate twice, grids capped by occupancy), keeps the fastest on the handle
  * and ends with a full decomposition.  *best / *best_ms (may be NULL): the
  * chosen setting and its peel + rows device time. */
 int dc_autotune(dc_graph* g, dc_tuning* best, float* best_ms);

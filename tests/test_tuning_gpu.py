@@ -35,7 +35,7 @@ def test_autotune(dc, orc, gpu):
     okm, olm, okmaxes, orows = orc.dcore(V, s, d)
     with dc.Graph.from_edges(V, s, d) as g:
         best, ms = g.autotune()
-        assert 1 <= best["peel_blocks_per_sm"] <= 4 and 1 <= best["rows_blocks_per_sm"] <= 4
+        assert 1 <= best["peel_blocks_per_sm"] <= 6 and 1 <= best["rows_blocks_per_sm"] <= 8
         assert best["peel_chunk"] in (32, 64, 128, 256)
         assert ms > 0
         assert g.tuning() == best
