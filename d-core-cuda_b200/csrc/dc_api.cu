@@ -521,7 +521,7 @@ extern "C" int dc_set_launch(dc_graph* h, int blocks_per_sm) {
 
 extern "C" int dc_get_tuning(dc_graph* h, dc_tuning* t) {
     if (!h || !t) return set_error(DC_ERR_INVALID, "null argument");
-    const int dflt = h->blocks_per_sm > 0 ? h->blocks_per_sm : 1;
+    const int dflt = h->blocks_per_sm > 0 ? h->blocks_per_sm : 2;
     t->peel_blocks_per_sm = h->peel_bps > 0 ? h->peel_bps : dflt;
     t->rows_blocks_per_sm = h->rows_bps > 0 ? h->rows_bps : dflt;
     t->peel_chunk = (int32_t)h->peel_chunk;

@@ -1481,12 +1481,16 @@ int ensure_tring(dc_graph* h, uint64_t need) {
     return DC_OK;
 }
 
+// Two 256-thread blocks per SM: measured best or near it from R-MAT 19 to 22
+// once the queue counters sit on separate lines (the autotuner refines it).
+static constexpr int kDefaultBlocksPerSm = 2;
+
 static int persistent_grid(dc_graph* h, const void* fn, int bps, int* blocks) {
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0);
     if (e != cudaSuccess || per_sm < 1)
         return set_error(DC_ERR_CUDA, "occupancy query failed (%s)", cudaGetErrorString(e));
-    if (bps <= 0) bps = h->blocks_per_sm > 0 ? h->blocks_per_sm : 1;
+    if (bps <= 0) bps = h->blocks_per_sm > 0 ? h->blocks_per_sm : kDefaultBlocksPerSm;
     per_sm = std::min(per_sm, bps);
     *blocks = per_sm * h->geom.sms;
     return DC_OK;

@@ -104,7 +104,7 @@ int coop_launch(dc_graph* h, const void* fn, void** args, int threads, const cha
 
 // Shared host helpers of the engine (dc_engine.cu).
 int ensure_tring(dc_graph* h, uint64_t need);
-// bps: blocks per SM for this kernel (0 = the handle's blocks_per_sm, else 1).
+// bps: blocks per SM for this kernel (0 = the handle's blocks_per_sm, else 2).
 int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out, int bps = 0);
 int check_ctl(dc_graph* h, EngineCtl* hc, const char* what);
 int scan_tmp64(dc_graph* h, uint64_t n);

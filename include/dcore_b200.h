@@ -363,7 +363,8 @@ int dc_server_set_row_repair(dc_server* s, int on);
  * tracing off. */
 typedef void (*dc_trace_fn)(const char* phase, const unsigned long long* rec, unsigned steps, void* user);
 int dc_set_trace(dc_graph* g, uint32_t max_steps, dc_trace_fn fn, void* user);
-/* Persistent-kernel blocks per SM (0 = default). */
+/* Persistent-kernel blocks per SM for every persistent kernel (0 = the
+ * default, 2; dc_set_tuning sets the peel and row kernels separately). */
 int dc_set_launch(dc_graph* g, int blocks_per_sm);
 
 /* Launch shapes of the persistent kernels: blocks per SM of the fused peel
