@@ -527,42 +527,65 @@ __global__ void k_counters_init(uint32_t V, const uint32_t* out_off, const int32
     }
 }
 
-// One histogram pass over the C_j prefix of a kmax-sorted neighbour list for
-// the window [lo, hi]; values above hi land in bin hi only on the first
-// window (hi == cap).  Four entries per lane per step; the pass stops after
-// a step whose last entry has left C_j (value -1), since every later entry
-// has a kmax no larger.
-__device__ __forceinline__ int hist_pass(const int32_t* cur, const uint32_t* a, int n, int lo, int hi, bool first,
-                                         bool sorted, int* bins) {
+// One histogram pass over the C_j prefixes of a vertex's out-list and
+// in-list together (both lists' loads in flight at once) for the window
+// [lo, hi]; values above hi land in bin hi only on the first window
+// (hi == cap).  Two entries per lane per list per step; on kmax-sorted lists
+// a list stops at its first neighbour outside C_j.  Returns the entries read.
+__device__ __forceinline__ int hist_pass2(const int32_t* cur, const uint32_t* ao, int no, const uint32_t* ai, int ni,
+                                          int lo, int hi, bool first, bool sorted, int* bo, int* bi) {
     const unsigned lane = threadIdx.x & 31u;
-    int b = 0;
-    for (; b < n; b += 128) {
-        int cu[4];
+    int to = 0, ti = 0, entries = 0;
+    bool doneo = no <= 0, donei = ni <= 0;
+    for (int b = 0; !(doneo && donei); b += 64) {
+        uint32_t eo[2], ei[2];
+        bool vo[2], vi[2];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            int e = b + r * 32 + (int)lane;
-            cu[r] = e < n ? ld_vol(&cur[a[e]]) : -1;
+        for (int r = 0; r < 2; ++r) {
+            const int e = b + r * 32 + (int)lane;
+            vo[r] = !doneo && e < no;
+            vi[r] = !donei && e < ni;
+            eo[r] = vo[r] ? ao[e] : 0u;
+            ei[r] = vi[r] ? ai[e] : 0u;
+        }
+        int co[2], ci[2];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            co[r] = vo[r] ? ld_vol(&cur[eo[r]]) : -1;
+            ci[r] = vi[r] ? ld_vol(&cur[ei[r]]) : -1;
         }
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            int x = cu[r];
-            if (x >= lo) {
-                if (x >= hi) {
-                    if (first || x == hi) atomicAdd(&bins[hi - lo], 1);
-                } else {
-                    atomicAdd(&bins[x - lo], 1);
-                }
-            }
+        for (int r = 0; r < 2; ++r) {
+            int x = co[r];
+            to += first ? (x >= hi) : (x == hi);
+            if (x >= lo && x < hi) atomicAdd(&bo[x - lo], 1);
+            x = ci[r];
+            ti += first ? (x >= hi) : (x == hi);
+            if (x >= lo && x < hi) atomicAdd(&bi[x - lo], 1);
         }
-        int last = min(b + 127, n - 1) - b;
-        int rr = last >> 5;
-        int mine = rr == 0 ? cu[0] : rr == 1 ? cu[1] : rr == 2 ? cu[2] : cu[3];
-        if (sorted && __shfl_sync(0xFFFFFFFFu, mine, last & 31) == -1) {
-            b += 128;
-            break;
+        // a list ends at its length, or (sorted by neighbour kmax) at the
+        // first neighbour outside C_j
+        const int lasto = __shfl_sync(0xFFFFFFFFu, co[1], 31);
+        const int lasti = __shfl_sync(0xFFFFFFFFu, ci[1], 31);
+        if (!doneo) {
+            entries += min(64, no - b);
+            if (b + 64 >= no || (sorted && lasto == -1)) doneo = true;
+        }
+        if (!donei) {
+            entries += min(64, ni - b);
+            if (b + 64 >= ni || (sorted && lasti == -1)) donei = true;
         }
     }
-    return min(b, n);
+#pragma unroll
+    for (int s = 16; s; s >>= 1) {
+        to += __shfl_xor_sync(0xFFFFFFFFu, to, s);
+        ti += __shfl_xor_sync(0xFFFFFFFFu, ti, s);
+    }
+    if (lane == 0) {
+        if (to) atomicAdd(&bo[hi - lo], to);
+        if (ti) atomicAdd(&bi[hi - lo], ti);
+    }
+    return entries;
 }
 
 // After x dropped from cap to nv (value already written): counts the
@@ -752,8 +775,8 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
                 hi_[lane] = 0;
                 hi_[lane + 32] = 0;
                 __syncwarp();
-                my_entries += hist_pass(p.cur, p.out_nbr + oo, p.out_len[x], lo, hi, first, p.sorted != 0, ho);
-                my_entries += hist_pass(p.cur, p.in_nbr + io, p.in_len[x], lo, hi, first, p.sorted != 0, hi_);
+                my_entries += hist_pass2(p.cur, p.out_nbr + oo, p.out_len[x], p.in_nbr + io, p.in_len[x], lo, hi, first,
+                                         p.sorted != 0, ho, hi_);
                 __syncwarp();
                 int b0 = 2 * lane, b1 = 2 * lane + 1;
                 int o0 = ho[b0], o1 = ho[b1], i0 = hi_[b0], i1 = hi_[b1];
