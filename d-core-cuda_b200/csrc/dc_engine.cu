@@ -593,7 +593,7 @@ __device__ __forceinline__ int hist_pass2(const int32_t* cur, const uint32_t* ao
 // takes x's support away from neighbours whose level lies in (nv, cap]:
 // out-neighbours lose one unit of cnt_in (unstable below j), in-neighbours
 // one unit of cnt_out (unstable below their own value).  Four entries per
-// lane per step; stops like hist_pass on kmax-sorted lists.  Returns the
+// lane per step; stops like hist_pass2 on kmax-sorted lists.  Returns the
 // entries read.
 __device__ __forceinline__ int recount_pass(const Trans2Params& p, EngineCtl* c, const uint32_t* a, int n, int nv,
                                             int cap, int j, bool out_list, int* cnt) {
