@@ -22,6 +22,14 @@ constexpr unsigned DC_DEV_ERR_NOTFOUND = 16u; // delete of an absent edge
 constexpr uint32_t kEmptySlot = 0xFFFFFFFFu;
 constexpr unsigned long long kWaitNs = 4000000000ull;  // 4 s per wait
 
+// A counter on a 128-byte line of its own.
+struct alignas(128) PadU {
+    unsigned v;
+};
+struct alignas(128) PadI {
+    int v;
+};
+
 // The counters every warp hits (ticket head and tail, the outstanding count,
 // the barrier) and the flags idle warps poll (phase_done, error) each sit in
 // a 128-byte line of their own: on one line they all land in one L2 slice,
@@ -56,13 +64,13 @@ struct EngineCtl {
     alignas(128) unsigned t_tail;  // next slot to reserve
     alignas(128) int outstanding;  // unfinished producers + pushed, unfinished items
     alignas(128) unsigned rc_cur[2];  // remaining-list sizes per peel instance
-    unsigned rc_next[2];
+    PadU rc_next[2];        // next level's remaining-list sizes (appended by every warp)
     int maxv[2];            // largest value per peel instance
     int step;               // level / transition index
     unsigned nworkers;      // producers per phase (warps in the grid)
     int level;              // current level / row of the persistent loop
     int next_min;           // smallest level / row a skipped step may jump to
-    int minkey[2];          // per peel instance: least peeling degree kept by the scan
+    PadI minkey[2];         // per peel instance: least peeling degree kept by the scan
     // optional per-step timing trace: 8 words per step
     //   [0] %globaltimer at step start, [1] when its work ran out,
     //   [2] queue items of the step, [3] %globaltimer at the closing barrier,

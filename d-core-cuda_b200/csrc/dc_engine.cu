@@ -288,15 +288,15 @@ struct PeelHook {
         } else if (c->t_tail == c->trace_tail0) {
             int m = 0x7FFFFFFF;
             for (int i = 0; i < ninst; ++i)
-                if (c->rc_next[i]) m = min(m, c->minkey[i]);
+                if (c->rc_next[i].v) m = min(m, c->minkey[i].v);
             c->level = max(c->level + 1, m == 0x7FFFFFFF ? c->level + 1 : m);
         } else {
             c->level = c->level + 1;
         }
         for (int i = 0; i < ninst; ++i) {
-            c->rc_cur[i] = c->rc_next[i];
-            c->rc_next[i] = 0;
-            c->minkey[i] = 0x7FFFFFFF;
+            c->rc_cur[i] = c->rc_next[i].v;
+            c->rc_next[i].v = 0;
+            c->minkey[i].v = 0x7FFFFFFF;
         }
         trace_step_end(c);
         c->t_tail = c->t_head;
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
                     I.cdeg[v] = cd;
                 }
             }
-            unsigned pos = warp_append(&c->rc_next[i], ok && in);
+            unsigned pos = warp_append(&c->rc_next[i].v, ok && in);
             if (ok && in) I.rem0[pos] = v;
         }
     }
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
                         kmin = min(kmin, kv);
                     }
                 }
-                unsigned pos = warp_append(&c->rc_next[i], keep);
+                unsigned pos = warp_append(&c->rc_next[i].v, keep);
                 if (keep) rn[pos] = v;
                 unsigned cnt = push ? peel_nitems(I, v, CH) : 0u;
                 tq_push_warp_multi(c, p.q, cnt, peel_item(v, 0, i), 1ull << 32);
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
             }
 #pragma unroll
             for (int s = 16; s; s >>= 1) kmin = min(kmin, __shfl_xor_sync(0xFFFFFFFFu, kmin, s));
-            if (lane == 0 && kmin != 0x7FFFFFFF) atomicMin(&c->minkey[i], kmin);
+            if (lane == 0 && kmin != 0x7FFFFFFF) atomicMin(&c->minkey[i].v, kmin);
         }
         block_producer_done(c, &s_prod);
         // ---- drain the cascade
@@ -1025,9 +1025,21 @@ __global__ void k_sort_big(const uint32_t* off, const int32_t* len, uint32_t* nb
 // ---------------------------------------------------------------------------
 // order by kmax, skyline assembly, expansion
 // ---------------------------------------------------------------------------
-__global__ void k_kmax_hist(uint32_t V, const int32_t* kmax, uint32_t* hist) {
+// Counts per kmax value.  Most vertices share a few small values, so the
+// counts go to per-block shared bins first (when kmax + 1 <= kHistShared).
+constexpr int kHistShared = 8192;
+__global__ void k_kmax_hist(uint32_t V, const int32_t* kmax, uint32_t* hist, int32_t K) {
+    extern __shared__ uint32_t sh[];
+    const bool shared = K + 1 <= kHistShared;
+    if (shared)
+        for (int i = threadIdx.x; i <= K; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
-        atomicAdd(&hist[kmax[v]], 1u);
+        atomicAdd(shared ? &sh[kmax[v]] : &hist[kmax[v]], 1u);
+    __syncthreads();
+    if (shared)
+        for (int i = threadIdx.x; i <= K; i += blockDim.x)
+            if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
 // w[k] += in + out degree of every vertex with kmax == k (shared-memory
@@ -1051,10 +1063,21 @@ __global__ void k_kmax_degree_hist(uint32_t V, const int32_t* kmax, const int32_
 }
 
 // cursor[k] = first position of bucket k in descending-kmax order
+// Warp-aggregated: lanes holding the same kmax take their positions with one
+// atomic (the leader's) instead of one each.
 __global__ void k_order_scatter(uint32_t V, const int32_t* kmax, uint32_t* cursor, uint32_t* order) {
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t p = atomicAdd(&cursor[kmax[v]], 1u);
-        order[p] = (uint32_t)v;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x) & ~31ull; base < V; base += stride) {
+        const uint64_t v = base + (threadIdx.x & ~31u) % blockDim.x + lane;
+        const bool ok = v < V;
+        const int key = ok ? kmax[v] : -1;
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+        const unsigned leader = __ffs(peers) - 1;
+        unsigned p0 = 0;
+        if (ok && lane == leader) p0 = atomicAdd(&cursor[key], (unsigned)__popc(peers));
+        p0 = __shfl_sync(0xFFFFFFFFu, p0, leader);
+        if (ok) order[p0 + __popc(peers & ((1u << lane) - 1u))] = (uint32_t)v;
     }
 }
 
@@ -1738,7 +1761,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     uint32_t* hist = s->cursor;
     DC_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * ((uint64_t)K + 2), h->stream));
     ++g_launches;
-    k_kmax_hist<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist);
+    k_kmax_hist<<<grid_for(h, V), kThreads, K + 1 <= kHistShared ? 4 * (K + 1) : 0, h->stream>>>(V, d.kmax_v, hist, K);
     std::vector<uint32_t> hh((size_t)K + 2), ck((size_t)K + 2), start((size_t)K + 2);
     DC_CUDA(cudaMemcpyAsync(hh.data(), hist, sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyDeviceToHost, h->stream));
     unsigned long long* acc = (unsigned long long*)s->tmp64;

@@ -60,8 +60,8 @@ struct NaParams {
 struct NaHook {
     unsigned nworkers;
     __device__ void operator()(EngineCtl* c) const {
-        c->rc_cur[0] = c->rc_next[0];
-        c->rc_next[0] = 0;
+        c->rc_cur[0] = c->rc_next[0].v;
+        c->rc_next[0].v = 0;
         c->t_tail = c->t_head;
         c->outstanding = (int)nworkers;
         c->phase_done = 0;
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kNaThreads) k_kmax_noalloc(NaParams p) {
             p.kmax[v] = -1;
             p.key[v] = (int)(p.in_off[v + 1] - p.in_off[v]);
         }
-        unsigned pos = warp_append(&c->rc_next[0], ok);
+        unsigned pos = warp_append(&c->rc_next[0].v, ok);
         if (ok) p.rem0[pos] = v;
     }
     if (!grid_sync_hook(c, hook)) return;
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kNaThreads) k_kmax_noalloc(NaParams p) {
                 else
                     keep = true;
             }
-            unsigned pos = warp_append(&c->rc_next[0], keep);
+            unsigned pos = warp_append(&c->rc_next[0].v, keep);
             if (keep) rn[pos] = v;
             unsigned cnt = push ? na_items(p, v) : 0u;
             tq_push_warp_multi(c, p.q, cnt, (unsigned long long)v, 1ull << 32);
