@@ -283,125 +283,125 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
             }
         }
         for (int sweep = 0;; ++sweep) {
-        __syncthreads();
-        if (threadIdx.x == 0) atomicSub(&S.out, 1);
-        __syncthreads();
-        // ---- drain
-        unsigned slot;
-        while (r_take(p, S, &slot)) {
-            const uint32_t x = vldu(&S.key[slot]);
-            int cap = vld(&S.cur[slot]);
-            if (cap == kUnset) cap = sky_at(p, x, k);
-            int nv = cap;
-            if (cap >= 1 && p.kmax_new[x] >= k) {
-                const uint32_t* ao = p.out_nbr + p.out_off[x];
-                const uint32_t* ai = p.in_nbr + p.in_off[x];
-                const int no = p.out_len[x], ni = p.in_len[x];
-                int carry_o = 0, carry_i = 0, hi = cap;
-                bool first = true;
-                for (;;) {
-                    const int lo = max(0, hi - (kRWin - 1));
-                    ho[lane] = 0;
-                    ho[lane + 32] = 0;
-                    hi_[lane] = 0;
-                    hi_[lane + 32] = 0;
-                    __syncwarp();
-                    r_hist(p, S, ao, no, k, lo, hi, first, ho);
-                    r_hist(p, S, ai, ni, k, lo, hi, first, hi_);
-                    __syncwarp();
-                    int found = -1;
-                    if (lane == 0) {
-                        for (int L = hi; L >= lo; --L) {
-                            carry_o += ho[L - lo];
-                            carry_i += hi_[L - lo];
-                            if (carry_o >= L && carry_i >= k) {
-                                found = L;
-                                break;
+            __syncthreads();
+            if (threadIdx.x == 0) atomicSub(&S.out, 1);
+            __syncthreads();
+            // ---- drain
+            unsigned slot;
+            while (r_take(p, S, &slot)) {
+                const uint32_t x = vldu(&S.key[slot]);
+                int cap = vld(&S.cur[slot]);
+                if (cap == kUnset) cap = sky_at(p, x, k);
+                int nv = cap;
+                if (cap >= 1 && p.kmax_new[x] >= k) {
+                    const uint32_t* ao = p.out_nbr + p.out_off[x];
+                    const uint32_t* ai = p.in_nbr + p.in_off[x];
+                    const int no = p.out_len[x], ni = p.in_len[x];
+                    int carry_o = 0, carry_i = 0, hi = cap;
+                    bool first = true;
+                    for (;;) {
+                        const int lo = max(0, hi - (kRWin - 1));
+                        ho[lane] = 0;
+                        ho[lane + 32] = 0;
+                        hi_[lane] = 0;
+                        hi_[lane + 32] = 0;
+                        __syncwarp();
+                        r_hist(p, S, ao, no, k, lo, hi, first, ho);
+                        r_hist(p, S, ai, ni, k, lo, hi, first, hi_);
+                        __syncwarp();
+                        int found = -1;
+                        if (lane == 0) {
+                            for (int L = hi; L >= lo; --L) {
+                                carry_o += ho[L - lo];
+                                carry_i += hi_[L - lo];
+                                if (carry_o >= L && carry_i >= k) {
+                                    found = L;
+                                    break;
+                                }
                             }
                         }
+                        found = __shfl_sync(0xFFFFFFFFu, found, 0);
+                        carry_o = __shfl_sync(0xFFFFFFFFu, carry_o, 0);
+                        carry_i = __shfl_sync(0xFFFFFFFFu, carry_i, 0);
+                        __syncwarp();
+                        if (found >= 0) {
+                            nv = found;
+                            break;
+                        }
+                        if (lo == 0) {  // a member keeps at least 0
+                            nv = 0;
+                            break;
+                        }
+                        hi = lo - 1;
+                        first = false;
                     }
-                    found = __shfl_sync(0xFFFFFFFFu, found, 0);
-                    carry_o = __shfl_sync(0xFFFFFFFFu, carry_o, 0);
-                    carry_i = __shfl_sync(0xFFFFFFFFu, carry_i, 0);
-                    __syncwarp();
-                    if (found >= 0) {
-                        nv = found;
-                        break;
+                    if (nv < cap) {
+                        if (lane == 0) atomicExch(&S.cur[slot], nv);
+                        __syncwarp();
+                        __threadfence_block();
+                        const int so = r_release(p, S, ao, no, k, nv, cap);
+                        const int si = r_release(p, S, ai, ni, k, nv, cap);
+                        // a neighbour fell below nv meanwhile: evaluate x again
+                        if (lane == 0 && nv >= 1 && (so < nv || si < k)) atomicCAS(&S.st[slot], 1u, 2u);
                     }
-                    if (lo == 0) {  // a member keeps at least 0
-                        nv = 0;
-                        break;
-                    }
-                    hi = lo - 1;
-                    first = false;
                 }
-                if (nv < cap) {
-                    if (lane == 0) atomicExch(&S.cur[slot], nv);
-                    __syncwarp();
+                __syncwarp();
+                if (lane == 0) {
+                    if (atomicCAS(&S.st[slot], 1u, 0u) == 2u) {
+                        atomicExch(&S.st[slot], 1u);
+                        enqueue(S, slot);
+                    }
                     __threadfence_block();
-                    const int so = r_release(p, S, ao, no, k, nv, cap);
-                    const int si = r_release(p, S, ai, ni, k, nv, cap);
-                    // a neighbour fell below nv meanwhile: evaluate x again
-                    if (lane == 0 && nv >= 1 && (so < nv || si < k)) atomicCAS(&S.st[slot], 1u, 2u);
+                    atomicSub(&S.out, 1);
+                }
+                __syncwarp();
+            }
+            __syncthreads();
+            if (S.abort) break;
+            if (sweep == 32) {  // bounded: a row that keeps failing is recomputed
+                if (threadIdx.x == 0) S.abort = 1;
+                __syncthreads();
+                break;
+            }
+            // ---- the row is quiet: every touched vertex must hold its value
+            // against the final values of its neighbours; queue any that does
+            // not and drain again
+            if (threadIdx.x == 0) {
+                S.qhead = S.qtail = 0;
+                S.out = 1;  // held by the sweep
+                S.k = 0;    // vertices found unstable
+            }
+            for (int i = threadIdx.x; i < kHash; i += kRThreads) S.ring[i] = kEmptySlot;
+            __syncthreads();
+            for (int i = wib; i < kHash; i += kRWarps) {
+                const uint32_t x = S.key[i];
+                if (x == kEmptyKey || p.kmax_new[x] < k) continue;
+                int val = S.cur[i];
+                if (val == kUnset) val = sky_at(p, x, k);
+                if (val < 1) continue;
+                int so = 0, si = 0;
+                const uint32_t* ao = p.out_nbr + p.out_off[x];
+                const uint32_t* ai = p.in_nbr + p.in_off[x];
+                for (int e = (int)lane; e < p.out_len[x]; e += 32) so += rv(p, S, ao[e], k) >= val;
+                for (int e = (int)lane; e < p.in_len[x]; e += 32) si += rv(p, S, ai[e], k) >= val;
+    #pragma unroll
+                for (int s = 16; s; s >>= 1) {
+                    so += __shfl_xor_sync(0xFFFFFFFFu, so, s);
+                    si += __shfl_xor_sync(0xFFFFFFFFu, si, s);
+                }
+                if (lane == 0 && (so < val || si < k)) {
+                    atomicAdd(&S.k, 1);
+                    push(S, x);
                 }
             }
-            __syncwarp();
-            if (lane == 0) {
-                if (atomicCAS(&S.st[slot], 1u, 0u) == 2u) {
-                    atomicExch(&S.st[slot], 1u);
-                    enqueue(S, slot);
-                }
-                __threadfence_block();
-                atomicSub(&S.out, 1);
-            }
-            __syncwarp();
-        }
-        __syncthreads();
-        if (S.abort) break;
-        if (sweep == 32) {  // bounded: a row that keeps failing is recomputed
-            if (threadIdx.x == 0) S.abort = 1;
             __syncthreads();
-            break;
-        }
-        // ---- the row is quiet: every touched vertex must hold its value
-        // against the final values of its neighbours; queue any that does
-        // not and drain again
-        if (threadIdx.x == 0) {
-            S.qhead = S.qtail = 0;
-            S.out = 1;  // held by the sweep
-            S.k = 0;    // vertices found unstable
-        }
-        for (int i = threadIdx.x; i < kHash; i += kRThreads) S.ring[i] = kEmptySlot;
-        __syncthreads();
-        for (int i = wib; i < kHash; i += kRWarps) {
-            const uint32_t x = S.key[i];
-            if (x == kEmptyKey || p.kmax_new[x] < k) continue;
-            int val = S.cur[i];
-            if (val == kUnset) val = sky_at(p, x, k);
-            if (val < 1) continue;
-            int so = 0, si = 0;
-            const uint32_t* ao = p.out_nbr + p.out_off[x];
-            const uint32_t* ai = p.in_nbr + p.in_off[x];
-            for (int e = (int)lane; e < p.out_len[x]; e += 32) so += rv(p, S, ao[e], k) >= val;
-            for (int e = (int)lane; e < p.in_len[x]; e += 32) si += rv(p, S, ai[e], k) >= val;
-#pragma unroll
-            for (int s = 16; s; s >>= 1) {
-                so += __shfl_xor_sync(0xFFFFFFFFu, so, s);
-                si += __shfl_xor_sync(0xFFFFFFFFu, si, s);
-            }
-            if (lane == 0 && (so < val || si < k)) {
-                atomicAdd(&S.k, 1);
-                push(S, x);
-            }
-        }
-        __syncthreads();
-        const bool again = S.k != 0;
-        __syncthreads();
-        if (threadIdx.x == 0) S.k = k;
-        if (!again) {
+            const bool again = S.k != 0;
             __syncthreads();
-            break;
-        }
+            if (threadIdx.x == 0) S.k = k;
+            if (!again) {
+                __syncthreads();
+                break;
+            }
         }
         __syncthreads();
         if (S.abort) {

@@ -120,8 +120,10 @@ void charge(dc_server* s, GraphSlot& g, uint64_t bytes) {
 }
 
 // Evicts idle resident graphs (least recently used first) until `need` more
-// bytes fit.  Called with the lock held; false when nothing is left to evict.
-bool make_room(dc_server* s, uint64_t need, const GraphSlot* keep) {
+// bytes fit.  Called with the lock held; the victim is marked busy and its
+// edges are downloaded with the lock released, so other workers keep going.
+// False when nothing is left to evict.
+bool make_room(dc_server* s, uint64_t need, const GraphSlot* keep, std::unique_lock<std::mutex>& lk) {
     while (s->used + need > s->budget) {
         GraphSlot* victim = nullptr;
         for (auto& g : s->graphs) {
@@ -130,15 +132,23 @@ bool make_room(dc_server* s, uint64_t need, const GraphSlot* keep) {
         }
         if (!victim) return false;
         GraphSlot& g = *victim;
+        g.busy = true;
+        dc_graph* h = g.h;
+        lk.unlock();
         uint64_t E = 0;
-        dc_graph_info(g.h, nullptr, &E);
-        g.src.resize(E);
-        g.dst.resize(E);
-        dc_graph_get_edges(g.h, g.src.data(), g.dst.data(), E, &E);
-        dc_graph_free(g.h);
+        dc_graph_info(h, nullptr, &E);
+        std::vector<uint32_t> src(E), dst(E);
+        dc_graph_get_edges(h, src.data(), dst.data(), E, &E);
+        dc_graph_free(h);
+        lk.lock();
+        g.src.swap(src);
+        g.dst.swap(dst);
         g.h = nullptr;
+        g.busy = false;
         charge(s, g, 0);
         s->evictions++;
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();
     }
     return true;
 }
@@ -151,7 +161,7 @@ bool make_room(dc_server* s, uint64_t need, const GraphSlot* keep) {
 int admit(dc_server* s, GraphSlot& g, std::unique_lock<std::mutex>& lk) {
     if (g.h) return DC_OK;
     const uint64_t need = reserve_bytes(g.V, g.src.size(), s->sms);
-    while (!make_room(s, need, &g) && s->used != 0) s->cv_done.wait_for(lk, std::chrono::milliseconds(2));
+    while (!make_room(s, need, &g, lk) && s->used != 0) s->cv_done.wait_for(lk, std::chrono::milliseconds(2));
     charge(s, g, need);
     s->admissions++;
     std::vector<uint32_t> src, dst;
@@ -182,11 +192,11 @@ int admit(dc_server* s, GraphSlot& g, std::unique_lock<std::mutex>& lk) {
 // its bound no longer fits the charge: idle graphs are evicted for it; when
 // none is left the batch runs over budget (it cannot wait for busy graphs
 // without risking that they wait for it).
-void grow_charge(dc_server* s, GraphSlot& g, uint64_t n_ins) {
+void grow_charge(dc_server* s, GraphSlot& g, uint64_t n_ins, std::unique_lock<std::mutex>& lk) {
     const uint64_t bound = footprint_bound(g.V, g.E + n_ins, s->sms);
     if (bound <= g.bytes) return;
     const uint64_t need = reserve_bytes(g.V, g.E + n_ins, s->sms);
-    make_room(s, need - g.bytes, &g);
+    make_room(s, need - g.bytes, &g, lk);
     charge(s, g, need);
 }
 
@@ -222,7 +232,7 @@ void worker(dc_server* s) {
         }
         for (uint8_t x : del) n_ins += x == 0;
         if (rc == DC_OK) {
-            grow_charge(s, g, n_ins);
+            grow_charge(s, g, n_ins, lk);
             lk.unlock();
             rc = dc_maintain(g.h, pairs.data(), del.data(), updates, s->method, nullptr);
             uint64_t bytes = 0, E = 0;
