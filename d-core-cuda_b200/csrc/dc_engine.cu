@@ -307,6 +307,26 @@ struct PeelHook {
     }
 };
 
+// Converged warp: when the warp holds no item of its own (*keep empty), it
+// keeps the first of the items the lowest lane with *cnt > 0 is about to push
+// (*first, then *first + chunk step for the rest) to process next itself; the
+// kept item counts as outstanding like a queued one.
+__device__ __forceinline__ void keep_first_item(EngineCtl* c, unsigned long long* keep, unsigned* cnt,
+                                                unsigned long long* first) {
+    if (*keep != kEmptyItem) return;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, *cnt > 0);
+    if (!m) return;
+    const unsigned src = __ffs(m) - 1;
+    const unsigned long long it = __shfl_sync(0xFFFFFFFFu, *first, src);
+    if (lane == src) {
+        *first += 1ull << 32;  // next chunk of the same vertex
+        --*cnt;
+    }
+    if (lane == 0) atomicAdd(&c->outstanding, 1);
+    *keep = it;
+}
+
 // Up to two independent peels advance level by level in one grid: the kmax
 // pass (peeling in-degree, swapInOut + KListInplace(k = 0), main.cu:218-220)
 // and row 0 (peeling out-degree), or two rows of the per-row method.  Level
@@ -397,9 +417,16 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
             if (lane == 0 && kmin != 0x7FFFFFFF) atomicMin(&c->minkey[i].v, kmin);
         }
         block_producer_done(c, &s_prod);
-        // ---- drain the cascade
+        // ---- drain the cascade: the warp's kept item first, else the queue
         unsigned long long item;
-        while (tq_take_warp(c, p.q, &ticket, &item)) {
+        unsigned long long pkeep = kEmptyItem;
+        for (;;) {
+            if (pkeep != kEmptyItem) {
+                item = pkeep;
+                pkeep = kEmptyItem;
+            } else if (!tq_take_warp(c, p.q, &ticket, &item)) {
+                break;
+            }
             const int i = (int)(item >> 63);
             const uint32_t x = (uint32_t)item;
             const unsigned ch = (unsigned)((item >> 32) & 0x7FFFFFFFull);
@@ -430,9 +457,13 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
                 bool pb = eb < e1 && (isa_b ? oldb == I.k : oldb == L + 1) && ld_vol(&I.val[ub]) == -1 &&
                           atomicCAS(&I.val[ub], -1, L) == -1;
                 unsigned cnta = pa ? peel_nitems(I, ua, CH) : 0u;
-                tq_push_warp_multi(c, p.q, cnta, peel_item(ua, 0, i), 1ull << 32);
+                unsigned long long fa = peel_item(ua, 0, i);
+                keep_first_item(c, &pkeep, &cnta, &fa);
+                tq_push_warp_multi(c, p.q, cnta, fa, 1ull << 32);
                 unsigned cntb = pb ? peel_nitems(I, ub, CH) : 0u;
-                tq_push_warp_multi(c, p.q, cntb, peel_item(ub, 0, i), 1ull << 32);
+                unsigned long long fb = peel_item(ub, 0, i);
+                keep_first_item(c, &pkeep, &cntb, &fb);
+                tq_push_warp_multi(c, p.q, cntb, fb, 1ull << 32);
                 pushed |= __any_sync(0xFFFFFFFFu, pa || pb);
             }
             if (pushed) pushed_mask |= 1u << i;
@@ -588,6 +619,28 @@ __device__ __forceinline__ int hist_pass2(const int32_t* cur, const uint32_t* ao
     return entries;
 }
 
+// Converged warp: when the warp holds no item of its own yet (*keep ==
+// kNoKeep), it keeps the first request of the lowest requesting lane to
+// evaluate next itself instead of queueing it: the link from a drop to the
+// neighbour's evaluation skips the queue's publish and take.  The kept item
+// counts as outstanding like a queued one.
+constexpr uint32_t kNoKeep = 0xFFFFFFFFu;
+__device__ __forceinline__ void keep_one(EngineCtl* c, uint32_t* keep, unsigned* nreq, uint32_t* req) {
+    if (*keep != kNoKeep) return;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, *nreq > 0);
+    if (!m) return;
+    const unsigned src = __ffs(m) - 1;
+    const uint32_t item = __shfl_sync(0xFFFFFFFFu, req[0], src);
+    if (lane == src) {
+        for (unsigned i = 1; i < 4; ++i)
+            if (i < *nreq) req[i - 1] = req[i];
+        --*nreq;
+    }
+    if (lane == 0) atomicAdd(&c->outstanding, 1);
+    *keep = item;
+}
+
 // After x dropped from cap to nv (value already written): counts the
 // neighbours of one list with value >= nv into *cnt (this lane's share) and
 // takes x's support away from neighbours whose level lies in (nv, cap]:
@@ -596,7 +649,7 @@ __device__ __forceinline__ int hist_pass2(const int32_t* cur, const uint32_t* ao
 // lane per step; stops like hist_pass2 on kmax-sorted lists.  Returns the
 // entries read.
 __device__ __forceinline__ int recount_pass(const Trans2Params& p, EngineCtl* c, const uint32_t* a, int n, int nv,
-                                            int cap, int j, bool out_list, int* cnt) {
+                                            int cap, int j, bool out_list, int* cnt, uint32_t* keep) {
     const unsigned lane = threadIdx.x & 31u;
     int b = 0;
     for (; b < n; b += 128) {
@@ -628,6 +681,7 @@ __device__ __forceinline__ int recount_pass(const Trans2Params& p, EngineCtl* c,
                 }
             }
         }
+        keep_one(c, keep, &nreq, req);
         tq_push_warp4(c, p.q, nreq, req);
         int last = min(b + 127, n - 1) - b;
         int rr = last >> 5;
@@ -740,9 +794,16 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
         if (lane == 0 && jmin != 0x7FFFFFFF) atomicMin(&c->next_min, jmin);
         block_producer_done(c, &s_prod);
 
-        // ---- drain
+        // ---- drain: the warp's kept item first, else the queue
         unsigned long long item;
-        while (tq_take_warp(c, p.q, &ticket, &item)) {
+        uint32_t keep = kNoKeep;
+        for (;;) {
+            if (keep != kNoKeep) {
+                item = keep;
+                keep = kNoKeep;
+            } else if (!tq_take_warp(c, p.q, &ticket, &item)) {
+                break;
+            }
             const uint32_t x = (uint32_t)item;
             if (lane == 0) {
                 atomicExch(&p.mark[x], 2u);
@@ -861,8 +922,8 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
                 c_o = 0;
                 c_i = 0;
                 // out-neighbours z hold x in cnt_in; in-neighbours y hold x in cnt_out
-                my_entries += recount_pass(p, c, p.out_nbr + oo, p.out_len[x], nv, cap, j, true, &c_o);
-                my_entries += recount_pass(p, c, p.in_nbr + io, p.in_len[x], nv, cap, j, false, &c_i);
+                my_entries += recount_pass(p, c, p.out_nbr + oo, p.out_len[x], nv, cap, j, true, &c_o, &keep);
+                my_entries += recount_pass(p, c, p.in_nbr + io, p.in_len[x], nv, cap, j, false, &c_i, &keep);
 #pragma unroll
                 for (int s = 16; s; s >>= 1) {
                     c_o += __shfl_xor_sync(0xFFFFFFFFu, c_o, s);
