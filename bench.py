@@ -617,6 +617,7 @@ def run_sched(args, w, rank, world, local):
         logs = []
         for method in (dc.MAINT_LOCAL, dc.MAINT_REPEEL):
             with dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16) as g:
+                g.set_row_repair(0)  # identical batches (and row work) on both copies
                 g.decompose()
                 g.maint_log(True)
                 _stream_times(dc, g, u, v, dl, tr_sizes, method)
@@ -640,6 +641,7 @@ def run_sched(args, w, rank, world, local):
     launches0 = dc.launch_count()
     for name, sch in (("learned", sched), ("rule", None)):
         g = dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16)
+        g.set_row_repair(0)  # both policies do the same row work; only the method differs
         g.decompose()
         g.set_scheduler(sch)
         torch.cuda.synchronize()

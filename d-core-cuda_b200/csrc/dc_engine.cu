@@ -1975,6 +1975,7 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
                                                                         d.sky_off);
         d.n_corners = total;
         d.rows_valid = true;
+        if (int rc = degree_kmax_sum(h, &h->full_work)) return rc;
         cudaEventRecord(h->ev[4], h->stream);
         cudaEventRecord(h->ev[5], h->stream);
         cudaEventRecord(h->ev[6], h->stream);
@@ -1994,7 +1995,7 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     // ---- method 0: rows 1..K derived row to row
     uint64_t nlog = 0;
     if (int rc = rows_from_row0(h, K, K, true, &nlog)) return rc;
-    h->full_entries = h->stat_entries;
+    if (int rc = degree_kmax_sum(h, &h->full_work)) return rc;
     if (int rc = build_skyline_from_log(h, nlog)) return rc;
     cudaEventRecord(h->ev[5], h->stream);
     d.valid = true;
@@ -2040,6 +2041,31 @@ int row_weights(dc_graph* h, uint64_t* out) {
         run += hw[k];
         out[k] = run;
     }
+    return DC_OK;
+}
+
+// sum over vertices of (in + out degree) x kmax: the list entries a per-row
+// pass over rows 1..kmax scans, a deterministic measure of a graph's row work
+__global__ void k_deg_kmax_sum(uint32_t V, const int32_t* kmax, const int32_t* in_len, const int32_t* out_len,
+                               unsigned long long* acc) {
+    unsigned long long w = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+        w += (unsigned long long)(in_len[v] + out_len[v]) * (unsigned long long)max(kmax[v], 0);
+#pragma unroll
+    for (int s = 16; s; s >>= 1) w += __shfl_xor_sync(0xFFFFFFFFu, w, s);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(acc, w);
+}
+
+int degree_kmax_sum(dc_graph* h, uint64_t* out) {
+    unsigned long long* acc = (unsigned long long*)h->scratch->tmp64;
+    DC_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), h->stream));
+    ++g_launches;
+    k_deg_kmax_sum<<<grid_for(h, h->g.V), kThreads, 0, h->stream>>>(h->g.V, h->d.kmax_v, h->g.in_len, h->g.out_len,
+                                                                     acc);
+    unsigned long long w = 0;
+    DC_CUDA(cudaMemcpyAsync(&w, acc, sizeof(w), cudaMemcpyDeviceToHost, h->stream));
+    DC_CUDA(cudaStreamSynchronize(h->stream));
+    *out = w;
     return DC_OK;
 }
 

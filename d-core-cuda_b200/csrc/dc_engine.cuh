@@ -91,6 +91,9 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
 // max(k_first, 1)..min(k_last, kmax) only; the decomposition then holds row 0
 // and that range.
 int decompose_range(dc_graph* h, int32_t k_first, int32_t k_last);
+// Sum over vertices of (in + out degree) x kmax (a deterministic measure of
+// the row work of a graph).
+int degree_kmax_sum(dc_graph* h, uint64_t* out);
 // out[k] = total in + out degree of C_k (vertices with kmax >= k), k = 0..kmax.
 int row_weights(dc_graph* h, uint64_t* out);
 // Dense rows [k0, k0+n) into dst (device pointer, row-major, V per row).

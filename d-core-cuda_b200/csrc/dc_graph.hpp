@@ -111,7 +111,7 @@ struct dc_graph {
     unsigned peel_chunk = 64;  // adjacency entries per peel work item
     int row_repair = 1;        // deletions: repair rows locally instead of recomputing
     uint64_t stat_evals = 0, stat_drops = 0, stat_entries = 0;
-    uint64_t full_entries = 0;  // entries scanned by the last full row derivation
+    uint64_t full_work = 0;  // sum over vertices of degree x kmax at the last full decomposition
     dc::EngineCtl ctl_init{};
     // optional per-step trace of persistent kernels (diagnostics)
     unsigned long long* trace_dev = nullptr;

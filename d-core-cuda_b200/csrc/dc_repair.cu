@@ -549,11 +549,14 @@ static int rgrid(dc_graph* h, uint64_t n) {
 uint32_t row_repair_max_deletions() { return kHashLimit / 4; }
 
 // Whether repairing the rows after deleting these edges (device arrays) is
-// expected to beat recomputing them: the entries the repair scans, times the
-// passes it makes over each (histogram, release, re-check), against the
-// entries the last full row derivation scanned.
+// expected to beat recomputing them: the entries the repair scans (sum over
+// the edges' endpoints of degree x kmax) against the graph's sum of degree x
+// kmax at its last full decomposition.  The row-to-row derivation scans about
+// a twentieth of the latter and the repair makes ~8 passes over its entries
+// (histogram, release, re-check), hence the factor 160.  Deterministic: the
+// same graph and batch always take the same path.
 bool row_repair_worthwhile(dc_graph* h, const uint32_t* d_u, const uint32_t* d_v, uint32_t n) {
-    if (n == 0 || 2ull * n > kHashLimit || h->full_entries == 0 || !h->d.kmax_v) return false;
+    if (n == 0 || 2ull * n > kHashLimit || h->full_work == 0 || !h->d.kmax_v) return false;
     unsigned long long* acc = (unsigned long long*)h->scratch->tmp64;
     if (cudaMemsetAsync(acc, 0, sizeof(unsigned long long), h->stream) != cudaSuccess) return false;
     ++g_launches;
@@ -565,7 +568,7 @@ bool row_repair_worthwhile(dc_graph* h, const uint32_t* d_u, const uint32_t* d_v
         cudaGetLastError();
         return false;
     }
-    return 8ull * w < h->full_entries;
+    return 160ull * w < h->full_work;
 }
 
 #define RP_CUDA(call)                                                                       \

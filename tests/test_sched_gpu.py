@@ -100,10 +100,13 @@ def _hot_stream(dc, V, s, d, sizes, rng, seed, hot_frac=0.2):
 
 
 def _per_method_log(dc, V, s, d, u, v, dl, sizes):
-    """The stream on one copy per method: features and device times."""
+    """The stream on one copy per method: features and device times.  Rows
+    are recomputed on both copies (no in-place repair), so both split their
+    batches the same way and log the same batches."""
     logs = []
     for method in (1, 2):
         with dc.Graph.from_edges(V, s, d, gap_min=2, gap_div=16) as g:
+            g.set_row_repair(0)
             g.decompose()
             g.maint_log(True)
             pos = 0
