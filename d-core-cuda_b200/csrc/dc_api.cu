@@ -525,7 +525,7 @@ extern "C" int dc_get_tuning(dc_graph* h, dc_tuning* t) {
     t->peel_blocks_per_sm = h->peel_bps > 0 ? h->peel_bps : dflt;
     t->rows_blocks_per_sm = h->rows_bps > 0 ? h->rows_bps : dflt;
     t->peel_chunk = (int32_t)h->peel_chunk;
-    t->reserved = 0;
+    t->rows_split_permille = h->rows_split;
     return DC_OK;
 }
 
@@ -536,9 +536,12 @@ extern "C" int dc_set_tuning(dc_graph* h, const dc_tuning* t) {
         return set_error(DC_ERR_INVALID, "dc_set_tuning: blocks per SM must be 1..8");
     if (t->peel_chunk < 16 || t->peel_chunk > 4096 || (t->peel_chunk & (t->peel_chunk - 1)))
         return set_error(DC_ERR_INVALID, "dc_set_tuning: peel_chunk must be a power of two in 16..4096");
+    if (t->rows_split_permille < 0 || t->rows_split_permille > 900)
+        return set_error(DC_ERR_INVALID, "dc_set_tuning: rows_split_permille must be 0..900");
     h->peel_bps = t->peel_blocks_per_sm;
     h->rows_bps = t->rows_blocks_per_sm;
     h->peel_chunk = (unsigned)t->peel_chunk;
+    h->rows_split = t->rows_split_permille;
     return DC_OK;
 }
 
@@ -588,6 +591,21 @@ extern "C" int dc_autotune(dc_graph* h, dc_tuning* best, float* best_ms) {
         if (ms < rows_best) {
             rows_best = ms;
             pick.rows_blocks_per_sm = bps;
+        }
+    }
+    // rows in one launch or split over two concurrent ones
+    for (int split : {300, 400, 500, 600}) {
+        dc_tuning t = pick;
+        t.rows_split_permille = split;
+        dc_set_tuning(h, &t);
+        float ms = 1e30f;
+        for (int r = 0; r < 2; ++r) {
+            if (int rc = decompose_range(h, 1, K)) return rc;
+            ms = std::min(ms, h->times.trans_ms);
+        }
+        if (ms < rows_best) {
+            rows_best = ms;
+            pick.rows_split_permille = split;
         }
     }
     dc_set_tuning(h, &pick);

@@ -1152,9 +1152,49 @@ __global__ void k_corner_bound(uint32_t V, const int32_t* kmax, const int32_t* r
     if ((threadIdx.x & 31u) == 0) atomicAdd(acc, s);
 }
 
-__global__ void k_sky_count(uint32_t V, uint64_t nlog, const uint32_t* log_v, unsigned long long* cnt) {
+// corners rows 1..s can hold per vertex: min(kmax, s, row0)
+// Corner bounds of a run split after row s: acc[0] = corners of rows 1..s,
+// acc[1] = corners of rows s+1..kmax (a vertex's value drops at least one
+// per corner, so it has at most min(rows, row 0 value) of them).
+__global__ void k_corner_bound_upto(uint32_t V, const int32_t* kmax, const int32_t* row0, int32_t s,
+                                    unsigned long long* acc) {
+    unsigned long long ta = 0, tb = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        const int32_t km = kmax[v], r0 = row0[v];
+        ta += (unsigned long long)max(0, min(min(km, s), r0));
+        tb += (unsigned long long)max(0, min(km - s, r0));
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        ta += __shfl_xor_sync(0xFFFFFFFFu, ta, o);
+        tb += __shfl_xor_sync(0xFFFFFFFFu, tb, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(&acc[0], ta);
+        atomicAdd(&acc[1], tb);
+    }
+}
+
+// log entries with a negative row are void (dropped corners)
+__global__ void k_sky_count(uint32_t V, uint64_t nlog, const uint32_t* log_v, const int32_t* log_k,
+                            unsigned long long* cnt) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nlog; i += (uint64_t)gridDim.x * blockDim.x)
-        atomicAdd(&cnt[log_v[i]], 1ull);
+        if (log_k[i] >= 0) atomicAdd(&cnt[log_v[i]], 1ull);
+}
+// A second row segment that jumped from row 0 to row k logs vertex v at row
+// k whenever its value differs from row 0; the corner is void when the value
+// equals row k-1's (cur after the first segment).  Counts the void entries.
+__global__ void k_seg_void(uint64_t n, const uint32_t* log_v, int32_t* log_k, const int32_t* log_l, int32_t k,
+                           const int32_t* cur, unsigned long long* dropped) {
+    unsigned long long t = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (log_k[i] == k && log_l[i] == cur[log_v[i]]) {
+            log_k[i] = -1;
+            ++t;
+        }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
+    if ((threadIdx.x & 31u) == 0 && t) atomicAdd(dropped, t);
 }
 __global__ void k_set_one(uint32_t V, unsigned long long* cnt) {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
@@ -1172,6 +1212,7 @@ __global__ void k_sky_fill_row0(uint32_t V, const unsigned long long* off, const
 __global__ void k_sky_fill_log(uint64_t nlog, const uint32_t* log_v, const int32_t* log_k, const int32_t* log_l,
                                const unsigned long long* off, int32_t* sky_k, int32_t* sky_l, uint32_t* fill) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nlog; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (log_k[i] < 0) continue;
         uint32_t v = log_v[i];
         uint32_t pos = atomicAdd(&fill[v], 1u);
         sky_k[off[v] + pos] = log_k[i];
@@ -1287,9 +1328,11 @@ int coop_launch(dc_graph* h, const void* fn, void** args, int threads, const cha
     return DC_OK;
 }
 
-int check_ctl(dc_graph* h, EngineCtl* hc, const char* what) {
-    DC_CUDA(cudaMemcpyAsync(hc, h->ctl, sizeof(EngineCtl), cudaMemcpyDeviceToHost, h->stream));
-    DC_CUDA(cudaStreamSynchronize(h->stream));
+int check_ctl(dc_graph* h, EngineCtl* hc, const char* what) { return check_ctl_on(h->ctl, h->stream, hc, what); }
+
+int check_ctl_on(EngineCtl* ctl, cudaStream_t st, EngineCtl* hc, const char* what) {
+    DC_CUDA(cudaMemcpyAsync(hc, ctl, sizeof(EngineCtl), cudaMemcpyDeviceToHost, st));
+    DC_CUDA(cudaStreamSynchronize(st));
     if (hc->error) {
         if (hc->error & DC_DEV_ERR_TIMEOUT)
             return set_error(DC_ERR_TIMEOUT, "%s: bounded device wait expired (site %u)", what, hc->err_where);
@@ -1345,6 +1388,20 @@ void free_decomp(Decomp& d, cudaStream_t st) {
 void free_scratch(dc_graph* h) {
     Scratch* s = h->scratch;
     if (!s) return;
+    dfree(h->stream, s->b_cur);
+    dfree(h->stream, s->b_cnt_out);
+    dfree(h->stream, s->b_cnt_in);
+    dfree(h->stream, s->b_mark);
+    dfree(h->stream, s->b_stamp);
+    dfree(h->stream, s->b_logidx);
+    dfree(h->stream, s->b_tring);
+    dfree(h->stream, s->b_ctl);
+    if (s->b_stream) {
+        cudaStreamSynchronize(s->b_stream);
+        cudaStreamDestroy(s->b_stream);
+    }
+    for (auto& e : s->b_ev)
+        if (e) cudaEventDestroy(e);
     dfree(h->stream, s->key);
     dfree(h->stream, s->cdeg);
     dfree(h->stream, s->cur);
@@ -1603,38 +1660,92 @@ static int persistent_grid(dc_graph* h, const void* fn, int bps, int* blocks) {
     return DC_OK;
 }
 
-// Launches a persistent kernel, waits, and converts its device status.
-int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out, int bps) {
+// Initialises a control block (on stream st) and launches a persistent
+// kernel there without waiting.  The handle's own block carries the trace.
+static int persistent_launch(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* ctl,
+                             cudaStream_t st, int bps) {
     int blocks = 0;
     if (int rc = persistent_grid(h, fn, bps, &blocks)) return rc;
-    {
-        EngineCtl& init = h->ctl_init;
-        memset(&init, 0, sizeof(init));
-        init.step = -1;
+    const bool own = ctl == h->ctl;
+    EngineCtl& init = own ? h->ctl_init : h->ctl_init_b;
+    memset(&init, 0, sizeof(init));
+    init.step = -1;
+    if (own) {
         init.trace = h->trace_dev;
         init.trace_cap = h->trace_cap;
-        DC_CUDA(cudaMemcpyAsync(h->ctl, &init, sizeof(EngineCtl), cudaMemcpyHostToDevice, h->stream));
-        if (h->trace_dev)
-            DC_CUDA(cudaMemsetAsync(h->trace_dev, 0, 64ull * h->trace_cap, h->stream));
     }
+    DC_CUDA(cudaMemcpyAsync(ctl, &init, sizeof(EngineCtl), cudaMemcpyHostToDevice, st));
+    if (own && h->trace_dev) DC_CUDA(cudaMemsetAsync(h->trace_dev, 0, 64ull * h->trace_cap, st));
     ++g_launches;
-    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kThreads), args, 0, h->stream);
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kThreads), args, 0, st);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return set_error(DC_ERR_CUDA, "%s: cooperative launch failed (%s)", name, cudaGetErrorString(e));
     }
-    int rc = check_ctl(h, out, name);
-    if (h->trace_dev && h->trace_host) {
+    return DC_OK;
+}
+
+// Waits for a persistent kernel launched on stream st with control block ctl
+// and converts its device status; the handle's own block also delivers the
+// trace.  A failed phase may leave items in its ring, which is cleared.
+static int finish_persistent(dc_graph* h, EngineCtl* ctl, cudaStream_t st, const char* name, EngineCtl* out) {
+    int rc = check_ctl_on(ctl, st, out, name);
+    const bool own = ctl == h->ctl;
+    if (own && h->trace_dev && h->trace_host) {
         cudaMemcpy(h->trace_host, h->trace_dev, 64ull * h->trace_cap, cudaMemcpyDeviceToHost);
         h->trace_steps = (unsigned)std::max(0, out->step);
         if (h->trace_cb) h->trace_cb(name, h->trace_host, h->trace_steps, h->trace_user);
     }
     if (rc != DC_OK) {
-        // a failed phase may leave items in the ring
-        cudaMemsetAsync(h->scratch->tring, 0xFF, sizeof(unsigned long long) * h->scratch->tring_cap, h->stream);
-        cudaStreamSynchronize(h->stream);
+        Scratch* s = h->scratch;
+        unsigned long long* ring = own ? s->tring : s->b_tring;
+        const uint64_t cap = own ? s->tring_cap : s->b_tring_cap;
+        cudaMemsetAsync(ring, 0xFF, sizeof(unsigned long long) * cap, st);
+        cudaStreamSynchronize(st);
     }
     return rc;
+}
+
+// Launches a persistent kernel, waits, and converts its device status.
+int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out, int bps) {
+    if (int rc = persistent_launch(h, fn, args, name, h->ctl, h->stream, bps)) return rc;
+    return finish_persistent(h, h->ctl, h->stream, name, out);
+}
+
+// State of the second row segment, sized for V vertices.
+static int ensure_segment_b(dc_graph* h, uint32_t V) {
+    Scratch* s = h->scratch;
+    if (!s->b_stream) {
+        DC_CUDA(cudaStreamCreateWithFlags(&s->b_stream, cudaStreamNonBlocking));
+        for (auto& e : s->b_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    if (!s->b_ctl && dmalloc(h->stream, &s->b_ctl, 1)) return DC_ERR_NOMEM;
+    if (s->b_cap_V < V || !s->b_cur) {
+        dfree(h->stream, s->b_cur);
+        dfree(h->stream, s->b_cnt_out);
+        dfree(h->stream, s->b_cnt_in);
+        dfree(h->stream, s->b_mark);
+        dfree(h->stream, s->b_stamp);
+        dfree(h->stream, s->b_logidx);
+        const uint64_t n = (uint64_t)V + 1;
+        if (dmalloc(h->stream, &s->b_cur, n) || dmalloc(h->stream, &s->b_cnt_out, n) ||
+            dmalloc(h->stream, &s->b_cnt_in, n) || dmalloc(h->stream, &s->b_mark, n) ||
+            dmalloc(h->stream, &s->b_stamp, n) || dmalloc(h->stream, &s->b_logidx, n))
+            return DC_ERR_NOMEM;
+        s->b_cap_V = V;
+    }
+    uint64_t need = 2ull * V + (uint64_t)h->geom.sms * 64 + 4096, cap = 1024;
+    while (cap < need) cap <<= 1;
+    if (s->b_tring_cap < cap || !s->b_tring) {
+        dfree(h->stream, s->b_tring);
+        s->b_tring_cap = 0;
+        if (dmalloc(h->stream, &s->b_tring, cap)) return DC_ERR_NOMEM;
+        s->b_tring_cap = cap;
+        DC_CUDA(cudaMemsetAsync(s->b_tring, 0xFF, sizeof(unsigned long long) * cap, h->stream));
+    }
+    // the second stream must see these allocations and the ring's reset
+    DC_CUDA(cudaStreamSynchronize(h->stream));
+    return DC_OK;
 }
 
 PeelInst make_inst(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* val, int slot) {
@@ -1701,16 +1812,23 @@ int run_peel(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* 
     return DC_OK;
 }
 
-int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
+int build_skyline_from_log(dc_graph* h, uint64_t nlog, uint64_t off2, uint64_t n2, uint64_t void2) {
     Scratch* s = h->scratch;
     Decomp& d = h->d;
     uint32_t V = h->g.V;
     unsigned long long* cnt = (unsigned long long*)s->tmp64;
     ++g_launches;
     k_set_one<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt);
-    if (nlog) k_sky_count<<<grid_for(h, nlog), kThreads, 0, h->stream>>>(V, nlog, s->log_v, cnt);
+    if (nlog) {
+        ++g_launches;
+        k_sky_count<<<grid_for(h, nlog), kThreads, 0, h->stream>>>(V, nlog, s->log_v, s->log_k, cnt);
+    }
+    if (n2) {
+        ++g_launches;
+        k_sky_count<<<grid_for(h, n2), kThreads, 0, h->stream>>>(V, n2, s->log_v + off2, s->log_k + off2, cnt);
+    }
     if (int rc = scan_tmp64(h, V)) return rc;
-    uint64_t total = (uint64_t)V + nlog;
+    uint64_t total = (uint64_t)V + nlog + n2 - void2;
     if (d.corner_cap < total) {
         dfree(h->stream, d.sky_k);
         dfree(h->stream, d.sky_l);
@@ -1720,10 +1838,16 @@ int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
     if (!d.sky_off && dmalloc(h->stream, &d.sky_off, (uint64_t)V + 1)) return DC_ERR_NOMEM;
     ++g_launches;
     k_sky_fill_row0<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt, s->row0, d.sky_k, d.sky_l, s->cursor);
-    if (nlog)
+    if (nlog) {
         ++g_launches;
         k_sky_fill_log<<<grid_for(h, nlog), kThreads, 0, h->stream>>>(nlog, s->log_v, s->log_k, s->log_l, cnt, d.sky_k,
                                                                       d.sky_l, s->cursor);
+    }
+    if (n2) {
+        ++g_launches;
+        k_sky_fill_log<<<grid_for(h, n2), kThreads, 0, h->stream>>>(n2, s->log_v + off2, s->log_k + off2,
+                                                                    s->log_l + off2, cnt, d.sky_k, d.sky_l, s->cursor);
+    }
     ++g_launches;
     k_sky_sort<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt, d.sky_k, d.sky_l, d.sky_off);
     d.n_corners = total;
@@ -1845,7 +1969,38 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     DC_CUDA(cudaMemcpyAsync(hist, start.data(), sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyHostToDevice, h->stream));
     ++g_launches;
     k_order_scatter<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist, s->order);
-    uint64_t lc = bound + 1;
+    // a full run may be split in two row segments run concurrently: rows
+    // K0..split on the handle's stream and split+1..Kstop (jumping from row 0)
+    // on a second stream, each with its own state; the first segment's log
+    // takes [0, capA), the second [capA, lc)
+    const int32_t k0 = std::max(1, K0);
+    int32_t split = 0;
+    if (k0 == 1 && Kstop == K && h->rows_split > 0) {
+        split = (int32_t)((int64_t)K * h->rows_split / 1000);
+        if (split < 1 || split >= Kstop) split = 0;
+    }
+    int seg_bps = h->rows_bps;
+    if (split) {
+        // both segments' blocks must be resident together for their grid barriers
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_trans2, kThreads, 0) != cudaSuccess)
+            per_sm = 0;
+        const int want = seg_bps > 0 ? seg_bps : (h->blocks_per_sm > 0 ? h->blocks_per_sm : kDefaultBlocksPerSm);
+        seg_bps = std::min(want, per_sm / 2);
+        if (seg_bps < 1) split = 0;
+    }
+    uint64_t lc = bound + 1, capA = lc;
+    if (split) {
+        DC_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(unsigned long long), h->stream));
+        ++g_launches;
+        k_corner_bound_upto<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, s->row0, split, acc);
+        unsigned long long ba[2] = {0, 0};
+        DC_CUDA(cudaMemcpyAsync(ba, acc, sizeof(ba), cudaMemcpyDeviceToHost, h->stream));
+        DC_CUDA(cudaStreamSynchronize(h->stream));
+        // the second segment's jump to row split+1 adds at most one corner per vertex
+        capA = ba[0] + 1;
+        lc = capA + ba[1] + V + 1;
+    }
     if (s->log_cap < lc) {
         dfree(h->stream, s->log_v);
         dfree(h->stream, s->log_k);
@@ -1853,6 +2008,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
         if (dmalloc(h->stream, &s->log_v, lc) || dmalloc(h->stream, &s->log_k, lc) || dmalloc(h->stream, &s->log_l, lc)) return DC_ERR_NOMEM;
         s->log_cap = lc;
     }
+    if (!split) capA = s->log_cap;
     // adjacency lists ordered by neighbour kmax (kept until the graph changes)
     int sorted = 0;
     if (allow_sort || g.sorted_kmax)
@@ -1870,8 +2026,8 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     tp.in_off = g.in_off; tp.in_len = g.in_len; tp.in_nbr = g.in_nbr;
     tp.kmax = d.kmax_v;
     tp.K = K;
-    tp.K0 = std::max(1, K0);
-    tp.Kstop = Kstop;
+    tp.K0 = k0;
+    tp.Kstop = split ? split : Kstop;
     tp.sorted = sorted;
     tp.order = s->order;
     tp.ck = s->ck;
@@ -1884,23 +2040,81 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     tp.log_v = s->log_v;
     tp.log_k = s->log_k;
     tp.log_l = s->log_l;
-    tp.log_cap = s->log_cap;
+    tp.log_cap = capA;
     tp.q.slots = s->tring;
     tp.q.mask = (unsigned)(s->tring_cap - 1);
     tp.ctl = h->ctl;
-    uint64_t nlog = 0;
+    Trans2Params tb = tp;
+    if (split) {
+        if (int rc = ensure_segment_b(h, V)) return rc;
+        // the second segment starts once the shared preparation is done
+        DC_CUDA(cudaEventRecord(s->b_ev[0], h->stream));
+        DC_CUDA(cudaStreamWaitEvent(s->b_stream, s->b_ev[0], 0));
+        DC_CUDA(cudaMemcpyAsync(s->b_cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, s->b_stream));
+        ++g_launches;
+        k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, s->b_stream>>>(
+            V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, s->b_cur, s->b_cnt_out, s->b_cnt_in);
+        DC_CUDA(cudaMemsetAsync(s->b_mark, 0, sizeof(uint32_t) * V, s->b_stream));
+        DC_CUDA(cudaMemsetAsync(s->b_stamp, 0xFF, sizeof(int32_t) * V, s->b_stream));
+        tb.K0 = split + 1;
+        tb.Kstop = Kstop;
+        tb.cur = s->b_cur;
+        tb.cnt_out = s->b_cnt_out;
+        tb.cnt_in = s->b_cnt_in;
+        tb.mark = s->b_mark;
+        tb.stamp = s->b_stamp;
+        tb.logidx = s->b_logidx;
+        tb.log_v = s->log_v + capA;
+        tb.log_k = s->log_k + capA;
+        tb.log_l = s->log_l + capA;
+        tb.log_cap = s->log_cap - capA;
+        tb.q.slots = s->b_tring;
+        tb.q.mask = (unsigned)(s->b_tring_cap - 1);
+        tb.ctl = s->b_ctl;
+    }
+    uint64_t nlog = 0, n2 = 0;
+    unsigned long long void2 = 0;
     cudaEventRecord(h->ev[3], h->stream);
-    if (Kstop >= tp.K0) {
+    if (tp.Kstop >= tp.K0) {
         void* args[] = {&tp};
-        EngineCtl hc;
-        if (int rc = run_persistent(h, (const void*)k_trans2, args, "transitions", &hc, h->rows_bps)) return rc;
+        void* args_b[] = {&tb};
+        if (int rc = persistent_launch(h, (const void*)k_trans2, args, "transitions", h->ctl, h->stream, seg_bps))
+            return rc;
+        int rcb = DC_OK;
+        if (split)
+            rcb = persistent_launch(h, (const void*)k_trans2, args_b, "transitions (second segment)", s->b_ctl,
+                                    s->b_stream, seg_bps);
+        EngineCtl hc, hb;
+        int rc = finish_persistent(h, h->ctl, h->stream, "transitions", &hc);
+        if (split && rcb == DC_OK) rcb = finish_persistent(h, s->b_ctl, s->b_stream, "transitions (second segment)", &hb);
+        if (rc) return rc;
+        if (rcb) return rcb;
         nlog = hc.log_count;
         h->stat_evals = hc.evals;
         h->stat_drops = hc.drops;
         h->stat_entries = hc.edges_scanned;
+        if (split) {
+            n2 = hb.log_count;
+            h->stat_evals += hb.evals;
+            h->stat_drops += hb.drops;
+            h->stat_entries += hb.edges_scanned;
+            DC_CUDA(cudaEventRecord(s->b_ev[1], s->b_stream));
+            DC_CUDA(cudaStreamWaitEvent(h->stream, s->b_ev[1], 0));
+            if (n2) {
+                DC_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), h->stream));
+                ++g_launches;
+                k_seg_void<<<grid_for(h, n2), kThreads, 0, h->stream>>>(n2, s->log_v + capA, s->log_k + capA,
+                                                                        s->log_l + capA, split + 1, s->cur, acc);
+                DC_CUDA(cudaMemcpyAsync(&void2, acc, sizeof(void2), cudaMemcpyDeviceToHost, h->stream));
+                DC_CUDA(cudaStreamSynchronize(h->stream));
+            }
+        }
     }
     cudaEventRecord(h->ev[4], h->stream);
     *nlog_out = nlog;
+    h->seg2_off = capA;
+    h->seg2_n = n2;
+    h->seg2_void = void2;
     return DC_OK;
 }
 
@@ -1996,7 +2210,7 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     uint64_t nlog = 0;
     if (int rc = rows_from_row0(h, K, K, true, &nlog)) return rc;
     if (int rc = degree_kmax_sum(h, &h->full_work)) return rc;
-    if (int rc = build_skyline_from_log(h, nlog)) return rc;
+    if (int rc = build_skyline_from_log(h, nlog, h->seg2_off, h->seg2_n, h->seg2_void)) return rc;
     cudaEventRecord(h->ev[5], h->stream);
     d.valid = true;
     if (materialize_rows) {
@@ -2107,7 +2321,7 @@ int decompose_range(dc_graph* h, int32_t k_first, int32_t k_last) {
     DC_CUDA(cudaMemcpyAsync(s->row0, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
     uint64_t nlog = 0;
     if (int rc = rows_from_row0(h, K, k1, true, &nlog, k0)) return rc;
-    if (int rc = build_skyline_from_log(h, nlog)) return rc;
+    if (int rc = build_skyline_from_log(h, nlog, h->seg2_off, h->seg2_n, h->seg2_void)) return rc;
     cudaEventRecord(h->ev[5], h->stream);
     DC_CUDA(cudaStreamSynchronize(h->stream));
     float ms = 0;

@@ -47,6 +47,20 @@ struct Scratch {
     // maintenance
     int32_t* kmax_old = nullptr;  // [V]
     int32_t* row0_old = nullptr;  // [V]
+    // second row segment: rows split over two concurrent launches, each
+    // with its own values, counters, marks, ticket ring and control block
+    uint32_t b_cap_V = 0;
+    int32_t* b_cur = nullptr;
+    int32_t* b_cnt_out = nullptr;
+    int32_t* b_cnt_in = nullptr;
+    uint32_t* b_mark = nullptr;
+    int32_t* b_stamp = nullptr;
+    uint32_t* b_logidx = nullptr;
+    unsigned long long* b_tring = nullptr;
+    uint64_t b_tring_cap = 0;
+    EngineCtl* b_ctl = nullptr;
+    cudaStream_t b_stream = nullptr;
+    cudaEvent_t b_ev[2] = {nullptr, nullptr};
 };
 
 // Allocation / release (all errors reported through set_error, return DC_*).
@@ -107,11 +121,16 @@ int coop_launch(dc_graph* h, const void* fn, void** args, int threads, const cha
 
 // Shared host helpers of the engine (dc_engine.cu).
 int ensure_tring(dc_graph* h, uint64_t need);
+// Device status of a control block (copied back on stream st, which is
+// synchronised) converted to DC_* codes.
+int check_ctl_on(EngineCtl* ctl, cudaStream_t st, EngineCtl* hc, const char* what);
 // bps: blocks per SM for this kernel (0 = the handle's blocks_per_sm, else 2).
 int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out, int bps = 0);
 int check_ctl(dc_graph* h, EngineCtl* hc, const char* what);
 int scan_tmp64(dc_graph* h, uint64_t n);
-int build_skyline_from_log(dc_graph* h, uint64_t nlog);
+// Skyline from row 0 and the corner log: entries [0, nlog) and, when a second
+// row segment ran, [off2, off2 + n2).
+int build_skyline_from_log(dc_graph* h, uint64_t nlog, uint64_t off2 = 0, uint64_t n2 = 0, uint64_t void2 = 0);
 // kmax (in-degree peel) and row 0 (out-degree peel) of the current graph into
 // d.kmax_v and the scratch row 0; reports the largest values.
 int peel_kmax_row0(dc_graph* h, int32_t* kmax, int32_t* lmax);

@@ -65,7 +65,7 @@ MAINT_AUTO, MAINT_LOCAL, MAINT_REPEEL = 0, 1, 2
 
 class Tuning(ctypes.Structure):
     _fields_ = [("peel_blocks_per_sm", ctypes.c_int32), ("rows_blocks_per_sm", ctypes.c_int32),
-                ("peel_chunk", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("peel_chunk", ctypes.c_int32), ("rows_split_permille", ctypes.c_int32)]
 
 
 class ServerInfo(ctypes.Structure):
@@ -554,10 +554,10 @@ class Graph:
     def tuning(self):
         t = Tuning()
         _check(lib().dc_get_tuning(self._h, ctypes.byref(t)))
-        return {f: getattr(t, f) for f, _ in Tuning._fields_ if f != "reserved"}
+        return {f: getattr(t, f) for f, _ in Tuning._fields_}
 
-    def set_tuning(self, peel_blocks_per_sm=1, rows_blocks_per_sm=1, peel_chunk=64):
-        t = Tuning(peel_blocks_per_sm, rows_blocks_per_sm, peel_chunk, 0)
+    def set_tuning(self, peel_blocks_per_sm=2, rows_blocks_per_sm=2, peel_chunk=64, rows_split_permille=0):
+        t = Tuning(peel_blocks_per_sm, rows_blocks_per_sm, peel_chunk, rows_split_permille)
         _check(lib().dc_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self):
@@ -566,7 +566,7 @@ class Graph:
         t = Tuning()
         ms = ctypes.c_float(0)
         _check(lib().dc_autotune(self._h, ctypes.byref(t), ctypes.byref(ms)))
-        return {f: getattr(t, f) for f, _ in Tuning._fields_ if f != "reserved"}, ms.value
+        return {f: getattr(t, f) for f, _ in Tuning._fields_}, ms.value
 
     def set_launch(self, blocks_per_sm):
         _check(lib().dc_set_launch(self._h, blocks_per_sm))

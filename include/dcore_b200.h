@@ -375,14 +375,17 @@ typedef struct dc_tuning {
     int32_t peel_blocks_per_sm; /* 1..8 (capped by occupancy) */
     int32_t rows_blocks_per_sm; /* 1..8 (capped by occupancy) */
     int32_t peel_chunk;         /* power of two, 16..4096 */
-    int32_t reserved;
+    int32_t rows_split_permille; /* 0: rows 1..kmax in one launch; s in 1..900: a full
+                                    decomposition runs rows 1..kmax*s/1000 and the rest
+                                    (starting from row 0) as two concurrent launches */
 } dc_tuning;
 int dc_get_tuning(dc_graph* g, dc_tuning* t);
 int dc_set_tuning(dc_graph* g, const dc_tuning* t);
 /* Autotuner: times the decomposition of this graph under candidate launch
  * shapes (peel grid 1..6 blocks per SM x chunk 32..256 on the peel alone,
- * then the row kernel's grid 1..8 blocks per SM on the rows alone, each
- * candidate twice, grids capped by occupancy), keeps the fastest on the handle
+ * then the row kernel's grid 1..8 blocks per SM on the rows alone, then the
+ * rows' split into two concurrent launches (none, 30..60 %), each candidate
+ * twice, grids capped by occupancy), keeps the fastest on the handle
  * and ends with a full decomposition.  *best / *best_ms (may be NULL): the
  * chosen setting and its peel + rows device time. */
 int dc_autotune(dc_graph* g, dc_tuning* best, float* best_ms);
