@@ -525,7 +525,7 @@ extern "C" int dc_get_tuning(dc_graph* h, dc_tuning* t) {
     t->peel_blocks_per_sm = h->peel_bps > 0 ? h->peel_bps : dflt;
     t->rows_blocks_per_sm = h->rows_bps > 0 ? h->rows_bps : dflt;
     t->peel_chunk = (int32_t)h->peel_chunk;
-    t->rows_split_permille = h->rows_split;
+    for (int i = 0; i < 3; ++i) t->rows_split_permille[i] = h->rows_split[i];
     return DC_OK;
 }
 
@@ -536,12 +536,20 @@ extern "C" int dc_set_tuning(dc_graph* h, const dc_tuning* t) {
         return set_error(DC_ERR_INVALID, "dc_set_tuning: blocks per SM must be 1..8");
     if (t->peel_chunk < 16 || t->peel_chunk > 4096 || (t->peel_chunk & (t->peel_chunk - 1)))
         return set_error(DC_ERR_INVALID, "dc_set_tuning: peel_chunk must be a power of two in 16..4096");
-    if (t->rows_split_permille < 0 || t->rows_split_permille > 900)
-        return set_error(DC_ERR_INVALID, "dc_set_tuning: rows_split_permille must be 0..900");
+    static_assert(kMaxRowSegments - 1 == 3, "dc_tuning holds three row cuts");
+    for (int i = 0; i < 3; ++i) {
+        const int32_t c = t->rows_split_permille[i];
+        const bool ok = c == 0 ? (i == 2 || t->rows_split_permille[i + 1] == 0)
+                               : (c <= 999 && (i == 0 || (t->rows_split_permille[i - 1] > 0 &&
+                                                          c > t->rows_split_permille[i - 1])));
+        if (c < 0 || !ok)
+            return set_error(DC_ERR_INVALID,
+                             "dc_set_tuning: rows_split_permille must hold ascending values in 1..999, then zeros");
+    }
     h->peel_bps = t->peel_blocks_per_sm;
     h->rows_bps = t->rows_blocks_per_sm;
     h->peel_chunk = (unsigned)t->peel_chunk;
-    h->rows_split = t->rows_split_permille;
+    for (int i = 0; i < 3; ++i) h->rows_split[i] = t->rows_split_permille[i];
     return DC_OK;
 }
 
@@ -593,20 +601,41 @@ extern "C" int dc_autotune(dc_graph* h, dc_tuning* best, float* best_ms) {
             pick.rows_blocks_per_sm = bps;
         }
     }
-    // rows in one launch or split over two concurrent ones
-    for (int split : {300, 400, 500, 600}) {
-        dc_tuning t = pick;
-        t.rows_split_permille = split;
-        dc_set_tuning(h, &t);
-        float ms = 1e30f;
-        for (int r = 0; r < 2; ++r) {
-            if (int rc = decompose_range(h, 1, K)) return rc;
-            ms = std::min(ms, h->times.trans_ms);
+    // row segments: one cut at a time (up to three), each the candidate
+    // that makes the rows fastest, while a new cut still helps
+    static const int32_t kCuts[] = {150, 200, 250, 300, 350, 400, 450, 500, 600, 700};
+    for (int level = 0; level < 3; ++level) {
+        int32_t best_cut = 0;
+        for (int32_t c : kCuts) {
+            dc_tuning t = pick;
+            int32_t v[4] = {0, 0, 0, 0};
+            int n = 0;
+            bool dup = false;
+            for (int i = 0; i < level; ++i) {
+                dup |= pick.rows_split_permille[i] == c;
+                v[n++] = pick.rows_split_permille[i];
+            }
+            if (dup) continue;
+            v[n++] = c;
+            std::sort(v, v + n);
+            for (int i = 0; i < 3; ++i) t.rows_split_permille[i] = v[i];
+            if (dc_set_tuning(h, &t) != DC_OK) continue;
+            float ms = 1e30f;
+            for (int r = 0; r < 2; ++r) {
+                if (int rc = decompose_range(h, 1, K)) return rc;
+                ms = std::min(ms, h->times.trans_ms);
+            }
+            if (ms < rows_best) {
+                rows_best = ms;
+                best_cut = c;
+            }
         }
-        if (ms < rows_best) {
-            rows_best = ms;
-            pick.rows_split_permille = split;
-        }
+        if (!best_cut) break;
+        int32_t v[4] = {0, 0, 0, 0};
+        for (int i = 0; i < level; ++i) v[i] = pick.rows_split_permille[i];
+        v[level] = best_cut;
+        std::sort(v, v + level + 1);
+        for (int i = 0; i < 3; ++i) pick.rows_split_permille[i] = v[i];
     }
     dc_set_tuning(h, &pick);
     if (int rc = decompose(h, 0, 0)) return rc;

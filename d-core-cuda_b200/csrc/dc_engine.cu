@@ -1153,25 +1153,29 @@ __global__ void k_corner_bound(uint32_t V, const int32_t* kmax, const int32_t* r
 }
 
 // corners rows 1..s can hold per vertex: min(kmax, s, row0)
-// Corner bounds of a run split after row s: acc[0] = corners of rows 1..s,
-// acc[1] = corners of rows s+1..kmax (a vertex's value drops at least one
-// per corner, so it has at most min(rows, row 0 value) of them).
-__global__ void k_corner_bound_upto(uint32_t V, const int32_t* kmax, const int32_t* row0, int32_t s,
-                                    unsigned long long* acc) {
-    unsigned long long ta = 0, tb = 0;
+// Row ranges of the segments of a split run of rows.
+struct SegBounds {
+    int32_t lo[kMaxRowSegments], hi[kMaxRowSegments];
+    int n;
+};
+// Corner bounds per segment: acc[i] = corners of rows lo[i]..hi[i] (a
+// vertex's value drops at least one per corner, so it has at most
+// min(rows it belongs to, row 0 value) of them; the first corner of a
+// segment that starts from row 0 is one of them).
+__global__ void k_corner_bounds(uint32_t V, const int32_t* kmax, const int32_t* row0, SegBounds b,
+                                unsigned long long* acc) {
+    unsigned long long t[kMaxRowSegments] = {};
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
         const int32_t km = kmax[v], r0 = row0[v];
-        ta += (unsigned long long)max(0, min(min(km, s), r0));
-        tb += (unsigned long long)max(0, min(km - s, r0));
+#pragma unroll
+        for (int i = 0; i < kMaxRowSegments; ++i)
+            if (i < b.n) t[i] += (unsigned long long)max(0, min(min(km, b.hi[i]) - b.lo[i] + 1, r0));
     }
 #pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        ta += __shfl_xor_sync(0xFFFFFFFFu, ta, o);
-        tb += __shfl_xor_sync(0xFFFFFFFFu, tb, o);
-    }
-    if ((threadIdx.x & 31u) == 0) {
-        atomicAdd(&acc[0], ta);
-        atomicAdd(&acc[1], tb);
+    for (int i = 0; i < kMaxRowSegments; ++i) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) t[i] += __shfl_xor_sync(0xFFFFFFFFu, t[i], o);
+        if ((threadIdx.x & 31u) == 0 && i < b.n && t[i]) atomicAdd(&acc[i], t[i]);
     }
 }
 
@@ -1181,9 +1185,9 @@ __global__ void k_sky_count(uint32_t V, uint64_t nlog, const uint32_t* log_v, co
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nlog; i += (uint64_t)gridDim.x * blockDim.x)
         if (log_k[i] >= 0) atomicAdd(&cnt[log_v[i]], 1ull);
 }
-// A second row segment that jumped from row 0 to row k logs vertex v at row
-// k whenever its value differs from row 0; the corner is void when the value
-// equals row k-1's (cur after the first segment).  Counts the void entries.
+// A row segment that jumped from row 0 to row k logs vertex v at row k
+// whenever its value differs from row 0; the corner is void when the value
+// equals row k-1's (cur after the previous segment).  Counts the void entries.
 __global__ void k_seg_void(uint64_t n, const uint32_t* log_v, int32_t* log_k, const int32_t* log_l, int32_t k,
                            const int32_t* cur, unsigned long long* dropped) {
     unsigned long long t = 0;
@@ -1388,20 +1392,20 @@ void free_decomp(Decomp& d, cudaStream_t st) {
 void free_scratch(dc_graph* h) {
     Scratch* s = h->scratch;
     if (!s) return;
-    dfree(h->stream, s->b_cur);
-    dfree(h->stream, s->b_cnt_out);
-    dfree(h->stream, s->b_cnt_in);
-    dfree(h->stream, s->b_mark);
-    dfree(h->stream, s->b_stamp);
-    dfree(h->stream, s->b_logidx);
-    dfree(h->stream, s->b_tring);
-    dfree(h->stream, s->b_ctl);
-    if (s->b_stream) {
-        cudaStreamSynchronize(s->b_stream);
-        cudaStreamDestroy(s->b_stream);
+    for (RowSegment& g : s->seg) {
+        if (g.stream) cudaStreamSynchronize(g.stream);
+        dfree(h->stream, g.cur);
+        dfree(h->stream, g.cnt_out);
+        dfree(h->stream, g.cnt_in);
+        dfree(h->stream, g.mark);
+        dfree(h->stream, g.stamp);
+        dfree(h->stream, g.logidx);
+        dfree(h->stream, g.tring);
+        dfree(h->stream, g.ctl);
+        if (g.stream) cudaStreamDestroy(g.stream);
+        for (auto& e : g.ev)
+            if (e) cudaEventDestroy(e);
     }
-    for (auto& e : s->b_ev)
-        if (e) cudaEventDestroy(e);
     dfree(h->stream, s->key);
     dfree(h->stream, s->cdeg);
     dfree(h->stream, s->cur);
@@ -1667,7 +1671,10 @@ static int persistent_launch(dc_graph* h, const void* fn, void** args, const cha
     int blocks = 0;
     if (int rc = persistent_grid(h, fn, bps, &blocks)) return rc;
     const bool own = ctl == h->ctl;
-    EngineCtl& init = own ? h->ctl_init : h->ctl_init_b;
+    EngineCtl* initp = &h->ctl_init;
+    for (int i = 0; i < kMaxRowSegments - 1; ++i)
+        if (ctl == h->scratch->seg[i].ctl) initp = &h->ctl_init_seg[i];
+    EngineCtl& init = *initp;
     memset(&init, 0, sizeof(init));
     init.step = -1;
     if (own) {
@@ -1698,8 +1705,13 @@ static int finish_persistent(dc_graph* h, EngineCtl* ctl, cudaStream_t st, const
     }
     if (rc != DC_OK) {
         Scratch* s = h->scratch;
-        unsigned long long* ring = own ? s->tring : s->b_tring;
-        const uint64_t cap = own ? s->tring_cap : s->b_tring_cap;
+        unsigned long long* ring = s->tring;
+        uint64_t cap = s->tring_cap;
+        for (const RowSegment& g : s->seg)
+            if (ctl == g.ctl) {
+                ring = g.tring;
+                cap = g.tring_cap;
+            }
         cudaMemsetAsync(ring, 0xFF, sizeof(unsigned long long) * cap, st);
         cudaStreamSynchronize(st);
     }
@@ -1712,39 +1724,38 @@ int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, E
     return finish_persistent(h, h->ctl, h->stream, name, out);
 }
 
-// State of the second row segment, sized for V vertices.
-static int ensure_segment_b(dc_graph* h, uint32_t V) {
+// State of row segment i + 1 (seg[i]), sized for V vertices.
+static int ensure_segment(dc_graph* h, int i, uint32_t V) {
     Scratch* s = h->scratch;
-    if (!s->b_stream) {
-        DC_CUDA(cudaStreamCreateWithFlags(&s->b_stream, cudaStreamNonBlocking));
-        for (auto& e : s->b_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    RowSegment& g = s->seg[i];
+    if (!g.stream) {
+        DC_CUDA(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+        for (auto& e : g.ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    if (!s->b_ctl && dmalloc(h->stream, &s->b_ctl, 1)) return DC_ERR_NOMEM;
-    if (s->b_cap_V < V || !s->b_cur) {
-        dfree(h->stream, s->b_cur);
-        dfree(h->stream, s->b_cnt_out);
-        dfree(h->stream, s->b_cnt_in);
-        dfree(h->stream, s->b_mark);
-        dfree(h->stream, s->b_stamp);
-        dfree(h->stream, s->b_logidx);
+    if (!g.ctl && dmalloc(h->stream, &g.ctl, 1)) return DC_ERR_NOMEM;
+    if (g.cap_V < V || !g.cur) {
+        dfree(h->stream, g.cur);
+        dfree(h->stream, g.cnt_out);
+        dfree(h->stream, g.cnt_in);
+        dfree(h->stream, g.mark);
+        dfree(h->stream, g.stamp);
+        dfree(h->stream, g.logidx);
+        g.cap_V = 0;
         const uint64_t n = (uint64_t)V + 1;
-        if (dmalloc(h->stream, &s->b_cur, n) || dmalloc(h->stream, &s->b_cnt_out, n) ||
-            dmalloc(h->stream, &s->b_cnt_in, n) || dmalloc(h->stream, &s->b_mark, n) ||
-            dmalloc(h->stream, &s->b_stamp, n) || dmalloc(h->stream, &s->b_logidx, n))
+        if (dmalloc(h->stream, &g.cur, n) || dmalloc(h->stream, &g.cnt_out, n) || dmalloc(h->stream, &g.cnt_in, n) ||
+            dmalloc(h->stream, &g.mark, n) || dmalloc(h->stream, &g.stamp, n) || dmalloc(h->stream, &g.logidx, n))
             return DC_ERR_NOMEM;
-        s->b_cap_V = V;
+        g.cap_V = V;
     }
     uint64_t need = 2ull * V + (uint64_t)h->geom.sms * 64 + 4096, cap = 1024;
     while (cap < need) cap <<= 1;
-    if (s->b_tring_cap < cap || !s->b_tring) {
-        dfree(h->stream, s->b_tring);
-        s->b_tring_cap = 0;
-        if (dmalloc(h->stream, &s->b_tring, cap)) return DC_ERR_NOMEM;
-        s->b_tring_cap = cap;
-        DC_CUDA(cudaMemsetAsync(s->b_tring, 0xFF, sizeof(unsigned long long) * cap, h->stream));
+    if (g.tring_cap < cap || !g.tring) {
+        dfree(h->stream, g.tring);
+        g.tring_cap = 0;
+        if (dmalloc(h->stream, &g.tring, cap)) return DC_ERR_NOMEM;
+        g.tring_cap = cap;
+        DC_CUDA(cudaMemsetAsync(g.tring, 0xFF, sizeof(unsigned long long) * cap, h->stream));
     }
-    // the second stream must see these allocations and the ring's reset
-    DC_CUDA(cudaStreamSynchronize(h->stream));
     return DC_OK;
 }
 
@@ -1812,23 +1823,35 @@ int run_peel(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* 
     return DC_OK;
 }
 
-int build_skyline_from_log(dc_graph* h, uint64_t nlog, uint64_t off2, uint64_t n2, uint64_t void2) {
+// Skyline from row 0 and the corner logs of the last run of rows: the
+// first segment's nlog entries at the log's start and the other segments'
+// ranges (h->seg_off / seg_n, voided entries skipped).
+int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
     Scratch* s = h->scratch;
     Decomp& d = h->d;
     uint32_t V = h->g.V;
     unsigned long long* cnt = (unsigned long long*)s->tmp64;
+    uint64_t lo[kMaxRowSegments], n[kMaxRowSegments];
+    int nr = 0;
+    uint64_t total = (uint64_t)V;
+    if (nlog) {
+        lo[nr] = 0;
+        n[nr++] = nlog;
+        total += nlog;
+    }
+    for (int i = 0; i < h->nseg_extra; ++i)
+        if (h->seg_n[i]) {
+            lo[nr] = h->seg_off[i];
+            n[nr++] = h->seg_n[i];
+            total += h->seg_n[i] - h->seg_void[i];
+        }
     ++g_launches;
     k_set_one<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt);
-    if (nlog) {
+    for (int r = 0; r < nr; ++r) {
         ++g_launches;
-        k_sky_count<<<grid_for(h, nlog), kThreads, 0, h->stream>>>(V, nlog, s->log_v, s->log_k, cnt);
-    }
-    if (n2) {
-        ++g_launches;
-        k_sky_count<<<grid_for(h, n2), kThreads, 0, h->stream>>>(V, n2, s->log_v + off2, s->log_k + off2, cnt);
+        k_sky_count<<<grid_for(h, n[r]), kThreads, 0, h->stream>>>(V, n[r], s->log_v + lo[r], s->log_k + lo[r], cnt);
     }
     if (int rc = scan_tmp64(h, V)) return rc;
-    uint64_t total = (uint64_t)V + nlog + n2 - void2;
     if (d.corner_cap < total) {
         dfree(h->stream, d.sky_k);
         dfree(h->stream, d.sky_l);
@@ -1838,15 +1861,11 @@ int build_skyline_from_log(dc_graph* h, uint64_t nlog, uint64_t off2, uint64_t n
     if (!d.sky_off && dmalloc(h->stream, &d.sky_off, (uint64_t)V + 1)) return DC_ERR_NOMEM;
     ++g_launches;
     k_sky_fill_row0<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt, s->row0, d.sky_k, d.sky_l, s->cursor);
-    if (nlog) {
+    for (int r = 0; r < nr; ++r) {
         ++g_launches;
-        k_sky_fill_log<<<grid_for(h, nlog), kThreads, 0, h->stream>>>(nlog, s->log_v, s->log_k, s->log_l, cnt, d.sky_k,
-                                                                      d.sky_l, s->cursor);
-    }
-    if (n2) {
-        ++g_launches;
-        k_sky_fill_log<<<grid_for(h, n2), kThreads, 0, h->stream>>>(n2, s->log_v + off2, s->log_k + off2,
-                                                                    s->log_l + off2, cnt, d.sky_k, d.sky_l, s->cursor);
+        k_sky_fill_log<<<grid_for(h, n[r]), kThreads, 0, h->stream>>>(n[r], s->log_v + lo[r], s->log_k + lo[r],
+                                                                      s->log_l + lo[r], cnt, d.sky_k, d.sky_l,
+                                                                      s->cursor);
     }
     ++g_launches;
     k_sky_sort<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, cnt, d.sky_k, d.sky_l, d.sky_off);
@@ -1937,6 +1956,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     Scratch* s = h->scratch;
     const uint32_t V = g.V;
     *nlog_out = 0;
+    h->nseg_extra = 0;
     cudaEventRecord(h->ev[2], h->stream);
     if (s->ck_cap < (uint32_t)K + 2) {
         dfree(h->stream, s->ck);
@@ -1969,37 +1989,54 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     DC_CUDA(cudaMemcpyAsync(hist, start.data(), sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyHostToDevice, h->stream));
     ++g_launches;
     k_order_scatter<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist, s->order);
-    // a full run may be split in two row segments run concurrently: rows
-    // K0..split on the handle's stream and split+1..Kstop (jumping from row 0)
-    // on a second stream, each with its own state; the first segment's log
-    // takes [0, capA), the second [capA, lc)
+    // a full run may be split in row segments run concurrently: segment 0
+    // (rows K0..cut[0]) on the handle's stream, segment i (rows
+    // cut[i-1]+1..cut[i], jumping there from row 0) on seg[i-1]'s stream,
+    // each with its own state and its own range of the corner log
     const int32_t k0 = std::max(1, K0);
-    int32_t split = 0;
-    if (k0 == 1 && Kstop == K && h->rows_split > 0) {
-        split = (int32_t)((int64_t)K * h->rows_split / 1000);
-        if (split < 1 || split >= Kstop) split = 0;
-    }
+    int32_t cut[kMaxRowSegments];
+    int nseg = 1;
+    if (k0 == 1 && Kstop == K)
+        for (int i = 0; i < kMaxRowSegments - 1 && h->rows_split[i] > 0; ++i) {
+            const int32_t c = (int32_t)((int64_t)K * h->rows_split[i] / 1000);
+            if (c >= 1 && c < Kstop && (nseg == 1 || c > cut[nseg - 2])) cut[nseg++ - 1] = c;
+        }
+    cut[nseg - 1] = Kstop;
     int seg_bps = h->rows_bps;
-    if (split) {
-        // both segments' blocks must be resident together for their grid barriers
+    if (nseg > 1) {
+        // every segment's blocks must be resident together for their grid barriers
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_trans2, kThreads, 0) != cudaSuccess)
             per_sm = 0;
+        while (nseg > 1 && per_sm / nseg < 1) {
+            cut[nseg - 2] = Kstop;
+            --nseg;
+        }
         const int want = seg_bps > 0 ? seg_bps : (h->blocks_per_sm > 0 ? h->blocks_per_sm : kDefaultBlocksPerSm);
-        seg_bps = std::min(want, per_sm / 2);
-        if (seg_bps < 1) split = 0;
+        if (nseg > 1) seg_bps = std::min(want, per_sm / nseg);
     }
-    uint64_t lc = bound + 1, capA = lc;
-    if (split) {
-        DC_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(unsigned long long), h->stream));
+    // log ranges: [off[i], off[i] + cap[i]) per segment
+    uint64_t off[kMaxRowSegments] = {}, capn[kMaxRowSegments] = {};
+    uint64_t lc = bound + 1;
+    if (nseg > 1) {
+        SegBounds sb;
+        sb.n = nseg;
+        for (int i = 0; i < nseg; ++i) {
+            sb.lo[i] = i == 0 ? k0 : cut[i - 1] + 1;
+            sb.hi[i] = cut[i];
+        }
+        DC_CUDA(cudaMemsetAsync(acc, 0, nseg * sizeof(unsigned long long), h->stream));
         ++g_launches;
-        k_corner_bound_upto<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, s->row0, split, acc);
-        unsigned long long ba[2] = {0, 0};
-        DC_CUDA(cudaMemcpyAsync(ba, acc, sizeof(ba), cudaMemcpyDeviceToHost, h->stream));
+        k_corner_bounds<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, s->row0, sb, acc);
+        unsigned long long bs[kMaxRowSegments] = {};
+        DC_CUDA(cudaMemcpyAsync(bs, acc, nseg * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
         DC_CUDA(cudaStreamSynchronize(h->stream));
-        // the second segment's jump to row split+1 adds at most one corner per vertex
-        capA = ba[0] + 1;
-        lc = capA + ba[1] + V + 1;
+        lc = 0;
+        for (int i = 0; i < nseg; ++i) {
+            off[i] = lc;
+            capn[i] = bs[i] + 1;
+            lc += capn[i];
+        }
     }
     if (s->log_cap < lc) {
         dfree(h->stream, s->log_v);
@@ -2008,7 +2045,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
         if (dmalloc(h->stream, &s->log_v, lc) || dmalloc(h->stream, &s->log_k, lc) || dmalloc(h->stream, &s->log_l, lc)) return DC_ERR_NOMEM;
         s->log_cap = lc;
     }
-    if (!split) capA = s->log_cap;
+    if (nseg == 1) capn[0] = s->log_cap;
     // adjacency lists ordered by neighbour kmax (kept until the graph changes)
     int sorted = 0;
     if (allow_sort || g.sorted_kmax)
@@ -2020,101 +2057,123 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     DC_CUDA(cudaMemsetAsync(s->mark, 0, sizeof(uint32_t) * V, h->stream));
     DC_CUDA(cudaMemsetAsync(s->stamp, 0xFF, sizeof(int32_t) * V, h->stream));
     if (int rc = ensure_tring(h, 2ull * V + (uint64_t)h->geom.sms * 64 + 4096)) return rc;
-    Trans2Params tp;
-    tp.V = V;
-    tp.out_off = g.out_off; tp.out_len = g.out_len; tp.out_nbr = g.out_nbr;
-    tp.in_off = g.in_off; tp.in_len = g.in_len; tp.in_nbr = g.in_nbr;
-    tp.kmax = d.kmax_v;
-    tp.K = K;
-    tp.K0 = k0;
-    tp.Kstop = split ? split : Kstop;
-    tp.sorted = sorted;
-    tp.order = s->order;
-    tp.ck = s->ck;
-    tp.cur = s->cur;
-    tp.cnt_out = s->cnt_out;
-    tp.cnt_in = s->key;
-    tp.mark = s->mark;
-    tp.stamp = s->stamp;
-    tp.logidx = s->logidx;
-    tp.log_v = s->log_v;
-    tp.log_k = s->log_k;
-    tp.log_l = s->log_l;
-    tp.log_cap = capA;
-    tp.q.slots = s->tring;
-    tp.q.mask = (unsigned)(s->tring_cap - 1);
-    tp.ctl = h->ctl;
-    Trans2Params tb = tp;
-    if (split) {
-        if (int rc = ensure_segment_b(h, V)) return rc;
-        // the second segment starts once the shared preparation is done
-        DC_CUDA(cudaEventRecord(s->b_ev[0], h->stream));
-        DC_CUDA(cudaStreamWaitEvent(s->b_stream, s->b_ev[0], 0));
-        DC_CUDA(cudaMemcpyAsync(s->b_cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, s->b_stream));
-        ++g_launches;
-        k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, s->b_stream>>>(
-            V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, s->b_cur, s->b_cnt_out, s->b_cnt_in);
-        DC_CUDA(cudaMemsetAsync(s->b_mark, 0, sizeof(uint32_t) * V, s->b_stream));
-        DC_CUDA(cudaMemsetAsync(s->b_stamp, 0xFF, sizeof(int32_t) * V, s->b_stream));
-        tb.K0 = split + 1;
-        tb.Kstop = Kstop;
-        tb.cur = s->b_cur;
-        tb.cnt_out = s->b_cnt_out;
-        tb.cnt_in = s->b_cnt_in;
-        tb.mark = s->b_mark;
-        tb.stamp = s->b_stamp;
-        tb.logidx = s->b_logidx;
-        tb.log_v = s->log_v + capA;
-        tb.log_k = s->log_k + capA;
-        tb.log_l = s->log_l + capA;
-        tb.log_cap = s->log_cap - capA;
-        tb.q.slots = s->b_tring;
-        tb.q.mask = (unsigned)(s->b_tring_cap - 1);
-        tb.ctl = s->b_ctl;
+    Trans2Params tp[kMaxRowSegments];
+    tp[0].V = V;
+    tp[0].out_off = g.out_off; tp[0].out_len = g.out_len; tp[0].out_nbr = g.out_nbr;
+    tp[0].in_off = g.in_off; tp[0].in_len = g.in_len; tp[0].in_nbr = g.in_nbr;
+    tp[0].kmax = d.kmax_v;
+    tp[0].K = K;
+    tp[0].K0 = k0;
+    tp[0].Kstop = cut[0];
+    tp[0].sorted = sorted;
+    tp[0].order = s->order;
+    tp[0].ck = s->ck;
+    tp[0].cur = s->cur;
+    tp[0].cnt_out = s->cnt_out;
+    tp[0].cnt_in = s->key;
+    tp[0].mark = s->mark;
+    tp[0].stamp = s->stamp;
+    tp[0].logidx = s->logidx;
+    tp[0].log_v = s->log_v;
+    tp[0].log_k = s->log_k;
+    tp[0].log_l = s->log_l;
+    tp[0].log_cap = capn[0];
+    tp[0].q.slots = s->tring;
+    tp[0].q.mask = (unsigned)(s->tring_cap - 1);
+    tp[0].ctl = h->ctl;
+    for (int i = 1; i < nseg; ++i)
+        if (int rc = ensure_segment(h, i - 1, V)) return rc;
+    if (nseg > 1) {
+        // the other segments start once the shared preparation is done
+        DC_CUDA(cudaEventRecord(s->seg[0].ev[0], h->stream));
+        for (int i = 1; i < nseg; ++i) {
+            RowSegment& sg = s->seg[i - 1];
+            DC_CUDA(cudaStreamWaitEvent(sg.stream, s->seg[0].ev[0], 0));
+            DC_CUDA(cudaMemcpyAsync(sg.cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, sg.stream));
+            ++g_launches;
+            k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, sg.stream>>>(
+                V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, sg.cur, sg.cnt_out, sg.cnt_in);
+            DC_CUDA(cudaMemsetAsync(sg.mark, 0, sizeof(uint32_t) * V, sg.stream));
+            DC_CUDA(cudaMemsetAsync(sg.stamp, 0xFF, sizeof(int32_t) * V, sg.stream));
+            Trans2Params& t = tp[i];
+            t = tp[0];
+            t.K0 = cut[i - 1] + 1;
+            t.Kstop = cut[i];
+            t.cur = sg.cur;
+            t.cnt_out = sg.cnt_out;
+            t.cnt_in = sg.cnt_in;
+            t.mark = sg.mark;
+            t.stamp = sg.stamp;
+            t.logidx = sg.logidx;
+            t.log_v = s->log_v + off[i];
+            t.log_k = s->log_k + off[i];
+            t.log_l = s->log_l + off[i];
+            t.log_cap = capn[i];
+            t.q.slots = sg.tring;
+            t.q.mask = (unsigned)(sg.tring_cap - 1);
+            t.ctl = sg.ctl;
+        }
     }
-    uint64_t nlog = 0, n2 = 0;
-    unsigned long long void2 = 0;
+    uint64_t nlog = 0;
+    uint64_t nseg_log[kMaxRowSegments] = {};
+    unsigned long long voids[kMaxRowSegments] = {};
     cudaEventRecord(h->ev[3], h->stream);
-    if (tp.Kstop >= tp.K0) {
-        void* args[] = {&tp};
-        void* args_b[] = {&tb};
-        if (int rc = persistent_launch(h, (const void*)k_trans2, args, "transitions", h->ctl, h->stream, seg_bps))
-            return rc;
-        int rcb = DC_OK;
-        if (split)
-            rcb = persistent_launch(h, (const void*)k_trans2, args_b, "transitions (second segment)", s->b_ctl,
-                                    s->b_stream, seg_bps);
-        EngineCtl hc, hb;
-        int rc = finish_persistent(h, h->ctl, h->stream, "transitions", &hc);
-        if (split && rcb == DC_OK) rcb = finish_persistent(h, s->b_ctl, s->b_stream, "transitions (second segment)", &hb);
+    if (tp[0].Kstop >= tp[0].K0) {
+        static const char* const kNames[kMaxRowSegments] = {"transitions", "transitions (segment 2)",
+                                                             "transitions (segment 3)", "transitions (segment 4)"};
+        void* args[kMaxRowSegments][1];
+        int launched = 0, rc = DC_OK;
+        for (int i = 0; i < nseg && rc == DC_OK; ++i) {
+            args[i][0] = &tp[i];
+            EngineCtl* ctl = i == 0 ? h->ctl : s->seg[i - 1].ctl;
+            cudaStream_t st = i == 0 ? h->stream : s->seg[i - 1].stream;
+            rc = persistent_launch(h, (const void*)k_trans2, args[i], kNames[i], ctl, st, seg_bps);
+            if (rc == DC_OK) ++launched;
+        }
+        h->stat_evals = h->stat_drops = h->stat_entries = 0;
+        for (int i = 0; i < launched; ++i) {
+            EngineCtl hc;
+            EngineCtl* ctl = i == 0 ? h->ctl : s->seg[i - 1].ctl;
+            cudaStream_t st = i == 0 ? h->stream : s->seg[i - 1].stream;
+            const int r = finish_persistent(h, ctl, st, kNames[i], &hc);
+            if (r != DC_OK) {
+                if (rc == DC_OK) rc = r;
+                continue;
+            }
+            nseg_log[i] = hc.log_count;
+            h->stat_evals += hc.evals;
+            h->stat_drops += hc.drops;
+            h->stat_entries += hc.edges_scanned;
+        }
         if (rc) return rc;
-        if (rcb) return rcb;
-        nlog = hc.log_count;
-        h->stat_evals = hc.evals;
-        h->stat_drops = hc.drops;
-        h->stat_entries = hc.edges_scanned;
-        if (split) {
-            n2 = hb.log_count;
-            h->stat_evals += hb.evals;
-            h->stat_drops += hb.drops;
-            h->stat_entries += hb.edges_scanned;
-            DC_CUDA(cudaEventRecord(s->b_ev[1], s->b_stream));
-            DC_CUDA(cudaStreamWaitEvent(h->stream, s->b_ev[1], 0));
-            if (n2) {
-                DC_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), h->stream));
+        nlog = nseg_log[0];
+        if (nseg > 1) {
+            DC_CUDA(cudaMemsetAsync(acc, 0, nseg * sizeof(unsigned long long), h->stream));
+            for (int i = 1; i < nseg; ++i) {
+                RowSegment& sg = s->seg[i - 1];
+                DC_CUDA(cudaEventRecord(sg.ev[1], sg.stream));
+                DC_CUDA(cudaStreamWaitEvent(h->stream, sg.ev[1], 0));
+                if (!nseg_log[i]) continue;
+                // a corner at the segment's first row is void where the value
+                // equals the previous segment's last row
+                const int32_t* prev = i == 1 ? s->cur : s->seg[i - 2].cur;
                 ++g_launches;
-                k_seg_void<<<grid_for(h, n2), kThreads, 0, h->stream>>>(n2, s->log_v + capA, s->log_k + capA,
-                                                                        s->log_l + capA, split + 1, s->cur, acc);
-                DC_CUDA(cudaMemcpyAsync(&void2, acc, sizeof(void2), cudaMemcpyDeviceToHost, h->stream));
-                DC_CUDA(cudaStreamSynchronize(h->stream));
+                k_seg_void<<<grid_for(h, nseg_log[i]), kThreads, 0, h->stream>>>(
+                    nseg_log[i], s->log_v + off[i], s->log_k + off[i], s->log_l + off[i], cut[i - 1] + 1, prev,
+                    acc + i);
+            }
+            DC_CUDA(cudaMemcpyAsync(voids, acc, nseg * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+            DC_CUDA(cudaStreamSynchronize(h->stream));
+            h->nseg_extra = nseg - 1;
+            for (int i = 1; i < nseg; ++i) {
+                h->seg_off[i - 1] = off[i];
+                h->seg_n[i - 1] = nseg_log[i];
+                h->seg_void[i - 1] = voids[i];
             }
         }
     }
     cudaEventRecord(h->ev[4], h->stream);
     *nlog_out = nlog;
-    h->seg2_off = capA;
-    h->seg2_n = n2;
-    h->seg2_void = void2;
     return DC_OK;
 }
 
@@ -2210,7 +2269,7 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     uint64_t nlog = 0;
     if (int rc = rows_from_row0(h, K, K, true, &nlog)) return rc;
     if (int rc = degree_kmax_sum(h, &h->full_work)) return rc;
-    if (int rc = build_skyline_from_log(h, nlog, h->seg2_off, h->seg2_n, h->seg2_void)) return rc;
+    if (int rc = build_skyline_from_log(h, nlog)) return rc;
     cudaEventRecord(h->ev[5], h->stream);
     d.valid = true;
     if (materialize_rows) {
@@ -2321,7 +2380,7 @@ int decompose_range(dc_graph* h, int32_t k_first, int32_t k_last) {
     DC_CUDA(cudaMemcpyAsync(s->row0, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
     uint64_t nlog = 0;
     if (int rc = rows_from_row0(h, K, k1, true, &nlog, k0)) return rc;
-    if (int rc = build_skyline_from_log(h, nlog, h->seg2_off, h->seg2_n, h->seg2_void)) return rc;
+    if (int rc = build_skyline_from_log(h, nlog)) return rc;
     cudaEventRecord(h->ev[5], h->stream);
     DC_CUDA(cudaStreamSynchronize(h->stream));
     float ms = 0;

@@ -6,6 +6,24 @@
 
 namespace dc {
 
+// One row segment after the first: rows split over concurrent launches,
+// each segment with its own values, counters, marks, ticket ring, control
+// block and stream.
+struct RowSegment {
+    uint32_t cap_V = 0;
+    int32_t* cur = nullptr;
+    int32_t* cnt_out = nullptr;
+    int32_t* cnt_in = nullptr;
+    uint32_t* mark = nullptr;
+    int32_t* stamp = nullptr;
+    uint32_t* logidx = nullptr;
+    unsigned long long* tring = nullptr;
+    uint64_t tring_cap = 0;
+    EngineCtl* ctl = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
 struct Scratch {
     uint32_t cap_V = 0;
     int32_t* key = nullptr;      // [V] peeling degree / cnt_in
@@ -47,20 +65,8 @@ struct Scratch {
     // maintenance
     int32_t* kmax_old = nullptr;  // [V]
     int32_t* row0_old = nullptr;  // [V]
-    // second row segment: rows split over two concurrent launches, each
-    // with its own values, counters, marks, ticket ring and control block
-    uint32_t b_cap_V = 0;
-    int32_t* b_cur = nullptr;
-    int32_t* b_cnt_out = nullptr;
-    int32_t* b_cnt_in = nullptr;
-    uint32_t* b_mark = nullptr;
-    int32_t* b_stamp = nullptr;
-    uint32_t* b_logidx = nullptr;
-    unsigned long long* b_tring = nullptr;
-    uint64_t b_tring_cap = 0;
-    EngineCtl* b_ctl = nullptr;
-    cudaStream_t b_stream = nullptr;
-    cudaEvent_t b_ev[2] = {nullptr, nullptr};
+    // row segments after the first (rows split over concurrent launches)
+    RowSegment seg[kMaxRowSegments - 1];
 };
 
 // Allocation / release (all errors reported through set_error, return DC_*).
@@ -130,7 +136,7 @@ int check_ctl(dc_graph* h, EngineCtl* hc, const char* what);
 int scan_tmp64(dc_graph* h, uint64_t n);
 // Skyline from row 0 and the corner log: entries [0, nlog) and, when a second
 // row segment ran, [off2, off2 + n2).
-int build_skyline_from_log(dc_graph* h, uint64_t nlog, uint64_t off2 = 0, uint64_t n2 = 0, uint64_t void2 = 0);
+int build_skyline_from_log(dc_graph* h, uint64_t nlog);
 // kmax (in-degree peel) and row 0 (out-degree peel) of the current graph into
 // d.kmax_v and the scratch row 0; reports the largest values.
 int peel_kmax_row0(dc_graph* h, int32_t* kmax, int32_t* lmax);

@@ -110,13 +110,18 @@ struct dc_graph {
     int rows_bps = 0;          // the row kernel's blocks per SM (0 = blocks_per_sm)
     unsigned peel_chunk = 64;  // adjacency entries per peel work item
     int row_repair = 1;        // deletions: repair rows locally instead of recomputing
-    int rows_split = 0;        // full decompositions: rows split at kmax * rows_split / 1000 (0 = one run)
-    uint64_t seg2_off = 0, seg2_n = 0;  // second segment's corner log: [seg2_off, seg2_off + seg2_n)
-    uint64_t seg2_void = 0;             // entries of it voided (row k < 0)
+    // full decompositions: rows cut after kmax * rows_split[i] / 1000 for
+    // each nonzero entry (ascending), segments run concurrently
+    int rows_split[dc::kMaxRowSegments - 1] = {};
+    // corner logs of the segments after the first from the last run:
+    // [seg_off[i], seg_off[i] + seg_n[i]), seg_void[i] entries voided (row k < 0)
+    int nseg_extra = 0;
+    uint64_t seg_off[dc::kMaxRowSegments - 1] = {}, seg_n[dc::kMaxRowSegments - 1] = {},
+             seg_void[dc::kMaxRowSegments - 1] = {};
     uint64_t stat_evals = 0, stat_drops = 0, stat_entries = 0;
     uint64_t full_work = 0;  // sum over vertices of degree x kmax at the last full decomposition
     dc::EngineCtl ctl_init{};
-    dc::EngineCtl ctl_init_b{};  // the second row segment's
+    dc::EngineCtl ctl_init_seg[dc::kMaxRowSegments - 1] = {};  // the other row segments'
     // optional per-step trace of persistent kernels (diagnostics)
     unsigned long long* trace_dev = nullptr;
     unsigned long long* trace_host = nullptr;

@@ -1072,7 +1072,7 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
         d.sky_k = nullptr;
         d.sky_l = nullptr;
         d.corner_cap = 0;
-        rc = build_skyline_from_log(h, nlog, h->seg2_off, h->seg2_n, h->seg2_void);
+        rc = build_skyline_from_log(h, nlog);
         if (rc == DC_OK) {
             unsigned long long* cnt = (unsigned long long*)s->tmp64;
             ++g_launches;

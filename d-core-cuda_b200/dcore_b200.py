@@ -65,7 +65,11 @@ MAINT_AUTO, MAINT_LOCAL, MAINT_REPEEL = 0, 1, 2
 
 class Tuning(ctypes.Structure):
     _fields_ = [("peel_blocks_per_sm", ctypes.c_int32), ("rows_blocks_per_sm", ctypes.c_int32),
-                ("peel_chunk", ctypes.c_int32), ("rows_split_permille", ctypes.c_int32)]
+                ("peel_chunk", ctypes.c_int32), ("rows_split_permille", ctypes.c_int32 * 3)]
+
+    def as_dict(self):
+        return {"peel_blocks_per_sm": self.peel_blocks_per_sm, "rows_blocks_per_sm": self.rows_blocks_per_sm,
+                "peel_chunk": self.peel_chunk, "rows_split_permille": list(self.rows_split_permille)}
 
 
 class ServerInfo(ctypes.Structure):
@@ -554,10 +558,15 @@ class Graph:
     def tuning(self):
         t = Tuning()
         _check(lib().dc_get_tuning(self._h, ctypes.byref(t)))
-        return {f: getattr(t, f) for f, _ in Tuning._fields_}
+        return t.as_dict()
 
-    def set_tuning(self, peel_blocks_per_sm=2, rows_blocks_per_sm=2, peel_chunk=64, rows_split_permille=0):
-        t = Tuning(peel_blocks_per_sm, rows_blocks_per_sm, peel_chunk, rows_split_permille)
+    def set_tuning(self, peel_blocks_per_sm=2, rows_blocks_per_sm=2, peel_chunk=64, rows_split_permille=()):
+        """rows_split_permille: up to three ascending cuts (per mille of kmax)
+        splitting a full run of rows into concurrent launches; () = none."""
+        cuts = [rows_split_permille] if isinstance(rows_split_permille, int) else list(rows_split_permille)
+        if len(cuts) > 3:
+            raise DCoreError(-1, "at most three row cuts")
+        t = Tuning(peel_blocks_per_sm, rows_blocks_per_sm, peel_chunk, (ctypes.c_int32 * 3)(*(cuts + [0] * (3 - len(cuts)))))
         _check(lib().dc_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self):
@@ -566,7 +575,7 @@ class Graph:
         t = Tuning()
         ms = ctypes.c_float(0)
         _check(lib().dc_autotune(self._h, ctypes.byref(t), ctypes.byref(ms)))
-        return {f: getattr(t, f) for f, _ in Tuning._fields_}, ms.value
+        return t.as_dict(), ms.value
 
     def set_launch(self, blocks_per_sm):
         _check(lib().dc_set_launch(self._h, blocks_per_sm))
