@@ -525,7 +525,7 @@ extern "C" int dc_get_tuning(dc_graph* h, dc_tuning* t) {
     t->peel_blocks_per_sm = h->peel_bps > 0 ? h->peel_bps : dflt;
     t->rows_blocks_per_sm = h->rows_bps > 0 ? h->rows_bps : dflt;
     t->peel_chunk = (int32_t)h->peel_chunk;
-    for (int i = 0; i < 3; ++i) t->rows_split_permille[i] = h->rows_split[i];
+    for (int i = 0; i < kMaxRowSegments - 1; ++i) t->rows_split_permille[i] = h->rows_split[i];
     return DC_OK;
 }
 
@@ -536,10 +536,11 @@ extern "C" int dc_set_tuning(dc_graph* h, const dc_tuning* t) {
         return set_error(DC_ERR_INVALID, "dc_set_tuning: blocks per SM must be 1..8");
     if (t->peel_chunk < 16 || t->peel_chunk > 4096 || (t->peel_chunk & (t->peel_chunk - 1)))
         return set_error(DC_ERR_INVALID, "dc_set_tuning: peel_chunk must be a power of two in 16..4096");
-    static_assert(kMaxRowSegments - 1 == 3, "dc_tuning holds three row cuts");
-    for (int i = 0; i < 3; ++i) {
+    constexpr int kCuts = kMaxRowSegments - 1;
+    static_assert(sizeof(t->rows_split_permille) == kCuts * sizeof(int32_t), "dc_tuning holds one cut per extra segment");
+    for (int i = 0; i < kCuts; ++i) {
         const int32_t c = t->rows_split_permille[i];
-        const bool ok = c == 0 ? (i == 2 || t->rows_split_permille[i + 1] == 0)
+        const bool ok = c == 0 ? (i == kCuts - 1 || t->rows_split_permille[i + 1] == 0)
                                : (c <= 999 && (i == 0 || (t->rows_split_permille[i - 1] > 0 &&
                                                           c > t->rows_split_permille[i - 1])));
         if (c < 0 || !ok)
@@ -549,7 +550,7 @@ extern "C" int dc_set_tuning(dc_graph* h, const dc_tuning* t) {
     h->peel_bps = t->peel_blocks_per_sm;
     h->rows_bps = t->rows_blocks_per_sm;
     h->peel_chunk = (unsigned)t->peel_chunk;
-    for (int i = 0; i < 3; ++i) h->rows_split[i] = t->rows_split_permille[i];
+    for (int i = 0; i < kCuts; ++i) h->rows_split[i] = t->rows_split_permille[i];
     return DC_OK;
 }
 
@@ -601,41 +602,62 @@ extern "C" int dc_autotune(dc_graph* h, dc_tuning* best, float* best_ms) {
             pick.rows_blocks_per_sm = bps;
         }
     }
-    // row segments: one cut at a time (up to three), each the candidate
-    // that makes the rows fastest, while a new cut still helps
-    static const int32_t kCuts[] = {150, 200, 250, 300, 350, 400, 450, 500, 600, 700};
-    for (int level = 0; level < 3; ++level) {
-        int32_t best_cut = 0;
-        for (int32_t c : kCuts) {
-            dc_tuning t = pick;
-            int32_t v[4] = {0, 0, 0, 0};
-            int n = 0;
-            bool dup = false;
-            for (int i = 0; i < level; ++i) {
-                dup |= pick.rows_split_permille[i] == c;
-                v[n++] = pick.rows_split_permille[i];
+    // row segments: a run of rows 1..s costs C(s) and (starting from the
+    // vertices of C_{s+1} with the rest already left) rows s+1..kmax cost
+    // about C(kmax) - C(s), so segments balance where the cumulative cost
+    // splits evenly.  C is measured at cuts of 5..90 % of kmax; for one to
+    // three cuts the set with the smallest predicted longest segment is
+    // timed for real, and the fastest of those and no split stays.  (More
+    // segments share the SMs too thinly: at R-MAT 22 five to eight measured
+    // slower than four.)
+    constexpr int kGrid = 18;
+    int32_t grid[kGrid];
+    float cost[kGrid];
+    int ng = 0;
+    for (int g = 0; g < kGrid; ++g) {
+        const int32_t c = 50 * (g + 1);
+        const int32_t srow = (int32_t)((int64_t)K * c / 1000);
+        if (srow < 1 || srow >= K || (ng && srow == (int32_t)((int64_t)K * grid[ng - 1] / 1000))) continue;
+        if (int rc = decompose_range(h, 1, srow)) return rc;
+        grid[ng] = c;
+        cost[ng++] = h->times.trans_ms;
+    }
+    const float total = rows_best;
+    constexpr int kCuts = kMaxRowSegments - 1, kTunedCuts = 3;
+    for (int ncut = 1; ncut <= kTunedCuts && ncut <= ng; ++ncut) {
+        // smallest predicted longest segment over all ncut-subsets of the grid
+        float best_pred = 1e30f;
+        int sel[kCuts] = {}, cur[kCuts] = {};
+        for (int q = 0; q < ncut; ++q) cur[q] = q;
+        for (;;) {
+            float prev = 0.f, longest = 0.f;
+            for (int q = 0; q < ncut; ++q) {
+                longest = std::max(longest, cost[cur[q]] - prev);
+                prev = cost[cur[q]];
             }
-            if (dup) continue;
-            v[n++] = c;
-            std::sort(v, v + n);
-            for (int i = 0; i < 3; ++i) t.rows_split_permille[i] = v[i];
-            if (dc_set_tuning(h, &t) != DC_OK) continue;
-            float ms = 1e30f;
-            for (int r = 0; r < 2; ++r) {
-                if (int rc = decompose_range(h, 1, K)) return rc;
-                ms = std::min(ms, h->times.trans_ms);
+            longest = std::max(longest, total - prev);
+            if (longest < best_pred) {
+                best_pred = longest;
+                for (int q = 0; q < ncut; ++q) sel[q] = cur[q];
             }
-            if (ms < rows_best) {
-                rows_best = ms;
-                best_cut = c;
-            }
+            int q = ncut - 1;
+            while (q >= 0 && cur[q] == ng - ncut + q) --q;
+            if (q < 0) break;
+            ++cur[q];
+            for (int r = q + 1; r < ncut; ++r) cur[r] = cur[r - 1] + 1;
         }
-        if (!best_cut) break;
-        int32_t v[4] = {0, 0, 0, 0};
-        for (int i = 0; i < level; ++i) v[i] = pick.rows_split_permille[i];
-        v[level] = best_cut;
-        std::sort(v, v + level + 1);
-        for (int i = 0; i < 3; ++i) pick.rows_split_permille[i] = v[i];
+        dc_tuning t = pick;
+        for (int q = 0; q < kCuts; ++q) t.rows_split_permille[q] = q < ncut ? grid[sel[q]] : 0;
+        if (dc_set_tuning(h, &t) != DC_OK) continue;
+        float ms = 1e30f;
+        for (int r = 0; r < 3; ++r) {
+            if (int rc = decompose_range(h, 1, K)) return rc;
+            ms = std::min(ms, h->times.trans_ms);
+        }
+        if (ms < rows_best) {
+            rows_best = ms;
+            for (int q = 0; q < kCuts; ++q) pick.rows_split_permille[q] = t.rows_split_permille[q];
+        }
     }
     dc_set_tuning(h, &pick);
     if (int rc = decompose(h, 0, 0)) return rc;

@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
 struct Trans2Params {
     uint32_t V;
     const uint32_t* out_off;
-    int32_t* out_len;  // working copies, pruned in place
+    int32_t* out_len;
     uint32_t* out_nbr;
     const uint32_t* in_off;
     int32_t* in_len;
@@ -492,6 +492,10 @@ struct Trans2Params {
     const int32_t* kmax;
     int32_t K;
     int32_t K0;     // first row to compute; cur holds row 0 (K0 > 1 jumps straight to row K0)
+    // K0 > 1 only: cur already holds -1 for the vertices outside C_K0 and the
+    // counters ignore them, so the first row has no leaving set and seeds
+    // every member whose out-count is below its value as well
+    int preleft;
     int32_t Kstop;  // last row to compute (rows above stay untouched)
     int sorted;     // lists ordered by neighbour kmax, descending
     const uint32_t* order;
@@ -530,7 +534,16 @@ struct TransHook {
     }
 };
 
-// Counters of v against every neighbour, at v's row-0 value.
+// Starting values of a run of rows that jumps to row a: row 0 inside C_a,
+// -1 (left) outside.
+__global__ void k_preleft_cur(uint32_t V, const int32_t* kmax, const int32_t* row0, int32_t a, int32_t* cur) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+        cur[v] = kmax[v] >= a ? row0[v] : -1;
+}
+
+// Counters of v against every neighbour, at v's starting value (vertices
+// with a value below 1 get zero counts: they are never evaluated and no
+// counter includes them).
 __global__ void k_counters_init(uint32_t V, const uint32_t* out_off, const int32_t* out_len, const uint32_t* out_nbr,
                                 const uint32_t* in_off, const int32_t* in_len, const uint32_t* in_nbr,
                                 const int32_t* cur, int32_t* cnt_out, int32_t* cnt_in) {
@@ -540,6 +553,13 @@ __global__ void k_counters_init(uint32_t V, const uint32_t* out_off, const int32
     for (uint64_t v = gw; v < V; v += nw) {
         int cv = cur[v];
         int co = 0, ci = 0;
+        if (cv < 1) {  // never evaluated, never counted: no support needed
+            if (lane == 0) {
+                cnt_out[v] = 0;
+                cnt_in[v] = 0;
+            }
+            continue;
+        }
         uint32_t o = out_off[v];
         int n = out_len[v];
         for (int i = lane; i < n; i += 32) co += (cur[out_nbr[o + i]] >= cv);
@@ -710,7 +730,8 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
     if (threadIdx.x == 0) s_prod = 0;
     if (!grid_sync_hook(c, hook)) return;
 
-    int jprev = 0;  // row currently held in cur
+    int jprev = p.preleft ? p.K0 : 0;  // row currently held in cur
+    bool seed_out = p.preleft != 0;
     for (;;) {
         const int j = ld_vol(&c->level);
         if (j > p.Kstop) break;
@@ -781,9 +802,10 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
             uint32_t v = 0;
             if (i < vj) {
                 v = p.order[i];
-                if (ld_vol(&p.cur[v]) >= 1) {
+                const int cv = ld_vol(&p.cur[v]);
+                if (cv >= 1) {
                     int ci = ld_vol(&p.cnt_in[v]);
-                    if (ci < j) req = mark_request(&p.mark[v], c);
+                    if (ci < j || (seed_out && ld_vol(&p.cnt_out[v]) < cv)) req = mark_request(&p.mark[v], c);
                     else jmin = min(jmin, min(ci, p.kmax[v]) + 1);
                 }
             }
@@ -951,6 +973,7 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
             if (lane == 0) tq_finish(c, 1);
         }
         jprev = j;
+        seed_out = false;
         if (!grid_sync_hook(c, hook)) break;
     }
     if (lane == 0) {
@@ -2050,12 +2073,24 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     int sorted = 0;
     if (allow_sort || g.sorted_kmax)
         if (int rc = sort_lists_by_kmax(h, K, &sorted)) return rc;
-    DC_CUDA(cudaMemcpyAsync(s->cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, h->stream));
-    ++g_launches;
-    k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, h->stream>>>(
-        V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, s->cur, s->cnt_out, s->key);
-    DC_CUDA(cudaMemsetAsync(s->mark, 0, sizeof(uint32_t) * V, h->stream));
-    DC_CUDA(cudaMemsetAsync(s->stamp, 0xFF, sizeof(int32_t) * V, h->stream));
+    // starting values and counters of a run that starts at row a: row 0,
+    // or (a > 1) row 0 inside C_a with the vertices outside already left
+    auto start_state = [&](cudaStream_t st, int32_t a, int32_t* cur, int32_t* co, int32_t* ci, uint32_t* mark,
+                           int32_t* stamp) -> int {
+        if (a > 1) {
+            ++g_launches;
+            k_preleft_cur<<<grid_for(h, V), kThreads, 0, st>>>(V, d.kmax_v, s->row0, a, cur);
+        } else {
+            DC_CUDA(cudaMemcpyAsync(cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, st));
+        }
+        ++g_launches;
+        k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, st>>>(
+            V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, cur, co, ci);
+        DC_CUDA(cudaMemsetAsync(mark, 0, sizeof(uint32_t) * V, st));
+        DC_CUDA(cudaMemsetAsync(stamp, 0xFF, sizeof(int32_t) * V, st));
+        return DC_OK;
+    };
+    if (int rc = start_state(h->stream, k0, s->cur, s->cnt_out, s->key, s->mark, s->stamp)) return rc;
     if (int rc = ensure_tring(h, 2ull * V + (uint64_t)h->geom.sms * 64 + 4096)) return rc;
     Trans2Params tp[kMaxRowSegments];
     tp[0].V = V;
@@ -2064,6 +2099,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     tp[0].kmax = d.kmax_v;
     tp[0].K = K;
     tp[0].K0 = k0;
+    tp[0].preleft = k0 > 1;
     tp[0].Kstop = cut[0];
     tp[0].sorted = sorted;
     tp[0].order = s->order;
@@ -2089,15 +2125,12 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
         for (int i = 1; i < nseg; ++i) {
             RowSegment& sg = s->seg[i - 1];
             DC_CUDA(cudaStreamWaitEvent(sg.stream, s->seg[0].ev[0], 0));
-            DC_CUDA(cudaMemcpyAsync(sg.cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, sg.stream));
-            ++g_launches;
-            k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, sg.stream>>>(
-                V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, sg.cur, sg.cnt_out, sg.cnt_in);
-            DC_CUDA(cudaMemsetAsync(sg.mark, 0, sizeof(uint32_t) * V, sg.stream));
-            DC_CUDA(cudaMemsetAsync(sg.stamp, 0xFF, sizeof(int32_t) * V, sg.stream));
+            if (int rc = start_state(sg.stream, cut[i - 1] + 1, sg.cur, sg.cnt_out, sg.cnt_in, sg.mark, sg.stamp))
+                return rc;
             Trans2Params& t = tp[i];
             t = tp[0];
             t.K0 = cut[i - 1] + 1;
+            t.preleft = 1;
             t.Kstop = cut[i];
             t.cur = sg.cur;
             t.cnt_out = sg.cnt_out;
@@ -2119,8 +2152,11 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     unsigned long long voids[kMaxRowSegments] = {};
     cudaEventRecord(h->ev[3], h->stream);
     if (tp[0].Kstop >= tp[0].K0) {
-        static const char* const kNames[kMaxRowSegments] = {"transitions", "transitions (segment 2)",
-                                                             "transitions (segment 3)", "transitions (segment 4)"};
+        static const char* const kNames[8] = {"transitions",           "transitions (segment 2)",
+                                              "transitions (segment 3)", "transitions (segment 4)",
+                                              "transitions (segment 5)", "transitions (segment 6)",
+                                              "transitions (segment 7)", "transitions (segment 8)"};
+        static_assert(kMaxRowSegments <= 8, "one name per segment");
         void* args[kMaxRowSegments][1];
         int launched = 0, rc = DC_OK;
         for (int i = 0; i < nseg && rc == DC_OK; ++i) {

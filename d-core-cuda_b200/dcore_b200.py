@@ -65,7 +65,7 @@ MAINT_AUTO, MAINT_LOCAL, MAINT_REPEEL = 0, 1, 2
 
 class Tuning(ctypes.Structure):
     _fields_ = [("peel_blocks_per_sm", ctypes.c_int32), ("rows_blocks_per_sm", ctypes.c_int32),
-                ("peel_chunk", ctypes.c_int32), ("rows_split_permille", ctypes.c_int32 * 3)]
+                ("peel_chunk", ctypes.c_int32), ("rows_split_permille", ctypes.c_int32 * 7)]
 
     def as_dict(self):
         return {"peel_blocks_per_sm": self.peel_blocks_per_sm, "rows_blocks_per_sm": self.rows_blocks_per_sm,
@@ -561,12 +561,12 @@ class Graph:
         return t.as_dict()
 
     def set_tuning(self, peel_blocks_per_sm=2, rows_blocks_per_sm=2, peel_chunk=64, rows_split_permille=()):
-        """rows_split_permille: up to three ascending cuts (per mille of kmax)
+        """rows_split_permille: up to seven ascending cuts (per mille of kmax)
         splitting a full run of rows into concurrent launches; () = none."""
         cuts = [rows_split_permille] if isinstance(rows_split_permille, int) else list(rows_split_permille)
-        if len(cuts) > 3:
-            raise DCoreError(-1, "at most three row cuts")
-        t = Tuning(peel_blocks_per_sm, rows_blocks_per_sm, peel_chunk, (ctypes.c_int32 * 3)(*(cuts + [0] * (3 - len(cuts)))))
+        if len(cuts) > 7:
+            raise DCoreError(-1, "at most seven row cuts")
+        t = Tuning(peel_blocks_per_sm, rows_blocks_per_sm, peel_chunk, (ctypes.c_int32 * 7)(*(cuts + [0] * (7 - len(cuts)))))
         _check(lib().dc_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self):

@@ -377,21 +377,23 @@ typedef struct dc_tuning {
     int32_t peel_chunk;         /* power of two, 16..4096 */
     /* Row segments of a full decomposition: each nonzero s cuts rows 1..kmax
      * after row kmax*s/1000, and the segments run as concurrent launches
-     * (each one after the first starts from row 0).  Nonzero entries are
-     * strictly ascending in 1..999 and precede the zeros; all zero = one
-     * launch. */
-    int32_t rows_split_permille[3];
+     * (each one after the first starts from row 0 inside its first row's
+     * core).  Nonzero entries are strictly ascending in 1..999 and precede
+     * the zeros; all zero = one launch.  Segments share the SMs: each gets
+     * at most 1/n of the row kernel's resident blocks. */
+    int32_t rows_split_permille[7];
 } dc_tuning;
 int dc_get_tuning(dc_graph* g, dc_tuning* t);
 int dc_set_tuning(dc_graph* g, const dc_tuning* t);
 /* Autotuner: times the decomposition of this graph under candidate launch
  * shapes (peel grid 1..6 blocks per SM x chunk 32..256 on the peel alone,
- * then the row kernel's grid 1..8 blocks per SM on the rows alone, then row
- * segments: cuts at 15..70 % of kmax added one at a time while the rows get
- * faster, up to three; each candidate twice, grids capped by occupancy),
- * keeps the fastest on the handle and ends with a full decomposition.
- * *best / *best_ms (may be NULL): the chosen setting and its peel + rows
- * device time. */
+ * then the row kernel's grid 1..8 blocks per SM on the rows alone, each
+ * candidate twice, grids capped by occupancy), then row segments: the
+ * cumulative cost of rows 1..s is measured at cuts of 5..90 % of kmax (in
+ * steps of 5 %), and for one to three cuts the set that balances the
+ * segments best is timed (three times); keeps the fastest on the handle and ends with a
+ * full decomposition.  *best / *best_ms (may be NULL): the chosen setting and
+ * its peel + rows device time. */
 int dc_autotune(dc_graph* g, dc_tuning* best, float* best_ms);
 
 /* Engine kernel launches since the library was loaded. */
