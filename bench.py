@@ -713,6 +713,9 @@ def main():
                     help="maintenance: recompute rows 1..R for deletions instead of repairing them in place")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="decomposition: keep the default launch shapes instead of running dc_autotune first")
+    ap.add_argument("--tuning", default="",
+                    help="decomposition launch shapes instead of the autotuner: "
+                         "peel_bps,rows_bps,chunk[,cut1,...] (cuts in per mille of kmax)")
     ap.add_argument("--emulate-ranks", type=int, default=0,
                     help="row sharding of one decomposition over N ranks, run one range after another on one GPU")
     args = ap.parse_args()
@@ -752,7 +755,15 @@ def main():
     E = int(len(s))
     g = dc.Graph.from_edges(V, s, d, device=local)
     stream = torch.cuda.ExternalStream(g.stream())
-    tuning, tune_ms = (g.autotune() if args.autotune else (g.tuning(), None))
+    if args.tuning:
+        f = [int(x) for x in args.tuning.split(",")]
+        g.set_tuning(f[0], f[1], f[2], f[3:])
+        tuning, tune_ms, tune_src = g.tuning(), None, "given (--tuning)"
+    elif args.autotune:
+        tuning, tune_ms = g.autotune()
+        tune_src = "autotuner (dc_autotune) before the timed steps"
+    else:
+        tuning, tune_ms, tune_src = g.tuning(), None, "defaults"
 
     def step():
         g.decompose(dc.METHOD_INCREMENTAL)
@@ -811,8 +822,12 @@ def main():
     ach = kernels[dom]["bytes"] / (kernels[dom]["ms"] / 1000.0) / 1e9
     b_alg = model["B_K"] + float(np.sum(model["B_row"]))
     touched = 8.0 * inf.get("entries", 0) + 16.0 * inf["evals"]
+    nseg = 1 + sum(1 for c in tuning["rows_split_permille"] if c)
     roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
             "peak_source": peak_kind, "traffic": kernel_traffic(dom, args.workload),
+            "k_trans2_launches_per_step": nseg,
+            "timing": "CUDA events on the graph's stream around each phase; the rows phase spans all of its "
+                      "k_trans2 launches (row segments on concurrent streams joined back to the graph's stream)",
             "model": "per-row peel bytes: B_K = 12E + 16V; B_k = 8 D_k + 16 I_k + 24 V_k + 4 (V - V_k)",
             "decomposition": {"alg_bytes": b_alg, "ms": ms_per_step,
                               "achieved_gbs": b_alg / (ms_per_step / 1000.0) / 1e9,
@@ -839,6 +854,8 @@ def main():
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             g2 = dc.Graph.from_edges(V, hs, hd, device=local)
+            g2.set_tuning(tuning["peel_blocks_per_sm"], tuning["rows_blocks_per_sm"], tuning["peel_chunk"],
+                          tuning["rows_split_permille"])
             k2, _ = g2.decompose(dc.METHOD_INCREMENTAL)
             g2.kmaxes(out=hk)
             g2.rows(0, k2 + 1, out=hrows[:k2 + 1])
@@ -868,8 +885,7 @@ def main():
                            "l2": "inputs larger than L2 (graph %.0f MB, rows %.0f MB)" % (
                                8.0 * E / 2**20, 4.0 * (K + 1) * V / 2**20),
                            "parallelism": f"replicas x{world}",
-                           "tuning": dict(tuning, source="autotuner (dc_autotune) before the timed steps"
-                                          if args.autotune else "defaults")},
+                           "tuning": dict(tuning, source=tune_src)},
                 "phases_ms": {"peel": peel_ms, "rows": rows_ms,
                               "other": ms_per_step - peel_ms - rows_ms},
                 "gpu_launches": int(launches), "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
