@@ -299,6 +299,16 @@ def run_maintenance(args, w, rank, world, local):
     u, v, dl = dc.gen_updates(V, s, d, w["ops"], 0.5, w["seed"] + 1000 + rank)
     g = dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16)
     g.set_row_repair(args.row_repair)
+    if args.tuning:
+        f = [int(x) for x in args.tuning.split(",")]
+        g.set_tuning(f[0], f[1], f[2], f[3:])
+        tune_src = "given (--tuning)"
+    elif args.autotune:
+        g.autotune()  # launch shapes and row cuts of the recomputations, chosen on the initial graph
+        tune_src = "autotuner (dc_autotune) on the initial graph, before the timed batches"
+    else:
+        tune_src = "defaults"
+    tuning = g.tuning()
     g.decompose(dc.METHOD_INCREMENTAL)
     sampler = ClockSampler(local)
     launches0 = dc.launch_count()
@@ -334,7 +344,7 @@ def run_maintenance(args, w, rank, world, local):
                        "headline": "batches of 10,000 updates", "per_batch_size": per_size,
                        "exactness": "each batch leaves kmaxes and rows equal to a full recomputation",
                        "method": {0: "scheduler", 1: "local", 2: "re-peel"}[args.maint_method],
-                       "row_repair": bool(args.row_repair)},
+                       "row_repair": bool(args.row_repair), "tuning": dict(tuning, source=tune_src)},
             "gpu_launches": int(launches), "clocks": clocks}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -551,7 +551,8 @@ extern "C" int dc_set_tuning(dc_graph* h, const dc_tuning* t) {
     h->rows_bps = t->rows_blocks_per_sm;
     h->peel_chunk = (unsigned)t->peel_chunk;
     for (int i = 0; i < kCuts; ++i) h->rows_split[i] = t->rows_split_permille[i];
-    return DC_OK;
+    API_CUDA(cudaSetDevice(h->device));
+    return prepare_row_segments(h);
 }
 
 // Coordinate search: the fused peel's grid and chunk size timed on the peel

@@ -1782,6 +1782,21 @@ static int ensure_segment(dc_graph* h, int i, uint32_t V) {
     return DC_OK;
 }
 
+// Allocates the state of the row segments the handle's cuts ask for, so
+// that no later run of rows allocates it (maintenance batches included).
+int prepare_row_segments(dc_graph* h) {
+    const uint32_t V = h->g.V;
+    if (!V) return DC_OK;
+    int n = 0;
+    while (n < kMaxRowSegments - 1 && h->rows_split[n] > 0) ++n;
+    if (!n) return DC_OK;
+    if (int rc = ensure_scratch(h, V)) return rc;
+    for (int i = 0; i < n; ++i)
+        if (int rc = ensure_segment(h, i, V)) return rc;
+    DC_CUDA(cudaStreamSynchronize(h->stream));
+    return DC_OK;
+}
+
 PeelInst make_inst(dc_graph* h, int which, const int32_t* member, int32_t k, int32_t* val, int slot) {
     DevGraph& g = h->g;
     Scratch* s = h->scratch;
@@ -2012,14 +2027,17 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     DC_CUDA(cudaMemcpyAsync(hist, start.data(), sizeof(uint32_t) * ((size_t)K + 2), cudaMemcpyHostToDevice, h->stream));
     ++g_launches;
     k_order_scatter<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, d.kmax_v, hist, s->order);
-    // a full run may be split in row segments run concurrently: segment 0
-    // (rows K0..cut[0]) on the handle's stream, segment i (rows
-    // cut[i-1]+1..cut[i], jumping there from row 0) on seg[i-1]'s stream,
-    // each with its own state and its own range of the corner log
+    // a run from row 1 (a full decomposition, or rows 1..R of a maintenance
+    // batch) may be split in row segments run concurrently: segment 0 (rows
+    // 1..cut[0]) on the handle's stream, segment i (rows cut[i-1]+1..cut[i],
+    // starting there from row 0) on seg[i-1]'s stream, each with its own
+    // state and its own range of the corner log; runs of fewer than
+    // kMinSplitRows rows stay whole
+    constexpr int32_t kMinSplitRows = 32;
     const int32_t k0 = std::max(1, K0);
     int32_t cut[kMaxRowSegments];
     int nseg = 1;
-    if (k0 == 1 && Kstop == K)
+    if (k0 == 1 && Kstop >= kMinSplitRows)
         for (int i = 0; i < kMaxRowSegments - 1 && h->rows_split[i] > 0; ++i) {
             const int32_t c = (int32_t)((int64_t)K * h->rows_split[i] / 1000);
             if (c >= 1 && c < Kstop && (nseg == 1 || c > cut[nseg - 2])) cut[nseg++ - 1] = c;
@@ -2062,11 +2080,14 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
         }
     }
     if (s->log_cap < lc) {
+        // a quarter of headroom: later runs (maintenance batches) rarely grow it again
+        const uint64_t cap = lc + lc / 4;
         dfree(h->stream, s->log_v);
         dfree(h->stream, s->log_k);
         dfree(h->stream, s->log_l);
-        if (dmalloc(h->stream, &s->log_v, lc) || dmalloc(h->stream, &s->log_k, lc) || dmalloc(h->stream, &s->log_l, lc)) return DC_ERR_NOMEM;
-        s->log_cap = lc;
+        s->log_cap = 0;
+        if (dmalloc(h->stream, &s->log_v, cap) || dmalloc(h->stream, &s->log_k, cap) || dmalloc(h->stream, &s->log_l, cap)) return DC_ERR_NOMEM;
+        s->log_cap = cap;
     }
     if (nseg == 1) capn[0] = s->log_cap;
     // adjacency lists ordered by neighbour kmax (kept until the graph changes)

@@ -137,6 +137,7 @@ int scan_tmp64(dc_graph* h, uint64_t n);
 // Skyline from row 0 and the corner log: entries [0, nlog) and, when a second
 // row segment ran, [off2, off2 + n2).
 int build_skyline_from_log(dc_graph* h, uint64_t nlog);
+int prepare_row_segments(dc_graph* h);
 // kmax (in-degree peel) and row 0 (out-degree peel) of the current graph into
 // d.kmax_v and the scratch row 0; reports the largest values.
 int peel_kmax_row0(dc_graph* h, int32_t* kmax, int32_t* lmax);
