@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <cmath>
 #include <vector>
 #include <sys/stat.h>
 
@@ -555,6 +556,53 @@ extern "C" int dc_set_tuning(dc_graph* h, const dc_tuning* t) {
     return prepare_row_segments(h);
 }
 
+// Smallest largest-segment cost over ncut cuts taken from the grid: best[j][i]
+// = the best largest cost of rows 1..s_i cut j times with the last cut at i,
+// best[j][i] = min over p < i of max(best[j-1][p], cost[i] - cost[p]); the
+// last segment adds total - cost[i].  O(ncut n^2); ties keep the lower cut.
+extern "C" int dc_plan_row_cuts(const int32_t* grid, const float* cost, int32_t n, float total, int32_t ncut,
+                                int32_t* cuts, float* longest) {
+    constexpr int kCuts = kMaxRowSegments - 1;
+    if (!grid || !cost || !cuts) return set_error(DC_ERR_INVALID, "dc_plan_row_cuts: null argument");
+    if (n < 1 || n > 4096 || ncut < 1 || ncut > kCuts || ncut > n)
+        return set_error(DC_ERR_INVALID, "dc_plan_row_cuts: need 1 <= n <= 4096 and 1 <= ncut <= min(n, %d)", kCuts);
+    for (int i = 0; i < n; ++i)
+        if (grid[i] < 1 || grid[i] > 999 || (i && grid[i] <= grid[i - 1]))
+            return set_error(DC_ERR_INVALID, "dc_plan_row_cuts: grid must be strictly ascending in 1..999");
+    std::vector<float> best((size_t)ncut * n);
+    std::vector<int32_t> from((size_t)ncut * n, -1);
+    for (int i = 0; i < n; ++i) best[i] = cost[i];
+    for (int j = 1; j < ncut; ++j)
+        for (int i = 0; i < n; ++i) {
+            float b = INFINITY;
+            int32_t arg = -1;
+            for (int p = j - 1; p < i; ++p) {
+                const float v = std::max(best[(size_t)(j - 1) * n + p], cost[i] - cost[p]);
+                if (v < b) {
+                    b = v;
+                    arg = p;
+                }
+            }
+            best[(size_t)j * n + i] = b;
+            from[(size_t)j * n + i] = arg;
+        }
+    float b = INFINITY;
+    int32_t last = -1;
+    for (int i = ncut - 1; i < n; ++i) {
+        const float v = std::max(best[(size_t)(ncut - 1) * n + i], total - cost[i]);
+        if (v < b) {
+            b = v;
+            last = i;
+        }
+    }
+    for (int j = ncut - 1; j >= 0; --j) {
+        cuts[j] = grid[last];
+        last = from[(size_t)j * n + last];
+    }
+    if (longest) *longest = b;
+    return DC_OK;
+}
+
 // Coordinate search: the fused peel's grid and chunk size timed on the peel
 // alone, then the row kernel's grid timed on the rows alone (kmax and row 0
 // reused); every candidate runs twice and keeps its faster time.  The
@@ -627,29 +675,10 @@ extern "C" int dc_autotune(dc_graph* h, dc_tuning* best, float* best_ms) {
     const float total = rows_best;
     constexpr int kCuts = kMaxRowSegments - 1, kTunedCuts = 3;
     for (int ncut = 1; ncut <= kTunedCuts && ncut <= ng; ++ncut) {
-        // smallest predicted longest segment over all ncut-subsets of the grid
-        float best_pred = 1e30f;
-        int sel[kCuts] = {}, cur[kCuts] = {};
-        for (int q = 0; q < ncut; ++q) cur[q] = q;
-        for (;;) {
-            float prev = 0.f, longest = 0.f;
-            for (int q = 0; q < ncut; ++q) {
-                longest = std::max(longest, cost[cur[q]] - prev);
-                prev = cost[cur[q]];
-            }
-            longest = std::max(longest, total - prev);
-            if (longest < best_pred) {
-                best_pred = longest;
-                for (int q = 0; q < ncut; ++q) sel[q] = cur[q];
-            }
-            int q = ncut - 1;
-            while (q >= 0 && cur[q] == ng - ncut + q) --q;
-            if (q < 0) break;
-            ++cur[q];
-            for (int r = q + 1; r < ncut; ++r) cur[r] = cur[r - 1] + 1;
-        }
+        int32_t sel[kCuts] = {};
+        if (dc_plan_row_cuts(grid, cost, ng, total, ncut, sel, nullptr) != DC_OK) break;
         dc_tuning t = pick;
-        for (int q = 0; q < kCuts; ++q) t.rows_split_permille[q] = q < ncut ? grid[sel[q]] : 0;
+        for (int q = 0; q < kCuts; ++q) t.rows_split_permille[q] = q < ncut ? sel[q] : 0;
         if (dc_set_tuning(h, &t) != DC_OK) continue;
         float ms = 1e30f;
         for (int r = 0; r < 3; ++r) {

@@ -156,6 +156,7 @@ SIGNATURES = {
     "dc_server_free": [vp],
     "dc_server_set_row_repair": [vp, ctypes.c_int],
     "dc_kmax_noalloc": [ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp, vp, i32p, vp],
+    "dc_plan_row_cuts": [i32p, f32p, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, i32p, f32p],
     "dc_launch_count": [u64p],
     "dc_last_error": [],
     "dc_version": [],
@@ -199,6 +200,18 @@ def launch_count():
     n = ctypes.c_uint64(0)
     _check(lib().dc_launch_count(ctypes.byref(n)))
     return n.value
+
+
+def plan_row_cuts(grid, cost, total, ncut):
+    """dc_plan_row_cuts: the ncut grid values (per mille of kmax) whose
+    segments' largest predicted cost is smallest; returns (cuts, that cost)."""
+    g = np.ascontiguousarray(grid, np.int32)
+    c = np.ascontiguousarray(cost, np.float32)
+    out = np.zeros(max(int(ncut), 1), np.int32)
+    lo = ctypes.c_float(0)
+    _check(lib().dc_plan_row_cuts(_p(g, i32p), _p(c, f32p), len(g), float(total), int(ncut), _p(out, i32p),
+                                  ctypes.byref(lo)))
+    return out[:ncut].tolist(), lo.value
 
 
 def device_count():

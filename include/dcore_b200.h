@@ -395,6 +395,15 @@ int dc_set_tuning(dc_graph* g, const dc_tuning* t);
  * full decomposition.  *best / *best_ms (may be NULL): the chosen setting and
  * its peel + rows device time. */
 int dc_autotune(dc_graph* g, dc_tuning* best, float* best_ms);
+/* Row cuts that balance a run of rows over concurrent segments (host only;
+ * the autotuner's planner).  cost[i] = measured cost of rows 1..s_i, s_i =
+ * kmax * grid[i] / 1000 (grid strictly ascending in 1..999, n in 1..4096);
+ * total = cost of all rows.  A segment from cut a to cut b costs about
+ * cost[b] - cost[a] (the last one total - cost[last]).  Writes the ncut
+ * (1..7, at most n) grid values whose largest segment cost is smallest,
+ * ascending, to cuts[0..ncut); *longest (may be NULL) receives that cost. */
+int dc_plan_row_cuts(const int32_t* grid, const float* cost, int32_t n, float total, int32_t ncut, int32_t* cuts,
+                     float* longest);
 
 /* Engine kernel launches since the library was loaded. */
 int dc_launch_count(unsigned long long* n);
