@@ -848,6 +848,29 @@ def main():
                             "achieved_gbs": v["bytes"] / (v["ms"] / 1000.0) / 1e9 if v["ms"] else None}
                         for k, v in kernels.items()}}
 
+    # ---- the same step with all rows in one persistent launch (no row cuts)
+    single = None
+    if any(tuning["rows_split_permille"]):
+        g.set_tuning(tuning["peel_blocks_per_sm"], tuning["rows_blocks_per_sm"], tuning["peel_chunk"], [])
+        for _ in range(2):
+            g.release_rows()
+            step()
+        st = []
+        for _ in range(3):
+            g.release_rows()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            st.append((e0.elapsed_time(e1), g.decomp_info()["rows_ms"]))
+        g.set_tuning(tuning["peel_blocks_per_sm"], tuning["rows_blocks_per_sm"], tuning["peel_chunk"],
+                     tuning["rows_split_permille"])
+        sm = float(np.mean([t for t, _ in st]))
+        single = {"ms_per_step": sm, "value": E / (sm / 1000.0), "rows_ms": float(np.mean([r for _, r in st])),
+                  "steps": 3, "note": "same step and launch shapes, rows 1..kmax in one persistent k_trans2 launch"}
+
     # ---- end to end through the C ABI with host buffers
     e2e = None
     if args.e2e_steps > 0:
@@ -898,7 +921,8 @@ def main():
                            "tuning": dict(tuning, source=tune_src)},
                 "phases_ms": {"peel": peel_ms, "rows": rows_ms,
                               "other": ms_per_step - peel_ms - rows_ms},
-                "gpu_launches": int(launches), "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
+                "gpu_launches": int(launches), "roofline": roof, "single_launch_rows": single, "e2e": e2e,
+                "cpu_baseline": cpu,
                 "reference_gpu": ref, "clocks": clocks}
         print(json.dumps(line), flush=True)
     g.free()
