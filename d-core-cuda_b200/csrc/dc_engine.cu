@@ -492,9 +492,9 @@ struct Trans2Params {
     const int32_t* kmax;
     int32_t K;
     int32_t K0;     // first row to compute; cur holds row 0 (K0 > 1 jumps straight to row K0)
-    // K0 > 1 only: cur already holds -1 for the vertices outside C_K0 and the
-    // counters ignore them, so the first row has no leaving set and seeds
-    // every member whose out-count is below its value as well
+    // cur already holds -1 for the vertices outside C_K0 and the counters
+    // ignore them, so the first row has no leaving set and seeds every
+    // member whose out-count is below its value as well
     int preleft;
     int32_t Kstop;  // last row to compute (rows above stay untouched)
     int sorted;     // lists ordered by neighbour kmax, descending
@@ -2094,16 +2094,13 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     int sorted = 0;
     if (allow_sort || g.sorted_kmax)
         if (int rc = sort_lists_by_kmax(h, K, &sorted)) return rc;
-    // starting values and counters of a run that starts at row a: row 0,
-    // or (a > 1) row 0 inside C_a with the vertices outside already left
+    // starting values and counters of a run that starts at row a: row 0
+    // inside C_a with the vertices outside already left (for a = 1 those of
+    // kmax 0), so the run's first step has no leaving pass
     auto start_state = [&](cudaStream_t st, int32_t a, int32_t* cur, int32_t* co, int32_t* ci, uint32_t* mark,
                            int32_t* stamp) -> int {
-        if (a > 1) {
-            ++g_launches;
-            k_preleft_cur<<<grid_for(h, V), kThreads, 0, st>>>(V, d.kmax_v, s->row0, a, cur);
-        } else {
-            DC_CUDA(cudaMemcpyAsync(cur, s->row0, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, st));
-        }
+        ++g_launches;
+        k_preleft_cur<<<grid_for(h, V), kThreads, 0, st>>>(V, d.kmax_v, s->row0, a, cur);
         ++g_launches;
         k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, st>>>(
             V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, cur, co, ci);
@@ -2120,7 +2117,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     tp[0].kmax = d.kmax_v;
     tp[0].K = K;
     tp[0].K0 = k0;
-    tp[0].preleft = k0 > 1;
+    tp[0].preleft = 1;
     tp[0].Kstop = cut[0];
     tp[0].sorted = sorted;
     tp[0].order = s->order;
