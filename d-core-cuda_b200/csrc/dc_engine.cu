@@ -492,9 +492,10 @@ struct Trans2Params {
     const int32_t* kmax;
     int32_t K;
     int32_t K0;     // first row to compute; cur holds row 0 (K0 > 1 jumps straight to row K0)
-    // cur already holds -1 for the vertices outside C_K0 and the counters
-    // ignore them, so the first row has no leaving set and seeds every
-    // member whose out-count is below its value as well
+    // preleft: cur already holds -1 for the vertices outside C_K0 and the
+    // counters ignore them, so the first row has no leaving set and seeds
+    // every member whose out-count is below its value as well (the host
+    // always starts runs this way; 0 = the leaving pass removes them)
     int preleft;
     int32_t Kstop;  // last row to compute (rows above stay untouched)
     int sorted;     // lists ordered by neighbour kmax, descending
@@ -534,7 +535,7 @@ struct TransHook {
     }
 };
 
-// Starting values of a run of rows that jumps to row a: row 0 inside C_a,
+// Starting values of a run of rows that starts at row a: row 0 inside C_a,
 // -1 (left) outside.
 __global__ void k_preleft_cur(uint32_t V, const int32_t* kmax, const int32_t* row0, int32_t a, int32_t* cur) {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
@@ -1175,7 +1176,6 @@ __global__ void k_corner_bound(uint32_t V, const int32_t* kmax, const int32_t* r
     if ((threadIdx.x & 31u) == 0) atomicAdd(acc, s);
 }
 
-// corners rows 1..s can hold per vertex: min(kmax, s, row0)
 // Row ranges of the segments of a split run of rows.
 struct SegBounds {
     int32_t lo[kMaxRowSegments], hi[kMaxRowSegments];
