@@ -32,7 +32,8 @@ def row_shards(weights, world):
     """Contiguous ranges [(first, last)] of rows 1..K over `world` ranks, K =
     len(weights) - 1, minimising the largest range cost, where a range costs
     the sum of its rows' weights plus one more weight of its first row for
-    the jump to it (none for the range starting at row 1).  Ranges are
+    starting there (the counters of C_first are built over its members'
+    lists; none for the range starting at row 1).  Ranges are
     inclusive and in ascending order; an empty range has first > last."""
     w = np.asarray(weights, np.float64)
     K = len(w) - 1
