@@ -664,7 +664,7 @@ extern "C" int dc_autotune(dc_graph* h, dc_tuning* best, float* best_ms) {
     float cost[kGrid];
     int ng = 0;
     dc_set_tuning(h, &pick);  // C measured at the chosen row grid
-    for (int g = 0; g < kGrid; ++g) {
+    for (int g = 0; g < kGrid && K >= kMinSplitRows; ++g) {  // shorter runs are never split
         const int32_t c = 50 * (g + 1);
         const int32_t srow = (int32_t)((int64_t)K * c / 1000);
         if (srow < 1 || srow >= K || (ng && srow == (int32_t)((int64_t)K * grid[ng - 1] / 1000))) continue;

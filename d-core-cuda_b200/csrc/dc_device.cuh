@@ -22,6 +22,7 @@ constexpr unsigned DC_DEV_ERR_NOTFOUND = 16u; // delete of an absent edge
 constexpr uint32_t kEmptySlot = 0xFFFFFFFFu;
 constexpr unsigned long long kWaitNs = 4000000000ull;  // 4 s per wait
 constexpr int kMaxRowSegments = 8;  // concurrent launches a full run of rows may split into
+constexpr int kMinSplitRows = 32;   // runs of fewer rows are never split
 
 // A counter on a 128-byte line of its own.
 struct alignas(128) PadU {

@@ -2033,7 +2033,6 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     // starting there from row 0) on seg[i-1]'s stream, each with its own
     // state and its own range of the corner log; runs of fewer than
     // kMinSplitRows rows stay whole
-    constexpr int32_t kMinSplitRows = 32;
     const int32_t k0 = std::max(1, K0);
     int32_t cut[kMaxRowSegments];
     int nseg = 1;

@@ -15,6 +15,7 @@ def test_empty_graph_ranges_and_tuning(dc, gpu):
         assert np.array_equal(g.rows(0, 1), np.zeros((1, 5), np.int32))
         best, ms = g.autotune()
         assert g.tuning() == best
+        assert not any(best["rows_split_permille"])  # kmax 0: nothing to split
         assert g.decompose() == (0, 0)
 
 
@@ -26,7 +27,8 @@ def test_tiny_cycle(dc, orc, gpu):
     with dc.Graph.from_edges(3, s, d) as g:
         assert g.decompose_rows(1, 1) == (okm, olm)
         assert np.array_equal(g.rows(1, 1), orows[1:2])
-        g.autotune()
+        best, _ = g.autotune()
+        assert not any(best["rows_split_permille"])  # runs under 32 rows are never split
         assert g.decompose() == (okm, olm)
         assert np.array_equal(g.rows(), orows)
 
