@@ -139,6 +139,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def parse_tuning(text):
+    """--tuning "peel_bps,rows_bps,chunk[,cut1,...]" -> set_tuning arguments
+    (cuts in per mille of kmax, at most seven)."""
+    f = [int(x) for x in text.split(",") if x.strip()]
+    if len(f) < 3 or len(f) > 10:
+        raise ValueError("--tuning wants peel_bps,rows_bps,chunk and up to seven cuts")
+    return f[0], f[1], f[2], f[3:]
+
+
 def kernel_traffic(kernel, workload):
     """DRAM bytes per launch from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
@@ -300,8 +309,7 @@ def run_maintenance(args, w, rank, world, local):
     g = dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16)
     g.set_row_repair(args.row_repair)
     if args.tuning:
-        f = [int(x) for x in args.tuning.split(",")]
-        g.set_tuning(f[0], f[1], f[2], f[3:])
+        g.set_tuning(*parse_tuning(args.tuning))
         tune_src = "given (--tuning)"
     elif args.autotune:
         g.autotune()  # launch shapes and row cuts of the recomputations, chosen on the initial graph
@@ -766,8 +774,7 @@ def main():
     g = dc.Graph.from_edges(V, s, d, device=local)
     stream = torch.cuda.ExternalStream(g.stream())
     if args.tuning:
-        f = [int(x) for x in args.tuning.split(",")]
-        g.set_tuning(f[0], f[1], f[2], f[3:])
+        g.set_tuning(*parse_tuning(args.tuning))
         tuning, tune_ms, tune_src = g.tuning(), None, "given (--tuning)"
     elif args.autotune:
         tuning, tune_ms = g.autotune()

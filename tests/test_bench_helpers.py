@@ -55,3 +55,12 @@ def test_serve_plan_is_seeded():
     for t_arr, gid, size, rate in phases:
         assert (np.diff(t_arr) > 0).all() and size.min() >= 1 and size.max() <= 10_000
         assert gid.max() < 64
+
+
+def test_parse_tuning():
+    import pytest
+    assert bench.parse_tuning("3,3,64") == (3, 3, 64, [])
+    assert bench.parse_tuning("3,3,64,150,250,450") == (3, 3, 64, [150, 250, 450])
+    for bad in ("3,3", "1,2,3,4,5,6,7,8,9,10,11", "a,b,c"):
+        with pytest.raises(ValueError):
+            bench.parse_tuning(bad)
