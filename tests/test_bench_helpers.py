@@ -1,6 +1,6 @@
 """Host-side helpers of the benchmark: the per-row peel byte model against a
-direct count on a small graph, the final edge set of an update stream, and
-the seeded serving plan."""
+direct count on a small graph, the final edge set of an update stream, the
+seeded serving plan and the --tuning parser."""
 import os
 import sys
 
