@@ -5,8 +5,9 @@ Two ways the path shards (no data-path collective in either):
 * rows: every rank holds the whole graph and computes kmax and row 0 itself,
   then a contiguous range of rows 1..kmax chosen from work weights that every
   rank derives identically (dc_row_weights: total degree of C_k); each range
-  starts with a jump from row 0 (dc_decompose_rows), so ranges are
-  independent.  Rows stay in the HBM of the rank that computed them.
+  starts from row 0 restricted to the core of its first row
+  (dc_decompose_rows), so ranges are independent.  Rows stay in the HBM of
+  the rank that computed them.
 * graphs: independent graphs (replicas of the benchmark, serving) are placed
   on ranks by size, largest first onto the least loaded rank.
 
@@ -21,7 +22,7 @@ def _pack(w, K, cap):
     for k in range(2, K + 1):
         if acc + w[k] > cap:
             shards.append((first, k - 1))
-            first, acc = k, 2.0 * w[k]  # its first row plus the jump to it
+            first, acc = k, 2.0 * w[k]  # its first row plus building its counters
         else:
             acc += w[k]
     shards.append((first, K))
