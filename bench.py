@@ -175,125 +175,191 @@ def reference_gpu(V, s, d, g):
             "timing": "host clock around dcore(), as main.cu:249-254 reports it"}
 
 
-def decomposition_bytes(V, s, d, kmaxes):
-    """Algorithmic bytes of a full decomposition as a per-row peel moves them
-    (the reference's dcore(), main.cu:197-262): the kmax pass B_K = 12 E + 16 V
-    (out-adjacency ids, in-degree read-modify-write, offsets, degree init,
-    result and state) and per row k B_k = 8 D_k + 16 I_k + 24 V_k + 4 (V - V_k)
-    with V_k = |{v : kmax(v) >= k}|, D_k = total degree of those vertices,
-    I_k = edges with both endpoints among them (ids + neighbour-kmax filter,
-    two 4+4 B degree updates per internal edge, per-core-vertex offsets,
-    degrees, state and result, zero rows for the rest)."""
-    K = int(kmaxes.max()) if len(kmaxes) else 0
-    deg = np.bincount(s, minlength=V) + np.bincount(d, minlength=V)
-    rev = lambda a: np.cumsum(a[::-1])[::-1]
-    Vk = rev(np.bincount(kmaxes, minlength=K + 1).astype(np.float64))
-    Dk = rev(np.bincount(kmaxes, weights=deg, minlength=K + 1))
-    Ik = rev(np.bincount(np.minimum(kmaxes[s], kmaxes[d]), minlength=K + 1).astype(np.float64))
-    return {"B_K": 12.0 * len(s) + 16.0 * V, "B_row": 8 * Dk + 16 * Ik + 24 * Vk + 4 * (V - Vk)}
-
-
-def cpu_baseline(w, V, s, d, budget_s=20.0):
-    """Oracle port on the host cores: kmax pass plus a stratified sample of
-    rows, extrapolated to the full decomposition."""
+def make_graph_oracle(w, rank):
+    """The same seeded graph as make_graph, built by the oracle's restatement
+    of the generators (the reference arm never loads the engine library)."""
     from oracle import oracle
-    threads = oracle.max_threads()
-    t0 = time.perf_counter()
-    K, kmaxes = oracle.kmax(V, s, d)
-    t_kmax = time.perf_counter() - t0
-    # probe one row to size the sample
-    t0 = time.perf_counter()
-    oracle.row(V, s, d, kmaxes, 0)
-    t_row0 = time.perf_counter() - t0
-    rows_total = K + 1
-    want = max(min(rows_total, 2 * threads), int(budget_s * threads / max(t_row0, 1e-3)))
-    want = max(1, min(rows_total, want))
-    stride = max(1, rows_total // want)
-    n, row_secs = oracle.rows_sample(V, s, d, kmaxes, K, stride, threads)
-    # all rows run in parallel over `threads` threads: estimated wall time is
-    # the kmax pass plus the extrapolated row-seconds spread over the threads
-    t_est = t_kmax + row_secs * rows_total / n / threads
-    return {"value": len(s) / t_est, "unit": "edges/s", "cores": threads, "kind": "port",
-            "sample": f"kmax pass + {n} of {rows_total} rows (every {stride}th row), bucket-queue peel per row "
-                      f"on {threads} threads; all-row time extrapolated from summed row seconds "
-                      f"({t_est:.1f} s estimated)"}
+    seed = w["seed"] + rank
+    if w["gen"] == "rmat":
+        return oracle.gen_rmat(w["scale"], w["ef"], seed)
+    s, d = oracle.gen_er(w["n"], w["m"], seed)
+    return w["n"], s, d
+
+
+def decomp_config(args, w, V, E, kmax, lmax, world):
+    """The config of a decomposition line; both arms print exactly this."""
+    return {"workload": args.workload, "graph": w["desc"], "V": int(V), "E": int(E), "kmax": int(kmax),
+            "lmax": int(lmax), "output": "kmax per vertex and dense rows lmax[k][v], k = 0..kmax",
+            "l2": "inputs larger than L2 (graph %.0f MB, rows %.0f MB)" % (8.0 * E / 2**20,
+                                                                         4.0 * (kmax + 1) * V / 2**20),
+            "parallelism": f"replicas x{world}"}
+
+
+def peel_bytes(V, s, d, kmaxes):
+    """Algorithmic bytes of the fused peel (kmax and row 0), as a per-row peel
+    moves them (the reference's passes, main.cu:27-195): the kmax pass
+    B_K = 12 E + 16 V (out-adjacency ids, in-degree read-modify-write;
+    offsets, degree init, result and state per vertex) and row 0
+    B_0 = 8 D_0 + 16 I_0 + 24 V (D_0 = all list entries, I_0 = E)."""
+    E = float(len(s))
+    return (12.0 * E + 16.0 * V) + (8.0 * 2 * E + 16.0 * E + 24.0 * V)
+
+
+def refinement_bytes(V, s, d, kmaxes, rows):
+    """Algorithmic bytes of rows 1..kmax derived row to row, from the oracle's
+    result: every value that changes from row k-1 to row k is evaluated once,
+    reading its lists' prefixes inside C_k = {kmax >= k} (4 B id + 4 B
+    neighbour value per entry), its old value and its new value (4 + 4 B),
+    and recording the change (v, k, l: 12 B); every vertex leaving C_k is
+    marked (4 B).  Unchanged values cost nothing: this is the floor of a
+    refinement that evaluates each change exactly once.  Returns (bytes,
+    changes, entries)."""
+    K = rows.shape[0] - 1
+    cv, ck = [], []
+    for k0 in range(1, K + 1, 16):
+        k1 = min(K + 1, k0 + 16)
+        ks = np.arange(k0, k1)
+        m = (rows[k0:k1] != rows[k0 - 1:k1 - 1]) & (kmaxes[None, :] >= ks[:, None])
+        kk, vv = np.nonzero(m)
+        cv.append(vv.astype(np.int64))
+        ck.append(ks[kk].astype(np.int64))
+    cv = np.concatenate(cv) if cv else np.zeros(0, np.int64)
+    ck = np.concatenate(ck) if ck else np.zeros(0, np.int64)
+    W = K + 2
+    entries = 0
+    for a, b in ((s, d), (d, s)):  # out-lists, then in-lists
+        keys = np.sort(a.astype(np.int64) * W + (K + 1 - kmaxes[b].astype(np.int64)))
+        hi = np.searchsorted(keys, cv * W + (K + 1 - ck), side="right")
+        lo = np.searchsorted(keys, cv * W, side="left")
+        entries += int((hi - lo).sum())
+        del keys
+    leaving = int(V - np.count_nonzero(kmaxes == K))
+    return 8.0 * entries + 20.0 * len(cv) + 4.0 * leaving, int(len(cv)), entries
+
+
+def oracle_decomposition(V, s, d, rows=None):
+    """The oracle's full decomposition on all host threads, timed from its
+    built CSR/CSC to the last row (no sampling, no extrapolation)."""
+    from oracle import oracle
+    K, L, kmaxes, out, secs, nt = oracle.dcore_timed(V, s, d, 0, rows)
+    return {"kmax": K, "lmax": L, "kmaxes": kmaxes, "rows": out, "seconds": secs, "threads": nt}
+
+
+def host_cpu():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline_from(res, E, what):
+    return {"value": E / res["seconds"], "unit": "edges/s", "cores": res["threads"], "kind": "port",
+            "sample": f"{what}: one full decomposition (kmax pass + all {res['kmax'] + 1} rows, bucket-queue "
+                      f"peel per row, rows in parallel) on {res['threads']} threads of {host_cpu()}, "
+                      f"{res['seconds']:.2f} s, timed from the built CSR/CSC; no sampling"}
+
+
+def check_parity(g, res, chunk=32):
+    """The engine's decomposition against the oracle's: kmax, lmax, every
+    kmax value and every dense row (checkDCore's criterion, main.cu:276-293).
+    Raises on any difference."""
+    info = g.decomp_info()
+    K = res["kmax"]
+    if (info["kmax"], info["lmax"]) != (K, res["lmax"]):
+        raise RuntimeError(f"parity: kmax/lmax {info['kmax']}/{info['lmax']} != oracle {K}/{res['lmax']}")
+    if not np.array_equal(g.kmaxes(), res["kmaxes"]):
+        raise RuntimeError("parity: kmax values differ from the oracle")
+    for k0 in range(0, K + 1, chunk):
+        n = min(chunk, K + 1 - k0)
+        if not np.array_equal(g.rows(k0, n), res["rows"][k0:k0 + n]):
+            raise RuntimeError(f"parity: rows {k0}..{k0 + n - 1} differ from the oracle")
+    return {"vs": "oracle (CPU restatement, oracle/dcore_oracle.c)", "exact": True, "kmax": K,
+            "rows_checked": K + 1, "values_checked": int((K + 1) * len(res["kmaxes"]) + len(res["kmaxes"]))}
 
 
 def run_reference(args, w, rank, world):
+    """The reference arm: the oracle's CPU restatement of the reference's
+    decomposition (the reference has no CPU implementation of the path) on
+    all host threads, one full decomposition per step.  Rank 0 only; nothing
+    of the engine is loaded."""
     if rank != 0:
         return
-    import dcore_b200 as dc
-    if w.get("serve") or w.get("sched"):
-        run_reference_recompute(args, w, dc)
+    if w.get("serve") or w.get("sched") or w.get("maint"):
+        run_reference_recompute(args, w)
         return
-    V, s, d = make_graph(dc, w, 0)
-    vals = []
-    base = None
+    V, s, d = make_graph_oracle(w, 0)
+    E = int(len(s))
+    rows = None
+    secs, res = [], None
     for i in range(args.warmup + args.steps):
-        b = cpu_baseline(w, V, s, d, budget_s=args.cpu_seconds)
+        res = oracle_decomposition(V, s, d, rows)
+        rows = res["rows"].base if res["rows"].base is not None else res["rows"]
         if i >= args.warmup:
-            vals.append(b["value"])
-            base = b
-    value = float(np.mean(vals))
-    metric, unit = METRIC, "edges/s"
-    if w.get("maint"):
-        # the CPU path maintains by recomputing (the reference's own check,
-        # checkDCore): one batch of 10,000 updates costs one decomposition
-        metric, unit = METRIC_MAINT, "updates/s"
-        value = 10_000 * value / len(s)
-        base = dict(base, unit=unit, sample=base["sample"] + "; one recomputation per batch of 10,000 updates")
-    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * len(s) / value, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": args.workload, "graph": w["desc"], "V": V, "E": int(len(s))},
-            "cpu_baseline": dict(base, value=value),
-            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            secs.append(res["seconds"])
+    ms = 1000.0 * float(np.mean(secs))
+    value = E / (ms / 1000.0)
+    line = {"metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic", "impl": "reference",
+            "config": decomp_config(args, w, V, E, res["kmax"], res["lmax"], world),
+            "cpu_baseline": dict(cpu_baseline_from(res, E, "each step"), value=value),
+            "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "step_seconds": secs}
     print(json.dumps(line), flush=True)
 
 
-def run_reference_recompute(args, w, dc):
-    """CPU path for the serving and scheduler workloads: the reference keeps a
-    decomposition current by recomputing it (checkDCore, main.cu:264-293), so
-    every batch costs one decomposition of its graph on the host cores."""
-    rng = np.random.default_rng(w["seed"] + 31)
-    vals, base = [], None
+def run_reference_recompute(args, w):
+    """CPU path for the maintenance, scheduler and serving workloads: the
+    reference keeps a decomposition current by recomputing it (checkDCore,
+    main.cu:264-293), so every batch costs one full decomposition of its
+    graph on the host cores.  Each step times one full oracle decomposition
+    of the workload's graph (for serving: the graph of median size)."""
+    from oracle import oracle
     if w.get("serve"):
         scales, efs, phases = serve_plan(w, 0, args.requests, args.rate)
-        t_arr, gid, size, _ = phases[1]
+        _, gid, size, _ = phases[1]
         nominal = (2.0 ** scales) * efs
         mid = int(np.argsort(nominal)[len(nominal) // 2])
-        V, s, d = dc.gen_rmat(int(scales[mid]), int(efs[mid]), w["seed"] * 1000 + mid)
-        dedup = len(s) / nominal[mid]
-        for i in range(args.warmup + args.steps):
-            b = cpu_baseline(w, V, s, d, budget_s=args.cpu_seconds)
-            if i >= args.warmup:
-                vals.append(b["value"])
-                base = b
-        rate = float(np.mean(vals))
+        V, s, d = oracle.gen_rmat(int(scales[mid]), int(efs[mid]), w["seed"] * 1000 + mid)
+        what = f"graph {mid} of the mix (scale {scales[mid]}, edge factor {efs[mid]})"
+    else:
+        V, s, d = oracle.gen_rmat(w["scale"], w["ef"], w["seed"])
+        what = w["desc"].split(";")[0]
+    E = int(len(s))
+    rows, secs, res = None, [], None
+    for i in range(args.warmup + args.steps):
+        res = oracle_decomposition(V, s, d, rows)
+        rows = res["rows"].base if res["rows"].base is not None else res["rows"]
+        if i >= args.warmup:
+            secs.append(res["seconds"])
+    rate = E / float(np.mean(secs))  # edges/s of one recomputation
+    if w.get("serve"):
+        dedup = E / nominal[mid]
         seconds = float(np.sum(nominal[gid] * dedup / rate))  # one recomputation per request
         value = float(size.sum()) / seconds
         metric = METRIC_SERVE
-        sample = (base["sample"] + f"; measured on graph {mid} (scale {scales[mid]}, edge factor {efs[mid]}), "
-                  f"every request costs one recomputation of its graph at that edges/s")
-        config = {"workload": args.workload, "graphs": w["desc"], "requests": int(len(t_arr))}
-    else:
-        V, s, d = dc.gen_rmat(w["scale"], w["ef"], w["seed"])
-        for i in range(args.warmup + args.steps):
-            b = cpu_baseline(w, V, s, d, budget_s=args.cpu_seconds)
-            if i >= args.warmup:
-                vals.append(b["value"])
-                base = b
-        rate = float(np.mean(vals))
+        note = "every request costs one recomputation of its graph at the measured edges/s"
+        config = {"workload": args.workload, "graphs": w["desc"], "requests": int(len(gid))}
+    elif w.get("sched"):
         ev_sizes = _log_uniform(np.random.default_rng(w["seed"] + 77), w["eval_batches"], w["eval_max"])
-        value = float(ev_sizes.mean()) * rate / len(s)
+        value = float(ev_sizes.mean()) * rate / E
         metric = METRIC_MAINT
-        sample = base["sample"] + "; every batch costs one recomputation of the graph"
-        config = {"workload": args.workload, "graph": w["desc"], "V": V, "E": int(len(s))}
+        note = "every batch costs one recomputation of the graph"
+        config = {"workload": args.workload, "graph": w["desc"], "V": V, "E": E}
+    else:
+        value = 10_000 * rate / E
+        metric = METRIC_MAINT
+        note = "one recomputation per batch of 10,000 updates"
+        config = {"workload": args.workload, "graph": w["desc"], "V": V, "E": E}
+    base = cpu_baseline_from(res, E, what)
     line = {"metric": metric, "value": value, "unit": "updates/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32", "data": "synthetic", "impl": "reference", "config": config,
-            "cpu_baseline": dict(base, value=value, unit="updates/s", sample=sample),
+            "warmup": args.warmup, "ms_per_step": 1000.0 * float(np.mean(secs)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic", "impl": "reference",
+            "config": config, "cpu_baseline": dict(base, value=value, unit="updates/s",
+                                                   sample=base["sample"] + "; " + note),
             "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -711,6 +777,195 @@ def run_sched(args, w, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_decomposition(args, w, rank, world, local, dist):
+    """Full decompositions of a freshly loaded graph.  The graph's edge list
+    stays resident in HBM; before each step (untimed) a new handle builds the
+    CSR/CSC from it, so every timed step is a first decomposition of that
+    graph: the fused peel, the neighbour-kmax reordering of the lists, rows
+    1..kmax, the skyline and the dense rows written to HBM.  Afterwards the
+    result is checked against the oracle's full decomposition, whose timing
+    is the CPU baseline."""
+    import torch
+    import dcore_b200 as dc
+    V, s, d = make_graph(dc, w, rank)
+    E = int(len(s))
+    dev = torch.device("cuda", local)
+    d_src = torch.from_numpy(s.view(np.int32)).to(dev)
+    d_dst = torch.from_numpy(d.view(np.int32)).to(dev)
+    g0 = dc.Graph.from_edges(V, s, d, device=local)
+    if args.tuning:
+        g0.set_tuning(*parse_tuning(args.tuning))
+        tuning, tune_src = g0.tuning(), "given (--tuning)"
+    elif args.autotune:
+        tuning, _ = g0.autotune()
+        tune_src = "autotuner (dc_autotune) on the graph, before the timed steps"
+    else:
+        tuning, tune_src = g0.tuning(), "defaults"
+    g0.free()
+
+    def fresh(cuts=True):
+        h = dc.Graph.from_device_edges(V, E, d_src.data_ptr(), d_dst.data_ptr(), device=local)
+        h.set_tuning(tuning["peel_blocks_per_sm"], tuning["rows_blocks_per_sm"], tuning["peel_chunk"],
+                     tuning["rows_split_permille"] if cuts else [])
+        h.synchronize()
+        return h
+
+    def timed_step(h):
+        """(ms, engine launches) of one decomposition + dense rows on h."""
+        st = torch.cuda.ExternalStream(h.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        n0 = dc.launch_count()
+        e0.record(st)
+        h.decompose(dc.METHOD_INCREMENTAL)
+        h.materialize_rows()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1), dc.launch_count() - n0
+
+    for _ in range(args.warmup):
+        h = fresh()
+        timed_step(h)
+        h.free()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    times, infos, launches = [], [], 0
+    g = None
+    for i in range(args.steps):
+        if g is not None:
+            g.free()
+        g = fresh()
+        ms, n = timed_step(g)
+        times.append(ms)
+        launches += n
+        infos.append(g.decomp_info())
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    t = torch.tensor([float(np.sum(times))], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_per_step = float(t.item()) / args.steps
+    value = world * E / (ms_per_step / 1000.0)
+    inf = infos[-1]
+    K = inf["kmax"]
+
+    # ---- the same step with rows 1..kmax in one persistent launch (no cuts)
+    single = None
+    if any(tuning["rows_split_permille"]):
+        st_ms = []
+        for i in range(4):
+            h = fresh(cuts=False)
+            ms, _ = timed_step(h)
+            if i:
+                st_ms.append((ms, h.decomp_info()["rows_ms"]))
+            h.free()
+        sm = float(np.mean([x for x, _ in st_ms]))
+        single = {"ms_per_step": sm, "value": E / (sm / 1000.0), "rows_ms": float(np.mean([r for _, r in st_ms])),
+                  "steps": len(st_ms), "note": "same step and launch shapes, rows 1..kmax in one persistent "
+                                               "k_trans2 launch"}
+
+    # ---- end to end through the C ABI with host buffers
+    e2e, hrows = None, None
+    if args.e2e_steps > 0:
+        hs = dc.pinned_array(E, np.uint32)
+        hd = dc.pinned_array(E, np.uint32)
+        hs[:] = s
+        hd[:] = d
+        hk = dc.pinned_array(V, np.int32)
+        hrows = dc.pinned_array((K + 1) * V, np.int32).reshape(K + 1, V)
+        et = []
+        for i in range(args.e2e_steps + 1):
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            g2 = dc.Graph.from_edges(V, hs, hd, device=local)
+            g2.set_tuning(tuning["peel_blocks_per_sm"], tuning["rows_blocks_per_sm"], tuning["peel_chunk"],
+                          tuning["rows_split_permille"])
+            k2, _ = g2.decompose(dc.METHOD_INCREMENTAL)
+            g2.kmaxes(out=hk)
+            g2.rows(0, k2 + 1, out=hrows[:k2 + 1])
+            g2.free()
+            torch.cuda.synchronize()
+            if i > 0:  # first call is a warm-up
+                et.append(time.perf_counter() - t0)
+        te = torch.tensor([float(np.mean(et))], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * E / float(te.item()), "unit": "edges/s", "h2d_bytes_per_step": 8 * E,
+               "d2h_bytes_per_step": 4 * V * (K + 2), "timing": "wall clock, synchronized, mean of steps",
+               "steps": len(et)}
+
+    # ---- oracle: full decomposition on the host cores (CPU baseline) and
+    # the parity check of the last timed step and of the e2e output
+    parity, cpu, res = None, None, None
+    if rank == 0 and not args.no_oracle:
+        res = oracle_decomposition(V, s, d)
+        cpu = cpu_baseline_from(res, E, "oracle run beside the engine")
+        parity = check_parity(g, res)
+        if e2e is not None:
+            if not (np.array_equal(hk, res["kmaxes"]) and np.array_equal(hrows, res["rows"])):
+                raise RuntimeError("parity: the e2e output differs from the oracle")
+            parity["e2e_output_checked"] = True
+
+    # ---- roofline of the dominant kernel (CUDA events on the engine stream)
+    peak, peak_kind = peaks()
+    peel_ms = float(np.mean([i["kmax_ms"] for i in infos]))
+    rows_ms = float(np.mean([i["rows_ms"] for i in infos]))
+    kernels = {"k_peel2": {"ms": peel_ms, "bytes": peel_bytes(V, s, d, None),
+                           "model": "per-row peel bytes of kmax + row 0: (12 E + 16 V) + (8 D_0 + 16 I_0 + 24 V)"},
+               "k_trans2": {"ms": rows_ms, "bytes": None,
+                            "model": "one evaluation per changed value: 8 B per C_k list entry of each change, "
+                                     "20 B per change, 4 B per vertex leaving C_k"}}
+    roof = None
+    if res is not None:
+        b_ref, n_changes, n_entries = refinement_bytes(V, s, d, res["kmaxes"], res["rows"])
+        kernels["k_trans2"].update(bytes=b_ref, changes=n_changes, entries=n_entries)
+        for k in kernels.values():
+            k["achieved_gbs"] = k["bytes"] / (k["ms"] / 1000.0) / 1e9 if k["ms"] else None
+            k["frac"] = k["achieved_gbs"] / peak if k["achieved_gbs"] else None
+        dom = max(kernels, key=lambda k: kernels[k]["ms"])
+        sort_b = 12.0 * 2 * E
+        expand_b = 4.0 * (K + 1) * V
+        b_alg = kernels["k_peel2"]["bytes"] + b_ref + sort_b + expand_b
+        roof = {"kernel": dom, "bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": peak,
+                "unit": "GB/s", "frac": kernels[dom]["frac"], "peak_source": peak_kind,
+                "traffic": kernel_traffic(dom, args.workload),
+                "timing": "CUDA events on the graph's stream around each phase inside dc_decompose; the rows "
+                          "phase spans all k_trans2 launches (row segments on concurrent streams joined back)",
+                "kernels": kernels,
+                "decomposition": {"alg_bytes": b_alg, "ms": ms_per_step,
+                                  "achieved_gbs": b_alg / (ms_per_step / 1000.0) / 1e9,
+                                  "frac": b_alg / (ms_per_step / 1000.0) / 1e9 / peak,
+                                  "model": "k_peel2 + k_trans2 models + list reordering 12 B per list entry + "
+                                           "dense rows 4 (kmax+1) V"},
+                "engine_counted": {"k_trans2_entries": inf.get("entries", 0), "evals": inf["evals"],
+                                   "drops": inf["drops"]}}
+    ref = reference_gpu(V, s, d, g) if rank == 0 else None
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                "config": decomp_config(args, w, V, E, K, inf["lmax"], world),
+                "engine": {"method": "fused peel (kmax + row 0), rows 1..kmax derived row to row",
+                           "tuning": dict(tuning, source=tune_src),
+                           "step": "first decomposition of a freshly built handle (CSR/CSC built untimed from "
+                                   "the HBM-resident edge list)"},
+                "phases_ms": {"peel": peel_ms, "rows": rows_ms, "other": ms_per_step - peel_ms - rows_ms},
+                "step_ms": times, "gpu_launches": int(launches), "roofline": roof, "parity": parity,
+                "single_launch_rows": single, "e2e": e2e, "cpu_baseline": cpu, "reference_gpu": ref,
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    g.free()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -719,8 +974,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="decomp-rmat22")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-oracle", action="store_true",
+                    help="decomposition: skip the oracle run (CPU baseline, parity check, roofline model)")
     ap.add_argument("--maint-method", type=int, default=0, help="0 scheduler, 1 local, 2 re-peel")
     ap.add_argument("--requests", type=int, default=0, help="serve: number of requests (0: workload default)")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: arrivals per second (0: workload default)")
@@ -769,170 +1024,7 @@ def main():
             dist.destroy_process_group()
         return
 
-    V, s, d = make_graph(dc, w, rank)
-    E = int(len(s))
-    g = dc.Graph.from_edges(V, s, d, device=local)
-    stream = torch.cuda.ExternalStream(g.stream())
-    if args.tuning:
-        g.set_tuning(*parse_tuning(args.tuning))
-        tuning, tune_ms, tune_src = g.tuning(), None, "given (--tuning)"
-    elif args.autotune:
-        tuning, tune_ms = g.autotune()
-        tune_src = "autotuner (dc_autotune) before the timed steps"
-    else:
-        tuning, tune_ms, tune_src = g.tuning(), None, "defaults"
-
-    def step():
-        g.decompose(dc.METHOD_INCREMENTAL)
-        g.materialize_rows()  # dense rows (kmax+1) x V in HBM
-
-    for _ in range(args.warmup):
-        g.release_rows()
-        step()
-    infos = []
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
-    launches0 = dc.launch_count()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    times = []
-    for _ in range(args.steps):
-        g.release_rows()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step()
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
-        infos.append(g.decomp_info())
-    launches = dc.launch_count() - launches0
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    if dist:
-        dist.barrier()
-    total_ms = float(np.sum(times))
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    ms_per_step = max_ms / args.steps
-    value = world * E / (ms_per_step / 1000.0)
-    K = infos[-1]["kmax"]
-
-    # ---- roofline of the dominant kernel (CUDA events on the engine stream)
-    peak, peak_kind = peaks()
-    inf = infos[-1]
-    peel_ms = float(np.mean([i["kmax_ms"] for i in infos]))
-    rows_ms = float(np.mean([i["rows_ms"] for i in infos]))
-    model = decomposition_bytes(V, s, d, g.kmaxes())
-    kernels = {
-        # fused kmax + row 0 peel
-        "k_peel2": {"ms": peel_ms, "bytes": model["B_K"] + model["B_row"][0]},
-        # rows 1..kmax
-        "k_trans2": {"ms": rows_ms, "bytes": float(np.sum(model["B_row"][1:]))},
-    }
-    dom = max(kernels, key=lambda k: kernels[k]["ms"])
-    ach = kernels[dom]["bytes"] / (kernels[dom]["ms"] / 1000.0) / 1e9
-    b_alg = model["B_K"] + float(np.sum(model["B_row"]))
-    touched = 8.0 * inf.get("entries", 0) + 16.0 * inf["evals"]
-    nseg = 1 + sum(1 for c in tuning["rows_split_permille"] if c)
-    roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-            "peak_source": peak_kind, "traffic": kernel_traffic(dom, args.workload),
-            "k_trans2_launches_per_step": nseg,
-            "timing": "CUDA events on the graph's stream around each phase; the rows phase spans all of its "
-                      "k_trans2 launches (row segments on concurrent streams joined back to the graph's stream)",
-            "model": "per-row peel bytes: B_K = 12E + 16V; B_k = 8 D_k + 16 I_k + 24 V_k + 4 (V - V_k)",
-            "decomposition": {"alg_bytes": b_alg, "ms": ms_per_step,
-                              "achieved_gbs": b_alg / (ms_per_step / 1000.0) / 1e9,
-                              "frac": b_alg / (ms_per_step / 1000.0) / 1e9 / peak},
-            "engine_touched_bytes": {"k_trans2": touched,
-                                     "gbs": touched / (rows_ms / 1000.0) / 1e9 if rows_ms else None},
-            "kernels": {k: {"ms": v["ms"], "alg_bytes": v["bytes"],
-                            "achieved_gbs": v["bytes"] / (v["ms"] / 1000.0) / 1e9 if v["ms"] else None}
-                        for k, v in kernels.items()}}
-
-    # ---- the same step with all rows in one persistent launch (no row cuts)
-    single = None
-    if any(tuning["rows_split_permille"]):
-        g.set_tuning(tuning["peel_blocks_per_sm"], tuning["rows_blocks_per_sm"], tuning["peel_chunk"], [])
-        for _ in range(2):
-            g.release_rows()
-            step()
-        st = []
-        for _ in range(3):
-            g.release_rows()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            step()
-            e1.record(stream)
-            e1.synchronize()
-            st.append((e0.elapsed_time(e1), g.decomp_info()["rows_ms"]))
-        g.set_tuning(tuning["peel_blocks_per_sm"], tuning["rows_blocks_per_sm"], tuning["peel_chunk"],
-                     tuning["rows_split_permille"])
-        sm = float(np.mean([t for t, _ in st]))
-        single = {"ms_per_step": sm, "value": E / (sm / 1000.0), "rows_ms": float(np.mean([r for _, r in st])),
-                  "steps": 3, "note": "same step and launch shapes, rows 1..kmax in one persistent k_trans2 launch"}
-
-    # ---- end to end through the C ABI with host buffers
-    e2e = None
-    if args.e2e_steps > 0:
-        hs = dc.pinned_array(E, np.uint32)
-        hd = dc.pinned_array(E, np.uint32)
-        hs[:] = s
-        hd[:] = d
-        hk = dc.pinned_array(V, np.int32)
-        hrows = dc.pinned_array((K + 1) * V, np.int32).reshape(K + 1, V)
-        et = []
-        for i in range(args.e2e_steps + 1):
-            if dist:
-                dist.barrier()
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            g2 = dc.Graph.from_edges(V, hs, hd, device=local)
-            g2.set_tuning(tuning["peel_blocks_per_sm"], tuning["rows_blocks_per_sm"], tuning["peel_chunk"],
-                          tuning["rows_split_permille"])
-            k2, _ = g2.decompose(dc.METHOD_INCREMENTAL)
-            g2.kmaxes(out=hk)
-            g2.rows(0, k2 + 1, out=hrows[:k2 + 1])
-            g2.free()
-            torch.cuda.synchronize()
-            if i > 0:  # first call is a warm-up
-                et.append(time.perf_counter() - t0)
-        te = torch.tensor([float(np.mean(et))], dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * E / float(te.item()), "unit": "edges/s", "h2d_bytes_per_step": 8 * E,
-               "d2h_bytes_per_step": 4 * V * (K + 2), "timing": "wall clock, synchronized, mean of steps"}
-        if np.any(hrows[0] != g.rows(0, 1)[0]):
-            raise RuntimeError("e2e rows differ from the device-resident run")
-
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w, V, s, d, budget_s=args.cpu_seconds)
-    ref = reference_gpu(V, s, d, g) if rank == 0 else None
-
-    if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-                "config": {"workload": args.workload, "graph": w["desc"], "V": V, "E": E, "kmax": K,
-                           "lmax": inf["lmax"], "method": "incremental rows", "output": "dense rows in HBM",
-                           "l2": "inputs larger than L2 (graph %.0f MB, rows %.0f MB)" % (
-                               8.0 * E / 2**20, 4.0 * (K + 1) * V / 2**20),
-                           "parallelism": f"replicas x{world}",
-                           "tuning": dict(tuning, source=tune_src)},
-                "phases_ms": {"peel": peel_ms, "rows": rows_ms,
-                              "other": ms_per_step - peel_ms - rows_ms},
-                "gpu_launches": int(launches), "roofline": roof, "single_launch_rows": single, "e2e": e2e,
-                "cpu_baseline": cpu,
-                "reference_gpu": ref, "clocks": clocks}
-        print(json.dumps(line), flush=True)
-    g.free()
+    run_decomposition(args, w, rank, world, local, dist)
     if dist:
         dist.destroy_process_group()
 

@@ -217,6 +217,25 @@ extern "C" int dc_kmax_noalloc(uint32_t V, uint64_t E, const uint32_t* d_in_off,
     p.q.slots = (unsigned long long*)(base + kNaRingOff);
     p.q.mask = (unsigned)(kNaRingSlots - 1);
 
+    // the queue ring is sized for kNaMaxE adjacency entries: the edge count
+    // the arrays really hold (out_off[V], in_off[V]) must be the E given
+    uint32_t ends[2] = {0, 0};
+    e = cudaMemcpyAsync(&ends[0], d_out_off + V, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&ends[1], d_in_off + V, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(DC_ERR_CUDA, "dc_kmax_noalloc: reading the edge counts failed: %s", cudaGetErrorString(e));
+    }
+    if (ends[0] > kNaMaxE || ends[1] > kNaMaxE)
+        return set_error(DC_ERR_CAPACITY,
+                         "dc_kmax_noalloc: the arrays hold %u out- / %u in-edges, beyond the fixed scratch limit of "
+                         "%llu edges",
+                         ends[0], ends[1], (unsigned long long)kNaMaxE);
+    if ((uint64_t)ends[0] != E || (uint64_t)ends[1] != E)
+        return set_error(DC_ERR_INVALID, "dc_kmax_noalloc: E = %llu but out_off[V] = %u and in_off[V] = %u",
+                         (unsigned long long)E, ends[0], ends[1]);
+
     // the shared scratch keeps the previous call's contents: reset the
     // control block and empty the queue ring
     e = cudaMemsetAsync(base, 0, kNaCtlBytes, st);

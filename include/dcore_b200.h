@@ -291,8 +291,10 @@ int dc_kmax_edge_batches(uint32_t V, const int32_t* kmaxes, uint64_t B, const ui
  * or serving loops where cudaMalloc's device-wide synchronisation would stall
  * other work.  The graph comes as plain device arrays: in_off[V+1] (CSC
  * offsets; in-degree of v = in_off[v+1] - in_off[v]), out_off[V+1] and
- * out_nbr[E] (CSR).  kmax[V] is written on the device, the largest value to
- * *kmax_max (may be NULL); the call waits for the GPU before returning.
+ * out_nbr[E] (CSR), with out_off[0] = in_off[0] = 0 and out_off[V] =
+ * in_off[V] = E (checked: DC_ERR_INVALID otherwise).  kmax[V] is written on
+ * the device, the largest value to *kmax_max (may be NULL); the call waits
+ * for the GPU before returning.
  * Limits: V <= 262,144 and E <= 4,194,304 (DC_ERR_CAPACITY beyond).  All
  * intermediate state lives in one fixed device array of about 11 MB that
  * this library reserves on every GPU that loads it, until process exit; all

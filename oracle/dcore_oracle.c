@@ -298,12 +298,31 @@ int32_t or_bz_row(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* d
  * returns OR_ERR_CAPACITY (size query).  Rows run in parallel over `threads`
  * OpenMP threads (<= 0: all), largest rows first.
  */
+int or_dcore_timed(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, int threads,
+                   int32_t* kmaxes_out, int32_t* lmaxes_out, uint64_t rows_cap,
+                   int32_t* kmax_out, int32_t* lmax_out, double* seconds);
+
 int or_dcore(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, int threads,
              int32_t* kmaxes_out, int32_t* lmaxes_out, uint64_t rows_cap,
              int32_t* kmax_out, int32_t* lmax_out) {
+    return or_dcore_timed(V, E, src, dst, threads, kmaxes_out, lmaxes_out, rows_cap, kmax_out, lmax_out, NULL);
+}
+
+/*
+ * or_dcore that also reports, in *seconds (may be NULL), the wall time of the
+ * decomposition itself: from the built CSR/CSC (the reference's dcore() gets
+ * its Graph already in that form, main.cu:197) to the last row.
+ */
+int or_dcore_timed(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, int threads,
+                   int32_t* kmaxes_out, int32_t* lmaxes_out, uint64_t rows_cap,
+                   int32_t* kmax_out, int32_t* lmax_out, double* seconds) {
     or_graph g;
     int rc = or_graph_build(V, E, src, dst, &g);
     if (rc != OR_OK) return rc;
+#ifdef _OPENMP
+    const double t_start = omp_get_wtime();
+#endif
+    if (seconds) *seconds = 0.0;
     or_scratch s0;
     uint64_t md = max_list(V, g.in_off), mo = max_list(V, g.out_off);
     if (scratch_init(&s0, V, md > mo ? md : mo) != OR_OK) { scratch_free(&s0); or_graph_free(&g); return OR_ERR_NOMEM; }
@@ -338,6 +357,9 @@ int or_dcore(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst, i
         }
         scratch_free(&s);
     }
+#ifdef _OPENMP
+    if (seconds) *seconds = omp_get_wtime() - t_start;
+#endif
     or_graph_free(&g);
     if (failed) return OR_ERR_NOMEM;
     *lmax_out = lm;

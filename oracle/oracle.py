@@ -34,6 +34,12 @@ def lib():
         _lib.or_dcore.restype = ctypes.c_int
         _lib.or_kedge_batches.argtypes = [ctypes.c_uint32, i32p, ctypes.c_uint64, u32p, u32p, i64p]
         _lib.or_kedge_batches.restype = ctypes.c_int64
+        _lib.og_gen_er.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p, u32p]
+        _lib.og_gen_er.restype = ctypes.c_int
+        _lib.og_gen_rmat.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, u32p, u32p,
+                                     ctypes.POINTER(ctypes.c_uint64)]
+        _lib.og_gen_rmat.restype = ctypes.c_int
     return _lib
 
 
@@ -84,6 +90,39 @@ def dcore(V, src, dst, threads=0):
     return km.value, lm.value, kmaxes[:V], rows[:, :V]
 
 
+def dcore_timed(V, src, dst, threads=0, rows=None):
+    """One full decomposition timed from the built CSR/CSC to the last row:
+    (kmax, lmax, kmaxes[V], rows[kmax+1, V], seconds, threads used).  rows
+    may be a preallocated int32 array of at least (kmax+1) * V values, so
+    that repeated calls do not allocate; it is sized by a kmax pass when
+    None or too small."""
+    L = lib()
+    L.or_dcore_timed.argtypes = [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_int, i32p, i32p,
+                                 ctypes.c_uint64, i32p, i32p, ctypes.POINTER(ctypes.c_double)]
+    L.or_dcore_timed.restype = ctypes.c_int
+    src, dst = _u32(src), _u32(dst)
+    kmaxes = np.empty(max(V, 1), np.int32)
+    km = ctypes.c_int32(0)
+    lm = ctypes.c_int32(0)
+    secs = ctypes.c_double(0)
+    nt = threads if threads > 0 else max_threads()
+    cap = 0 if rows is None else rows.size // max(V, 1)
+    if rows is None or cap == 0:
+        _, kmaxes_ = kmax(V, src, dst)
+        cap = int(kmaxes_.max()) + 1 if V else 1
+        rows = np.empty(cap * max(V, 1), np.int32)
+    rc = L.or_dcore_timed(V, len(src), _ptr(src, u32p), _ptr(dst, u32p), nt, _ptr(kmaxes, i32p),
+                          rows.ctypes.data_as(i32p), cap, ctypes.byref(km), ctypes.byref(lm), ctypes.byref(secs))
+    if rc == -5:  # the preallocated rows were too small: size them and run again
+        rows = np.empty((km.value + 1) * max(V, 1), np.int32)
+        return dcore_timed(V, src, dst, threads, rows)
+    if rc != 0:
+        raise RuntimeError(f"oracle or_dcore_timed failed: {rc}")
+    K = km.value
+    out = rows[:(K + 1) * max(V, 1)].reshape(K + 1, max(V, 1))[:, :V]
+    return K, lm.value, kmaxes[:V], out, secs.value, nt
+
+
 def kmax(V, src, dst):
     src, dst = _u32(src), _u32(dst)
     out = np.empty(max(V, 1), np.int32)
@@ -123,6 +162,31 @@ def rows_sample(V, src, dst, kmaxes, kmax, stride, threads=0):
     if n < 0:
         raise RuntimeError(f"oracle or_rows_sample failed: {n}")
     return n, secs.value
+
+
+def gen_er(n, m, seed):
+    """Seeded directed G(n, m), sorted by (src, dst): the engine's dc_gen_er
+    restated (gen_oracle.c)."""
+    src = np.empty(max(m, 1), np.uint32)
+    dst = np.empty(max(m, 1), np.uint32)
+    rc = lib().og_gen_er(n, m, seed, _ptr(src, u32p), _ptr(dst, u32p))
+    if rc:
+        raise RuntimeError(f"oracle og_gen_er failed: {rc}")
+    return src[:m], dst[:m]
+
+
+def gen_rmat(scale, edge_factor, seed, a=0.57, b=0.19, c=0.19, permute=True):
+    """Seeded R-MAT (self-loops and duplicates removed, labels permuted), the
+    engine's dc_gen_rmat restated (gen_oracle.c): (V, src, dst)."""
+    cap = edge_factor << scale
+    src = np.empty(max(cap, 1), np.uint32)
+    dst = np.empty(max(cap, 1), np.uint32)
+    n = ctypes.c_uint64(0)
+    rc = lib().og_gen_rmat(scale, edge_factor, a, b, c, seed, int(permute), cap, _ptr(src, u32p), _ptr(dst, u32p),
+                           ctypes.byref(n))
+    if rc:
+        raise RuntimeError(f"oracle og_gen_rmat failed: {rc}")
+    return 1 << scale, src[:n.value], dst[:n.value]
 
 
 def max_threads():

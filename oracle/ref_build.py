@@ -2,7 +2,8 @@
 the reference sources compiled where they lie (main.cu with its main()
 renamed, src/*.cpp, src/graph_gpu.cu), the harness oracle/ref_harness.cu and
 the allocation-padding shim oracle/ref_shim.h, for sm_100a.  Needs the
-reference checkout; the binary is then used by the tests and the benchmark
+reference checkout ($DCORE_REFERENCE, or "reference" beside this
+repository); the binary is then used by the tests and the benchmark
 only (never by the engine)."""
 import glob
 import os
@@ -11,7 +12,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF = os.environ.get("DCORE_REFERENCE", "/root/reference")
+# the reference checkout: $DCORE_REFERENCE, else a directory named
+# "reference" beside this repository's checkout
+REF = os.environ.get("DCORE_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 BIN = os.path.join(OUT, "ref_dcore")
 
 

@@ -4,8 +4,8 @@ The reference ships one worked example (dataset/ in llysdal/d-core-cuda):
   digraph             text graph, 8 vertices, 26 edges
   digraph-binary-g=1  its binary cache written by Graph::writeBinary
   digraph.decomp      its decomposition written by writeDecompFile
-These are data fixtures, copied byte for byte.  Run from a checkout that has
-the reference tree available; the copies are committed so the tests need only
+These are data fixtures, copied byte for byte.  Run with the reference checkout's
+path as the argument; the copies are committed so the tests need only
 this repository.
 """
 import os
@@ -24,4 +24,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference checkout>")
+    main(sys.argv[1])

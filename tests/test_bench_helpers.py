@@ -1,6 +1,8 @@
-"""Host-side helpers of the benchmark: the per-row peel byte model against a
-direct count on a small graph, the final edge set of an update stream, the
-seeded serving plan and the --tuning parser."""
+"""Host-side helpers of the benchmark: the byte models against direct counts
+on small graphs, the shared config of both arms, the reference arm's
+isolation from the engine library, the final edge set of an update stream,
+the seeded serving plan and the --tuning parser."""
+import json
 import os
 import sys
 
@@ -13,19 +15,53 @@ if ROOT not in sys.path:
 import bench  # noqa: E402
 
 
-def test_decomposition_bytes_model(dc, orc):
-    V, s, d = dc.gen_rmat(10, 8, 3)
-    K, kmaxes = orc.kmax(V, s, d)
-    m = bench.decomposition_bytes(V, s, d, kmaxes)
-    assert m["B_K"] == 12.0 * len(s) + 16.0 * V
-    assert len(m["B_row"]) == K + 1
-    deg = np.bincount(s, minlength=V) + np.bincount(d, minlength=V)
-    for k in (0, 1, K // 2, K):
+def test_refinement_bytes_model(orc):
+    """The row-refinement byte model against a direct count: every value
+    that changes from row k-1 to row k reads its lists' entries inside C_k."""
+    V, s, d = orc.gen_rmat(10, 8, 3)
+    K, L, kmaxes, rows = orc.dcore(V, s, d)
+    b, changes, entries = bench.refinement_bytes(V, s, d, kmaxes, rows)
+    n_ch = n_ent = 0
+    for k in range(1, K + 1):
         inside = kmaxes >= k
-        Vk = inside.sum()
-        Dk = deg[inside].sum()
-        Ik = (inside[s] & inside[d]).sum()
-        assert m["B_row"][k] == 8 * Dk + 16 * Ik + 24 * Vk + 4 * (V - Vk)
+        for v in np.nonzero(inside & (rows[k] != rows[k - 1]))[0]:
+            n_ch += 1
+            n_ent += int(inside[d[s == v]].sum() + inside[s[d == v]].sum())
+    assert (changes, entries) == (n_ch, n_ent)
+    assert b == 8.0 * n_ent + 20.0 * n_ch + 4.0 * (V - np.count_nonzero(kmaxes == K))
+
+
+def test_peel_bytes_model(orc):
+    V, s, d = orc.gen_rmat(9, 8, 2)
+    E = len(s)
+    assert bench.peel_bytes(V, s, d, None) == (12.0 * E + 16.0 * V) + (16.0 * E + 16.0 * E + 24.0 * V)
+
+
+def test_decomp_config_is_the_same_for_both_arms():
+    """The reference arm and the engine arm print one config for a workload."""
+    class A:
+        workload = "decomp-rmat22"
+    w = bench.WORKLOADS["decomp-rmat22"]
+    a = bench.decomp_config(A, w, 4194304, 65245102, 592, 591, 1)
+    b = bench.decomp_config(A, w, 4194304, 65245102, 592, 591, 1)
+    assert a == b and a["workload"] == "decomp-rmat22" and a["E"] == 65245102
+
+
+def test_reference_arm_does_not_load_the_engine(tmp_path):
+    """bench.py --impl reference runs the oracle alone: the engine library
+    must not be loaded by that process."""
+    import subprocess
+    code = ("import sys, json; sys.argv=['bench.py','--impl','reference','--workload','decomp-er10k',"
+            "'--steps','1','--warmup','1']; import bench; bench.main(); "
+            "print(json.dumps([m for m in open('/proc/self/maps').read().split() if m.endswith('.so')]))")
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = p.stdout.strip().splitlines()
+    line = json.loads(lines[0])
+    maps = json.loads(lines[-1])
+    assert line["impl"] == "reference" and line["config"]["E"] == 100_000 and line["steps"] == 1
+    assert not any("libdcore_b200" in m for m in maps)
+    assert any("liboracle" in m for m in maps)
 
 
 def test_final_edges_of_a_stream(dc):

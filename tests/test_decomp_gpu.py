@@ -82,6 +82,24 @@ def test_rmat_medium_incremental(dc, orc, gpu, scale, seed):
     check_against_oracle(dc, orc, V, s, d, 0)
 
 
+@pytest.mark.parametrize("tuned", [False, True])
+def test_rmat20_against_oracle(dc, orc, gpu, tuned):
+    """R-MAT 20 (1M vertices, 16M edges): large enough for long cascades in
+    the persistent kernels' queues, checked value by value against the
+    oracle, with the default launch shapes and with row segments."""
+    V, s, d = dc.gen_rmat(20, 16, 7)
+    okm, olm, okmaxes, orows = orc.dcore(V, s, d)
+    with dc.Graph.from_edges(V, s, d) as g:
+        if tuned:
+            g.set_tuning(3, 3, 128, [150, 200, 450])
+        assert g.decompose() == (okm, olm)
+        assert np.array_equal(g.kmaxes(), okmaxes)
+        for k0 in range(0, okm + 1, 64):
+            n = min(64, okm + 1 - k0)
+            bad = np.argwhere(g.rows(k0, n) != orows[k0:k0 + n])
+            assert bad.size == 0, f"rows {k0}..: {len(bad)} mismatches, first {bad[:3].tolist()}"
+
+
 @pytest.mark.parametrize("method", METHODS)
 def test_edge_cases(dc, orc, gpu, method):
     z = np.zeros(0, np.uint32)

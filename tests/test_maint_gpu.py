@@ -60,6 +60,37 @@ def test_mixed_stream_matches_recompute(dc, orc, gpu, method, scale, seed, repai
             i += bs
 
 
+def test_rmat20_mixed_batches_against_oracle(dc, orc, gpu):
+    """R-MAT 20 (1M vertices) with a mixed stream in batches of 10,000, 100
+    and 1 under the engine's own method choice and row repair: after each
+    batch kmaxes and every row equal the oracle's decomposition of the
+    updated graph."""
+    V, s, d = dc.gen_rmat(20, 16, 12)
+    u, v, dl = dc.gen_updates(V, s, d, 10_101, 0.5, 77)
+    base = (s.astype(np.uint64) << np.uint64(32)) | d
+    with dc.Graph.from_edges(V, s, d, gap_min=2, gap_div=16) as g:
+        g.decompose()
+        i = 0
+        for bs in (10_000, 100, 1):
+            g.maintain(u[i:i + bs], v[i:i + bs], dl[i:i + bs])
+            i += bs
+            # the edge set after the first i operations (a valid stream:
+            # deletions remove present edges, insertions add absent ones)
+            ops = (u[:i].astype(np.uint64) << np.uint64(32)) | v[:i]
+            keys, inv = np.unique(np.concatenate([base, ops]), return_inverse=True)
+            mult = np.bincount(inv, weights=np.concatenate([np.ones(len(base)), np.where(dl[:i] == 1, -1.0, 1.0)]),
+                               minlength=len(keys))
+            live = keys[mult > 0]
+            fs, fd = (live >> np.uint64(32)).astype(np.uint32), (live & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+            okm, olm, okmaxes, orows = orc.dcore(V, fs, fd)
+            info = g.decomp_info()
+            assert (info["kmax"], info["lmax"]) == (okm, olm)
+            assert np.array_equal(g.kmaxes(), okmaxes)
+            for k0 in range(0, okm + 1, 64):
+                n = min(64, okm + 1 - k0)
+                assert np.array_equal(g.rows(k0, n), orows[k0:k0 + n]), (bs, k0)
+
+
 @pytest.mark.parametrize("method", METHODS)
 def test_er10k_single_inserts_and_deletes(dc, orc, gpu, method):
     s, d = dc.gen_er(10_000, 100_000, 2)

@@ -1,6 +1,6 @@
 """Row sharding on one GPU: the ranges a multi-GPU run would give to its
 ranks, computed one after another on one device (ranks never wait on one
-another, so this is exactly their work), together equal the full
+another, so this is exactly their work), together equal the oracle's full
 decomposition."""
 import numpy as np
 import pytest
@@ -11,12 +11,9 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("scale,ef,seed,world", [(12, 8, 1, 2), (14, 16, 2, 4), (15, 16, 3, 8)])
-def test_row_ranges_cover_full_decomposition(dc, gpu, scale, ef, seed, world):
+def test_row_ranges_cover_full_decomposition(dc, orc, gpu, scale, ef, seed, world):
     V, s, d = dc.gen_rmat(scale, ef, seed)
-    with dc.Graph.from_edges(V, s, d) as full:
-        K, L = full.decompose()
-        ref_rows = full.rows()
-        ref_km = full.kmaxes()
+    K, L, ref_km, ref_rows = orc.dcore(V, s, d)
     with dc.Graph.from_edges(V, s, d) as g:
         k, l = g.decompose_rows(1, 0)  # kmax and row 0 only
         assert (k, l) == (K, L)

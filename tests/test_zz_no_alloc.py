@@ -50,16 +50,37 @@ def _regular_kmax(dc, V, src, dst):
         return g.kmaxes(), kmax
 
 
-def test_noalloc_kmax_matches_regular_entry_point_twice_in_a_row(dc, gpu):
+def test_noalloc_kmax_matches_regular_entry_point_twice_in_a_row(dc, orc, gpu):
     graphs = [dc.gen_rmat(14, 16, 21), dc.gen_rmat(13, 8, 22)]
     s, d = dc.gen_er(10_000, 100_000, 23)
     graphs.append((10_000, s, d))
     for V, src, dst in graphs:
         ref, ref_max = _regular_kmax(dc, V, src, dst)
+        o_max, o_kmaxes = orc.kmax(V, src, dst)
+        assert o_max == ref_max and np.array_equal(o_kmaxes, ref)
         for _ in range(2):  # back to back: the scratch keeps the previous call's contents
             got, got_max = _noalloc_kmax(dc, V, src, dst)
             assert got_max == ref_max
             assert np.array_equal(got, ref)
+
+
+def test_noalloc_rejects_edge_count_that_disagrees_with_the_arrays(dc, gpu):
+    """The fixed queue ring is sized from E, so E must be the number of
+    edges the offset arrays really hold."""
+    import torch
+    V, src, dst = dc.gen_rmat(10, 8, 24)
+    in_off, out_off, out_nbr = _csr(V, src, dst)
+    dev = torch.device("cuda", 0)
+    t_in = torch.from_numpy(in_off.view(np.int32)).to(dev)
+    t_oo = torch.from_numpy(out_off.view(np.int32)).to(dev)
+    t_on = torch.from_numpy(np.ascontiguousarray(out_nbr).view(np.int32)).to(dev)
+    t_k = torch.zeros(V, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    torch.cuda.synchronize()
+    rc = dc.lib().dc_kmax_noalloc(V, len(src) - 1, t_in.data_ptr(), t_oo.data_ptr(), t_on.data_ptr(),
+                                  t_k.data_ptr(), None, stream)
+    assert rc == -1
+    assert "out_off[V]" in dc.last_error()
 
 
 def test_noalloc_rejects_graphs_beyond_its_limit(dc, gpu):
