@@ -520,6 +520,21 @@ extern "C" int dc_set_launch(dc_graph* h, int blocks_per_sm) {
     return DC_OK;
 }
 
+extern "C" int dc_set_wait_limit(dc_graph* h, uint64_t ns) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    if (ns != 0 && (ns < 1000000ull || ns > 600000000000ull))
+        return set_error(DC_ERR_INVALID, "wait limit must be 0 (default) or 1 ms .. 600 s");
+    h->wait_ns = ns;
+    return DC_OK;
+}
+
+extern "C" int dc_test_withhold_barrier(dc_graph* h, int32_t block) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    if (block < -1) return set_error(DC_ERR_INVALID, "block must be -1 (off) or a block index");
+    h->barrier_fault_block = block;
+    return DC_OK;
+}
+
 extern "C" int dc_get_tuning(dc_graph* h, dc_tuning* t) {
     if (!h || !t) return set_error(DC_ERR_INVALID, "null argument");
     const int dflt = h->blocks_per_sm > 0 ? h->blocks_per_sm : 2;

@@ -4,9 +4,10 @@
 //   - work queue: ring of vertex ids with claim / done counters and a
 //     termination test, so cascades run without per-round barriers
 //   - warp-aggregated append
-// Every spin in here is bounded by kWaitNs of %globaltimer time; on expiry
-// the waiter sets DC_DEV_ERR_TIMEOUT in EngineCtl::error and returns, so a
-// fault in the protocol ends the kernel with a status instead of a hang.
+// Every spin in here is bounded by the control block's wait limit
+// (EngineCtl::wait_ns, kWaitNs when 0) of %globaltimer time; on expiry the
+// waiter sets DC_DEV_ERR_TIMEOUT in EngineCtl::error and returns, so a fault
+// in the protocol ends the kernel with a status instead of a hang.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -20,7 +21,7 @@ constexpr unsigned DC_DEV_ERR_CAPACITY = 8u;  // a log or list buffer overflowed
 constexpr unsigned DC_DEV_ERR_NOTFOUND = 16u; // delete of an absent edge
 
 constexpr uint32_t kEmptySlot = 0xFFFFFFFFu;
-constexpr unsigned long long kWaitNs = 4000000000ull;  // 4 s per wait
+constexpr unsigned long long kWaitNs = 4000000000ull;  // default limit of one wait: 4 s
 constexpr int kMaxRowSegments = 8;  // concurrent launches a full run of rows may split into
 constexpr int kMinSplitRows = 32;   // runs of fewer rows are never split
 
@@ -81,7 +82,18 @@ struct EngineCtl {
     unsigned long long* trace;
     unsigned trace_cap;
     unsigned trace_tail0;
+    // limit of one bounded wait in ns (0: kWaitNs)
+    unsigned long long wait_ns;
+    // failure-detection tests: block test_skip_block - 1 leaves at its first
+    // grid barrier without arriving, so every other block's barrier wait runs
+    // out (0: off)
+    int test_skip_block;
 };
+
+__device__ __forceinline__ unsigned long long wait_limit(const EngineCtl* c) {
+    const unsigned long long w = *reinterpret_cast<const volatile unsigned long long*>(&c->wait_ns);
+    return w ? w : kWaitNs;
+}
 
 __device__ __forceinline__ unsigned ld_vol(const unsigned* p) {
     return *reinterpret_cast<const volatile unsigned*>(p);
@@ -102,10 +114,11 @@ __device__ __forceinline__ void set_dev_error(EngineCtl* c, unsigned code, unsig
 
 // Software grid barrier.  All blocks of a cooperative launch are co-resident,
 // so every block reaches it unless one has already bailed out on an error;
-// waiters then leave on the error word or after kWaitNs.
+// waiters then leave on the error word or after the wait limit.
 // Returns true when the grid may continue.
 __device__ __forceinline__ bool grid_sync(EngineCtl* c) {
     __shared__ unsigned s_ok;
+    if (c->test_skip_block && (int)blockIdx.x == c->test_skip_block - 1) return false;
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned nb = gridDim.x;
@@ -117,10 +130,10 @@ __device__ __forceinline__ bool grid_sync(EngineCtl* c) {
             __threadfence();
             atomicAdd(&c->bar_gen, 1u);
         } else {
-            unsigned long long t0 = gtimer();
+            const unsigned long long t0 = gtimer(), lim = wait_limit(c);
             while (ld_vol(&c->bar_gen) == gen) {
                 if (ld_vol(&c->error)) break;
-                if (gtimer() - t0 > kWaitNs) {
+                if (gtimer() - t0 > lim) {
                     set_dev_error(c, DC_DEV_ERR_TIMEOUT, 1);
                     break;
                 }
@@ -139,6 +152,7 @@ __device__ __forceinline__ bool grid_sync(EngineCtl* c) {
 template <typename Hook>
 __device__ __forceinline__ bool grid_sync_hook(EngineCtl* c, Hook hook) {
     __shared__ unsigned s_ok2;
+    if (c->test_skip_block && (int)blockIdx.x == c->test_skip_block - 1) return false;
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned nb = gridDim.x;
@@ -151,10 +165,10 @@ __device__ __forceinline__ bool grid_sync_hook(EngineCtl* c, Hook hook) {
             __threadfence();
             atomicAdd(&c->bar_gen, 1u);
         } else {
-            unsigned long long t0 = gtimer();
+            const unsigned long long t0 = gtimer(), lim = wait_limit(c);
             while (ld_vol(&c->bar_gen) == gen) {
                 if (ld_vol(&c->error)) break;
-                if (gtimer() - t0 > kWaitNs) {
+                if (gtimer() - t0 > lim) {
                     set_dev_error(c, DC_DEV_ERR_TIMEOUT, 4);
                     break;
                 }
@@ -250,12 +264,12 @@ __device__ __forceinline__ uint32_t q_take(EngineCtl* c, RingQueue q, unsigned i
     uint32_t* s = &q.slots[idx & q.mask];
     uint32_t v = atomicExch(s, kEmptySlot);
     if (v != kEmptySlot) return v;
-    unsigned long long t0 = gtimer();
+    const unsigned long long t0 = gtimer(), lim = wait_limit(c);
     for (;;) {
         v = atomicExch(s, kEmptySlot);
         if (v != kEmptySlot) return v;
         if (ld_vol(&c->error)) return kEmptySlot;
-        if (gtimer() - t0 > kWaitNs) {
+        if (gtimer() - t0 > lim) {
             set_dev_error(c, DC_DEV_ERR_TIMEOUT, 2);
             return kEmptySlot;
         }
@@ -413,7 +427,7 @@ __device__ __forceinline__ bool tq_take_warp(EngineCtl* c, TicketQueue q, unsign
                 break;
             }
             if (++spins == 64) t0 = gtimer();
-            if (spins > 64 && (spins & 63) == 0 && gtimer() - t0 > kWaitNs) {
+            if (spins > 64 && (spins & 63) == 0 && gtimer() - t0 > wait_limit(c)) {
                 set_dev_error(c, DC_DEV_ERR_TIMEOUT, 5);
                 *ticket = kNoTicket;
                 state = 2;
@@ -430,7 +444,7 @@ __device__ __forceinline__ bool tq_take_warp(EngineCtl* c, TicketQueue q, unsign
 }
 
 // Idle-wait helper for the drain loops: returns false once the phase has made
-// no progress for kWaitNs (error recorded).
+// no progress for the wait limit (error recorded).
 struct IdleClock {
     unsigned long long t0;
     unsigned last_done;
@@ -445,7 +459,7 @@ struct IdleClock {
             t0 = gtimer();
             return true;
         }
-        if (gtimer() - t0 > kWaitNs) {
+        if (gtimer() - t0 > wait_limit(c)) {
             set_dev_error(c, DC_DEV_ERR_TIMEOUT, 3);
             return false;
         }

@@ -1700,9 +1700,14 @@ static int persistent_launch(dc_graph* h, const void* fn, void** args, const cha
     EngineCtl& init = *initp;
     memset(&init, 0, sizeof(init));
     init.step = -1;
+    init.wait_ns = h->wait_ns;
     if (own) {
         init.trace = h->trace_dev;
         init.trace_cap = h->trace_cap;
+        if (h->barrier_fault_block >= 0) {  // one launch only
+            init.test_skip_block = h->barrier_fault_block + 1;
+            h->barrier_fault_block = -1;
+        }
     }
     DC_CUDA(cudaMemcpyAsync(ctl, &init, sizeof(EngineCtl), cudaMemcpyHostToDevice, st));
     if (own && h->trace_dev) DC_CUDA(cudaMemsetAsync(h->trace_dev, 0, 64ull * h->trace_cap, st));

@@ -120,6 +120,11 @@ struct dc_graph {
              seg_void[dc::kMaxRowSegments - 1] = {};
     uint64_t stat_evals = 0, stat_drops = 0, stat_entries = 0;
     uint64_t full_work = 0;  // sum over vertices of degree x kmax at the last full decomposition
+    // limit of one bounded device wait in ns (0: the default, dc::kWaitNs)
+    uint64_t wait_ns = 0;
+    // failure-detection tests: block of the next persistent launch that
+    // leaves at its first grid barrier without arriving (-1: none)
+    int32_t barrier_fault_block = -1;
     dc::EngineCtl ctl_init{};
     dc::EngineCtl ctl_init_seg[dc::kMaxRowSegments - 1] = {};  // the other row segments'
     // optional per-step trace of persistent kernels (diagnostics)

@@ -744,6 +744,8 @@ static int apply_deletions(dc_graph* h, const NetBatch& nb) {
         return rc;
     }
     MT_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
+    if (h->wait_ns)
+        MT_CUDA(cudaMemcpyAsync(&h->ctl->wait_ns, &h->wait_ns, sizeof(h->wait_ns), cudaMemcpyHostToDevice, h->stream));
     ++g_launches;
     k_del_validate<<<mgrid(h, nb.del_u.size() * 32), kMThreads, 0, h->stream>>>(
         (uint32_t)nb.del_u.size(), du, dv, dn, g.out_off, g.out_len, g.out_nbr, h->ctl);
@@ -838,6 +840,8 @@ static int apply_insertions(dc_graph* h, const NetBatch& nb, uint32_t** d_iu_out
     MT_CUDA(cudaMemsetAsync(s->key2, 0, 4ull * V, h->stream));
     MT_CUDA(cudaMemsetAsync(s->cdeg2, 0, 4ull * V, h->stream));
     MT_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
+    if (h->wait_ns)
+        MT_CUDA(cudaMemcpyAsync(&h->ctl->wait_ns, &h->wait_ns, sizeof(h->wait_ns), cudaMemcpyHostToDevice, h->stream));
     ++g_launches;
     k_ins_need<<<mgrid(h, n), kMThreads, 0, h->stream>>>(n, iu, iv, s->key2, s->cdeg2);
     ++g_launches;

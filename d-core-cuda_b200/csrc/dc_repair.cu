@@ -217,7 +217,7 @@ __device__ bool r_take(const RepairParams& p, RowState& S, unsigned* slot) {
                 break;
             }
             if (spins == 64) t0 = gtimer();
-            if (spins > 64 && (spins & 63) == 0 && gtimer() - t0 > kWaitNs) {
+            if (spins > 64 && (spins & 63) == 0 && gtimer() - t0 > wait_limit(p.ctl)) {
                 set_dev_error(p.ctl, DC_DEV_ERR_TIMEOUT, 40);
                 atomicExch(&S.abort, 1);
                 state = 2;
@@ -621,6 +621,8 @@ int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_
         s->log_cap = cap;
     }
     RP_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
+    if (h->wait_ns)
+        RP_CUDA(cudaMemcpyAsync(&h->ctl->wait_ns, &h->wait_ns, sizeof(h->wait_ns), cudaMemcpyHostToDevice, h->stream));
     RP_CUDA(cudaStreamSynchronize(h->stream));
     RepairParams p;
     p.V = V;

@@ -155,6 +155,8 @@ SIGNATURES = {
     "dc_server_graph_result": [vp, ctypes.c_uint32, i32p, i32p, ctypes.c_uint64, i32p],
     "dc_server_free": [vp],
     "dc_server_set_row_repair": [vp, ctypes.c_int],
+    "dc_set_wait_limit": [vp, ctypes.c_uint64],
+    "dc_test_withhold_barrier": [vp, ctypes.c_int32],
     "dc_kmax_noalloc": [ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp, vp, i32p, vp],
     "dc_plan_row_cuts": [i32p, f32p, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, i32p, f32p],
     "dc_launch_count": [u64p],
@@ -592,6 +594,16 @@ class Graph:
 
     def set_launch(self, blocks_per_sm):
         _check(lib().dc_set_launch(self._h, blocks_per_sm))
+
+    def set_wait_limit(self, ns):
+        """Limit of every bounded device wait (ns; 0 = the 4 s default)."""
+        _check(lib().dc_set_wait_limit(self._h, int(ns)))
+
+    def withhold_barrier(self, block=0):
+        """Failure-detection tests: block `block` of the next persistent
+        launch leaves at its first grid barrier without arriving (-1
+        cancels)."""
+        _check(lib().dc_test_withhold_barrier(self._h, int(block)))
 
     def synchronize(self):
         _check(lib().dc_synchronize(self._h))

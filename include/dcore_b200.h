@@ -407,6 +407,20 @@ int dc_autotune(dc_graph* g, dc_tuning* best, float* best_ms);
 int dc_plan_row_cuts(const int32_t* grid, const float* cost, int32_t n, float total, int32_t ncut, int32_t* cuts,
                      float* longest);
 
+/* Limit of every bounded device-side wait of this handle's kernels (grid
+ * barriers, work-queue waits), in ns: 0 restores the default of 4 s, else
+ * 1 ms .. 600 s.  A wait that runs out ends the kernel and the call returns
+ * DC_ERR_TIMEOUT; the handle stays usable.  No reference counterpart (the
+ * reference's kernels have no bounded waits and trap on a full buffer,
+ * src/cuda_utils.cuh:7,11). */
+int dc_set_wait_limit(dc_graph* g, uint64_t ns);
+/* Failure-detection tests: block `block` of the handle's next persistent
+ * launch leaves at its first grid barrier without arriving, so the other
+ * blocks' barrier waits run out and the call returns DC_ERR_TIMEOUT after
+ * the wait limit; applies to one launch, -1 cancels.  No reference
+ * counterpart. */
+int dc_test_withhold_barrier(dc_graph* g, int32_t block);
+
 /* Engine kernel launches since the library was loaded. */
 int dc_launch_count(unsigned long long* n);
 
