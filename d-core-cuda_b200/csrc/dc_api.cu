@@ -297,6 +297,15 @@ extern "C" int dc_row_weights(dc_graph* h, uint64_t* weights, uint64_t capacity)
     return row_weights(h, weights);
 }
 
+extern "C" int dc_graph_kmax_edge_batches(dc_graph* h, uint64_t B, const uint32_t* d_from, const uint32_t* d_to,
+                                          int64_t* d_batch_of, int64_t* n_batches) {
+    if (!h || !n_batches || (B && (!d_from || !d_to || !d_batch_of)))
+        return set_error(DC_ERR_INVALID, "dc_graph_kmax_edge_batches: null argument");
+    if (!h->d.peel_valid) return set_error(DC_ERR_STATE, "no kmax on this graph (dc_decompose first)");
+    API_CUDA(cudaSetDevice(h->device));
+    return kmax_edge_batches_device(h, B, d_from, d_to, d_batch_of, n_batches);
+}
+
 extern "C" int dc_maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_delete, uint64_t b, int method,
                            dc_maint_stats* stats) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");

@@ -99,6 +99,11 @@ bool row_repair_worthwhile(dc_graph* h, const uint32_t* d_u, const uint32_t* d_v
 // Maintenance method for a batch (rule of thumb or the learned scheduler).
 int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del);
 
+// KEDGE_BATCHING partition of a device edge batch by the graph's current
+// kmax (dc_partition.cu).
+int kmax_edge_batches_device(dc_graph* h, uint64_t B, const uint32_t* d_from, const uint32_t* d_to,
+                             int64_t* d_batch_of, int64_t* n_batches);
+
 // Full decomposition; method 0 = incremental rows, 1 = per-row peel.
 int decompose(dc_graph* h, int method, int materialize_rows);
 // Rows K0..Kstop from row 0 (in the scratch row0) and kmax; corners left in

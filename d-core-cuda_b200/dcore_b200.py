@@ -157,6 +157,7 @@ SIGNATURES = {
     "dc_server_set_row_repair": [vp, ctypes.c_int],
     "dc_set_wait_limit": [vp, ctypes.c_uint64],
     "dc_test_withhold_barrier": [vp, ctypes.c_int32],
+    "dc_graph_kmax_edge_batches": [vp, ctypes.c_uint64, vp, vp, vp, ctypes.POINTER(ctypes.c_int64)],
     "dc_kmax_noalloc": [ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp, vp, i32p, vp],
     "dc_plan_row_cuts": [i32p, f32p, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, i32p, f32p],
     "dc_launch_count": [u64p],
@@ -594,6 +595,15 @@ class Graph:
 
     def set_launch(self, blocks_per_sm):
         _check(lib().dc_set_launch(self._h, blocks_per_sm))
+
+    def kmax_edge_batches_device(self, d_from_ptr, d_to_ptr, B, d_batch_of_ptr):
+        """getKmaxEdgeBatches (KEDGE_BATCHING) on the GPU by the graph's
+        current kmax: device arrays in and out; returns the number of
+        sub-batches."""
+        n = ctypes.c_int64(0)
+        _check(lib().dc_graph_kmax_edge_batches(self._h, int(B), vp(d_from_ptr), vp(d_to_ptr), vp(d_batch_of_ptr),
+                                                ctypes.byref(n)))
+        return n.value
 
     def set_wait_limit(self, ns):
         """Limit of every bounded device wait (ns; 0 = the 4 s default)."""

@@ -284,6 +284,18 @@ int dc_maint_log_get(dc_graph* g, float* features, int32_t* methods, float* time
 int dc_kmax_edge_batches(uint32_t V, const int32_t* kmaxes, uint64_t B, const uint32_t* from, const uint32_t* to,
                          int64_t* batch_of, int64_t* n_batches);
 
+/* The same partition on the GPU, for batches already in device memory:
+ * d_from[B], d_to[B] (device) against the graph's current kmax values (after
+ * dc_decompose or dc_maintain), d_batch_of[B] (device) receives the
+ * sub-batch of every edge, numbered exactly as dc_kmax_edge_batches numbers
+ * them; *n_batches (host) their number.  Runs on the graph's stream with
+ * O(B) work and scratch (a stable radix sort of the edges by root), where the
+ * reference allocates and scans a vector<bool>(V) per sub-batch on the host
+ * (getKmaxEdgeBatches, main.cu:1441-1488; vector<bool> at main.cu:1469).
+ * B < 2^31. */
+int dc_graph_kmax_edge_batches(dc_graph* g, uint64_t B, const uint32_t* d_from, const uint32_t* d_to,
+                               int64_t* d_batch_of, int64_t* n_batches);
+
 /* kmax of every vertex (in-degree core numbers, the values dc_decompose
  * reports through dc_get_kmaxes) without allocating any device memory.  No
  * counterpart in the reference: it is for callers that cannot let a library
