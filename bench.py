@@ -958,7 +958,9 @@ def run_decomposition(args, w, rank, world, local, dist):
                            "tuning": dict(tuning, source=tune_src),
                            "step": "first decomposition of a freshly built handle (CSR/CSC built untimed from "
                                    "the HBM-resident edge list)"},
-                "phases_ms": {"peel": peel_ms, "rows": rows_ms, "other": ms_per_step - peel_ms - rows_ms},
+                "phases_ms": {"peel": peel_ms, "rows": rows_ms, "other": ms_per_step - peel_ms - rows_ms,
+                              "of_other": {k: float(np.mean([i[k + "_ms"] for i in infos]))
+                                           for k in ("row0", "skyline", "expand")}},
                 "step_ms": times, "gpu_launches": int(launches), "roofline": roof, "parity": parity,
                 "single_launch_rows": single, "e2e": e2e, "cpu_baseline": cpu, "reference_gpu": ref,
                 "clocks": clocks}

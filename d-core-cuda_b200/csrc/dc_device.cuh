@@ -397,6 +397,36 @@ __device__ __forceinline__ void tq_push_warp4(EngineCtl* c, TicketQueue q, unsig
     }
 }
 
+// Converged warp: each lane pushes items[r] for every bit r set in mask
+// (r < 4), in bit order.
+__device__ __forceinline__ void tq_push_warp_mask4(EngineCtl* c, TicketQueue q, unsigned mask,
+                                                   const uint32_t items[4]) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned cnt = __popc(mask);
+    unsigned x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (unsigned)o) x += y;
+    }
+    unsigned total = __shfl_sync(0xFFFFFFFFu, x, 31);
+    if (total == 0) return;
+    unsigned base = 0;
+    if (lane == 0) {
+        atomicAdd(&c->outstanding, (int)total);
+        base = atomicAdd(&c->t_tail, total);
+    }
+    base = __shfl_sync(0xFFFFFFFFu, base, 0) + (x - cnt);
+    if (cnt) __threadfence();
+#pragma unroll
+    for (unsigned r = 0; r < 4; ++r) {
+        if (mask & (1u << r)) {
+            volatile unsigned long long* s = &q.slots[(base + __popc(mask & ((1u << r) - 1u))) & q.mask];
+            *s = (unsigned long long)items[r];
+        }
+    }
+}
+
 // Converged warp: returns true with *item set, or false when the phase is
 // over (or an error / timeout occurred).  *ticket holds the warp's current
 // ticket between calls (kNoTicket initially).
@@ -441,6 +471,25 @@ __device__ __forceinline__ bool tq_take_warp(EngineCtl* c, TicketQueue q, unsign
     __threadfence();
     *item = it;
     return state == 1;
+}
+
+// tq_take_warp with lazily counted finishes: *pending (lane 0's count of
+// items this warp finished but has not yet subtracted from `outstanding`) is
+// subtracted in one atomic when the warp's slot is not filled at once, i.e.
+// before the warp can wait; a warp that keeps finding items never touches
+// `outstanding` for them until then.  On a false return *pending is 0.
+__device__ __forceinline__ bool tq_take_warp_lazy(EngineCtl* c, TicketQueue q, unsigned* ticket,
+                                                  unsigned long long* item, unsigned* pending) {
+    const unsigned lane = threadIdx.x & 31u;
+    if (lane == 0) {
+        if (*ticket == kNoTicket) *ticket = atomicAdd(&c->t_head, 1u);
+        volatile unsigned long long* s = &q.slots[*ticket & q.mask];
+        if (*s == kEmptyItem && *pending) {
+            tq_finish(c, (int)*pending);
+            *pending = 0;
+        }
+    }
+    return tq_take_warp(c, q, ticket, item);
 }
 
 // Idle-wait helper for the drain loops: returns false once the phase has made

@@ -106,6 +106,44 @@ __device__ unsigned long long block_excl_scan64(unsigned long long x, unsigned l
     return res;
 }
 
+// Block-wide reservation for the peel's scans: every thread of the block
+// contributes nk entries to append to a list (counter *list_ctr) and ni queue
+// items; thread 0 reserves both ranges with one atomic each (the items'
+// outstanding count is raised before their slots can be filled) and every
+// thread gets its own offsets.  All threads of the block must call it.
+__device__ __forceinline__ void block_reserve(EngineCtl* c, unsigned* list_ctr, unsigned nk, unsigned ni,
+                                              unsigned* keep_off, unsigned* item_off) {
+    __shared__ unsigned s_kb, s_ib;
+    unsigned long long tot;
+    const unsigned long long ex = block_excl_scan64(((unsigned long long)nk << 32) | ni, &tot);
+    if (threadIdx.x == 0) {
+        const unsigned tk = (unsigned)(tot >> 32), ti = (unsigned)tot;
+        s_kb = tk ? atomicAdd(list_ctr, tk) : 0u;
+        s_ib = 0;
+        if (ti) {
+            atomicAdd(&c->outstanding, (int)ti);
+            s_ib = atomicAdd(&c->t_tail, ti);
+        }
+    }
+    __syncthreads();
+    *keep_off = s_kb + (unsigned)(ex >> 32);
+    *item_off = s_ib + (unsigned)ex;
+    __syncthreads();
+}
+
+// Block-wide minimum, one global atomicMin per block (all threads call it).
+__device__ __forceinline__ void block_atomic_min(int* dst, int x) {
+    __shared__ int s_m;
+    if (threadIdx.x == 0) s_m = 0x7FFFFFFF;
+    __syncthreads();
+#pragma unroll
+    for (int o = 16; o; o >>= 1) x = min(x, __shfl_xor_sync(0xFFFFFFFFu, x, o));
+    if ((threadIdx.x & 31u) == 0 && x != 0x7FFFFFFF) atomicMin(&s_m, x);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_m != 0x7FFFFFFF) atomicMin(dst, s_m);
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // cooperative exclusive scan (u64), n elements in place; out[n] = total
 // ---------------------------------------------------------------------------
@@ -345,11 +383,11 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
     if (threadIdx.x == 0) s_prod = 0;
     __syncthreads();
 
-    // ---- init
+    // ---- init (remaining lists appended block by block: one atomic per block chunk)
     for (int i = 0; i < p.ninst; ++i) {
         const PeelInst& I = p.in[i];
-        for (uint64_t base = (uint64_t)gwarp * 32; base < p.V; base += (uint64_t)nwarps * 32) {
-            uint64_t vi = base + lane;
+        for (uint64_t base = (uint64_t)blockIdx.x * kThreads; base < p.V; base += (uint64_t)gridDim.x * kThreads) {
+            uint64_t vi = base + threadIdx.x;
             bool ok = vi < p.V, in = false;
             uint32_t v = (uint32_t)vi;
             if (ok) {
@@ -372,7 +410,8 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
                     I.cdeg[v] = cd;
                 }
             }
-            unsigned pos = warp_append(&c->rc_next[i].v, ok && in);
+            unsigned pos, unused;
+            block_reserve(c, &c->rc_next[i].v, (ok && in) ? 1u : 0u, 0u, &pos, &unused);
             if (ok && in) I.rem0[pos] = v;
         }
     }
@@ -391,9 +430,11 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
             const unsigned n_rem = ld_vol(&c->rc_cur[i]);
             const uint32_t* rc = (it & 1) ? I.rem1 : I.rem0;
             uint32_t* rn = (it & 1) ? I.rem0 : I.rem1;
+            // block-cooperative: the kept vertices and the pushed items of a
+            // chunk of blockDim vertices take one reservation per block
             int kmin = 0x7FFFFFFF;
-            for (unsigned base = gwarp * 32; base < n_rem; base += nwarps * 32) {
-                unsigned idx = base + lane;
+            for (unsigned base = blockIdx.x * kThreads; base < n_rem; base += gridDim.x * kThreads) {
+                unsigned idx = base + threadIdx.x;
                 bool ok = idx < n_rem;
                 uint32_t v = ok ? rc[idx] : 0;
                 bool keep = false, push = false;
@@ -406,25 +447,32 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
                         kmin = min(kmin, kv);
                     }
                 }
-                unsigned pos = warp_append(&c->rc_next[i].v, keep);
-                if (keep) rn[pos] = v;
-                unsigned cnt = push ? peel_nitems(I, v, CH) : 0u;
-                tq_push_warp_multi(c, p.q, cnt, peel_item(v, 0, i), 1ull << 32);
+                const unsigned cnt = push ? peel_nitems(I, v, CH) : 0u;
+                unsigned kpos, ipos;
+                block_reserve(c, &c->rc_next[i].v, keep ? 1u : 0u, cnt, &kpos, &ipos);
+                if (keep) rn[kpos] = v;
+                if (cnt) {
+                    __threadfence();
+                    for (unsigned j = 0; j < cnt; ++j) {
+                        volatile unsigned long long* sl = &p.q.slots[(ipos + j) & p.q.mask];
+                        *sl = peel_item(v, j, i);
+                    }
+                }
                 if (__any_sync(0xFFFFFFFFu, push)) pushed_mask |= 1u << i;
             }
-#pragma unroll
-            for (int s = 16; s; s >>= 1) kmin = min(kmin, __shfl_xor_sync(0xFFFFFFFFu, kmin, s));
-            if (lane == 0 && kmin != 0x7FFFFFFF) atomicMin(&c->minkey[i].v, kmin);
+            block_atomic_min(&c->minkey[i].v, kmin);
         }
         block_producer_done(c, &s_prod);
-        // ---- drain the cascade: the warp's kept item first, else the queue
+        // ---- drain the cascade: the warp's kept item first, else the queue;
+        // finished items are counted off in batches (before the warp waits)
         unsigned long long item;
         unsigned long long pkeep = kEmptyItem;
+        unsigned done_pending = 0;
         for (;;) {
             if (pkeep != kEmptyItem) {
                 item = pkeep;
                 pkeep = kEmptyItem;
-            } else if (!tq_take_warp(c, p.q, &ticket, &item)) {
+            } else if (!tq_take_warp_lazy(c, p.q, &ticket, &item, &done_pending)) {
                 break;
             }
             const int i = (int)(item >> 63);
@@ -468,7 +516,7 @@ __global__ void __launch_bounds__(kThreads) k_peel2(Peel2Params p) {
             }
             if (pushed) pushed_mask |= 1u << i;
             __syncwarp();
-            if (lane == 0) tq_finish(c, 1);
+            if (lane == 0) ++done_pending;
         }
         if (lane == 0) {
             for (int i = 0; i < p.ninst; ++i)
@@ -542,12 +590,34 @@ __global__ void k_preleft_cur(uint32_t V, const int32_t* kmax, const int32_t* ro
         cur[v] = kmax[v] >= a ? row0[v] : -1;
 }
 
+// This lane's share of #{entries u of list a[0..n) : cur[u] >= cv}, 128
+// entries per warp step; on kmax-sorted lists (sorted != 0) the count stops
+// after the step whose last entry has cur == -1 (outside C_a: so is every
+// later entry).
+__device__ __forceinline__ int count_at_least(const int32_t* cur, const uint32_t* a, int n, int cv, int sorted) {
+    const unsigned lane = threadIdx.x & 31u;
+    int c = 0;
+    for (int b = 0; b < n; b += 128) {
+        int x[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int e = b + 32 * r + (int)lane;
+            x[r] = e < n ? cur[a[e]] : -1;
+            c += (x[r] >= cv);
+        }
+        if (sorted && b + 128 < n && __shfl_sync(0xFFFFFFFFu, x[3], 31) == -1) break;
+    }
+    return c;
+}
+
 // Counters of v against every neighbour, at v's starting value (vertices
 // with a value below 1 get zero counts: they are never evaluated and no
-// counter includes them).
+// counter includes them).  On kmax-sorted lists (sorted != 0) a list ends at
+// its first neighbour outside C_a: cur holds -1 there and for every later
+// entry, which counts nothing.
 __global__ void k_counters_init(uint32_t V, const uint32_t* out_off, const int32_t* out_len, const uint32_t* out_nbr,
                                 const uint32_t* in_off, const int32_t* in_len, const uint32_t* in_nbr,
-                                const int32_t* cur, int32_t* cnt_out, int32_t* cnt_in) {
+                                const int32_t* cur, int32_t* cnt_out, int32_t* cnt_in, int sorted) {
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -561,12 +631,8 @@ __global__ void k_counters_init(uint32_t V, const uint32_t* out_off, const int32
             }
             continue;
         }
-        uint32_t o = out_off[v];
-        int n = out_len[v];
-        for (int i = lane; i < n; i += 32) co += (cur[out_nbr[o + i]] >= cv);
-        o = in_off[v];
-        n = in_len[v];
-        for (int i = lane; i < n; i += 32) ci += (cur[in_nbr[o + i]] >= cv);
+        co = count_at_least(cur, out_nbr + out_off[v], out_len[v], cv, sorted);
+        ci = count_at_least(cur, in_nbr + in_off[v], in_len[v], cv, sorted);
 #pragma unroll
         for (int s = 16; s; s >>= 1) {
             co += __shfl_xor_sync(0xFFFFFFFFu, co, s);
@@ -579,53 +645,96 @@ __global__ void k_counters_init(uint32_t V, const uint32_t* out_off, const int32
     }
 }
 
-// One histogram pass over the C_j prefixes of a vertex's out-list and
-// in-list together (both lists' loads in flight at once) for the window
-// [lo, hi]; values above hi land in bin hi only on the first window
-// (hi == cap).  Two entries per lane per list per step; on kmax-sorted lists
-// a list stops at its first neighbour outside C_j.  Returns the entries read.
-__device__ __forceinline__ int hist_pass2(const int32_t* cur, const uint32_t* ao, int no, const uint32_t* ai, int ni,
-                                          int lo, int hi, bool first, bool sorted, int* bo, int* bi) {
+// Converged warp: when the warp holds no item of its own yet (*keep ==
+// kNoKeep), it keeps the first request of the lowest requesting lane to
+// evaluate next itself instead of queueing it: the link from a drop to the
+// neighbour's evaluation skips the queue's publish and take.  The kept item
+// counts as outstanding like a queued one.
+constexpr uint32_t kNoKeep = 0xFFFFFFFFu;
+// Requests of a lane: bit r of *req set = u[r] is requested (r < 4); the
+// items stay in registers (no dynamically indexed array).
+__device__ __forceinline__ uint32_t first_requested(unsigned req, const uint32_t u[4]) {
+    return (req & 1u) ? u[0] : (req & 2u) ? u[1] : (req & 4u) ? u[2] : u[3];
+}
+__device__ __forceinline__ void keep_one(EngineCtl* c, uint32_t* keep, unsigned* req, const uint32_t u[4]) {
+    if (*keep != kNoKeep) return;
     const unsigned lane = threadIdx.x & 31u;
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, *req != 0u);
+    if (!m) return;
+    const unsigned src = __ffs(m) - 1;
+    const uint32_t item = __shfl_sync(0xFFFFFFFFu, first_requested(*req, u), src);
+    if (lane == src) *req &= *req - 1u;  // drop the kept request
+    if (lane == 0) atomicAdd(&c->outstanding, 1);
+    *keep = item;
+}
+
+// ---- vectorised list passes of the row kernel ----------------------------
+// A list is read with 16-byte id loads: the list at element offset o of its
+// array, length n, is covered by the virtual indices t in [o & 3, (o & 3) + n)
+// of the 16-byte aligned window starting at o - (o & 3); lane l takes the
+// four ids at t = b + 4 l .. b + 4 l + 3 of the step starting at b (128
+// entries per list and step), so eight neighbour values per lane (both
+// lists) are gathered in flight at once.  The adjacency arrays are 16-byte
+// aligned and padded so that the last window of the last list stays inside.
+__device__ __forceinline__ void load_ids4(const uint32_t* nbr, uint32_t o, int end, int b, bool active, uint32_t u[4]) {
+    const int t0 = b + 4 * (int)(threadIdx.x & 31u);
+    uint4 w = make_uint4(0u, 0u, 0u, 0u);
+    if (active && t0 < end) w = *reinterpret_cast<const uint4*>(nbr + (o - (o & 3u)) + t0);
+    u[0] = w.x;
+    u[1] = w.y;
+    u[2] = w.z;
+    u[3] = w.w;
+}
+
+__device__ __forceinline__ int sel4(const int x[4], int q) { return q == 0 ? x[0] : q == 1 ? x[1] : q == 2 ? x[2] : x[3]; }
+
+// Value of the step's last entry (virtual index last >= b) for the early stop
+// on kmax-sorted lists.
+__device__ __forceinline__ int last_value(const int x[4], int b, int last) {
+    const int r = last - b;
+    return __shfl_sync(0xFFFFFFFFu, sel4(x, r & 3), r >> 2);
+}
+
+// hist_pass2 with 16-byte id loads (same bins, counts and stopping rule).
+__device__ __forceinline__ int hist_pass2v(const int32_t* cur, const uint32_t* onbr, uint32_t oo, int no,
+                                           const uint32_t* inbr, uint32_t io, int ni, int lo, int hi, bool first,
+                                           bool sorted, int* bo, int* bi) {
+    const unsigned lane = threadIdx.x & 31u;
+    const int so = (int)(oo & 3u), si = (int)(io & 3u), endo = so + no, endi = si + ni;
     int to = 0, ti = 0, entries = 0;
     bool doneo = no <= 0, donei = ni <= 0;
-    for (int b = 0; !(doneo && donei); b += 64) {
-        uint32_t eo[2], ei[2];
-        bool vo[2], vi[2];
+    for (int b = 0; !(doneo && donei); b += 128) {
+        uint32_t uo[4], ui[4];
+        load_ids4(onbr, oo, endo, b, !doneo, uo);
+        load_ids4(inbr, io, endi, b, !donei, ui);
+        const int t0 = b + 4 * (int)lane;
+        int co[4], ci[4];
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int e = b + r * 32 + (int)lane;
-            vo[r] = !doneo && e < no;
-            vi[r] = !donei && e < ni;
-            eo[r] = vo[r] ? ao[e] : 0u;
-            ei[r] = vi[r] ? ai[e] : 0u;
-        }
-        int co[2], ci[2];
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            co[r] = vo[r] ? ld_vol(&cur[eo[r]]) : -1;
-            ci[r] = vi[r] ? ld_vol(&cur[ei[r]]) : -1;
+        for (int q = 0; q < 4; ++q) {
+            const int t = t0 + q;
+            co[q] = (!doneo && t >= so && t < endo) ? ld_vol(&cur[uo[q]]) : -1;
+            ci[q] = (!donei && t >= si && t < endi) ? ld_vol(&cur[ui[q]]) : -1;
         }
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            int x = co[r];
+        for (int q = 0; q < 4; ++q) {
+            int x = co[q];
             to += first ? (x >= hi) : (x == hi);
             if (x >= lo && x < hi) atomicAdd(&bo[x - lo], 1);
-            x = ci[r];
+            x = ci[q];
             ti += first ? (x >= hi) : (x == hi);
             if (x >= lo && x < hi) atomicAdd(&bi[x - lo], 1);
         }
-        // a list ends at its length, or (sorted by neighbour kmax) at the
-        // first neighbour outside C_j
-        const int lasto = __shfl_sync(0xFFFFFFFFu, co[1], 31);
-        const int lasti = __shfl_sync(0xFFFFFFFFu, ci[1], 31);
         if (!doneo) {
-            entries += min(64, no - b);
-            if (b + 64 >= no || (sorted && lasto == -1)) doneo = true;
+            const int last = min(b + 127, endo - 1);
+            entries += last + 1 - max(b, so);
+            const int lv = last_value(co, b, last);
+            if (b + 128 >= endo || (sorted && lv == -1)) doneo = true;
         }
         if (!donei) {
-            entries += min(64, ni - b);
-            if (b + 64 >= ni || (sorted && lasti == -1)) donei = true;
+            const int last = min(b + 127, endi - 1);
+            entries += last + 1 - max(b, si);
+            const int lv = last_value(ci, b, last);
+            if (b + 128 >= endi || (sorted && lv == -1)) donei = true;
         }
     }
 #pragma unroll
@@ -640,82 +749,100 @@ __device__ __forceinline__ int hist_pass2(const int32_t* cur, const uint32_t* ao
     return entries;
 }
 
-// Converged warp: when the warp holds no item of its own yet (*keep ==
-// kNoKeep), it keeps the first request of the lowest requesting lane to
-// evaluate next itself instead of queueing it: the link from a drop to the
-// neighbour's evaluation skips the queue's publish and take.  The kept item
-// counts as outstanding like a queued one.
-constexpr uint32_t kNoKeep = 0xFFFFFFFFu;
-__device__ __forceinline__ void keep_one(EngineCtl* c, uint32_t* keep, unsigned* nreq, uint32_t* req) {
-    if (*keep != kNoKeep) return;
+// Converged warp: each lane pushes items_a[r] for bits r of ma and items_b[r]
+// for bits r of mb (r < 4), one reservation for the warp.
+__device__ __forceinline__ void tq_push_warp_mask8(EngineCtl* c, TicketQueue q, unsigned ma, const uint32_t items_a[4],
+                                                   unsigned mb, const uint32_t items_b[4]) {
     const unsigned lane = threadIdx.x & 31u;
-    const unsigned m = __ballot_sync(0xFFFFFFFFu, *nreq > 0);
-    if (!m) return;
-    const unsigned src = __ffs(m) - 1;
-    const uint32_t item = __shfl_sync(0xFFFFFFFFu, req[0], src);
-    if (lane == src) {
-        for (unsigned i = 1; i < 4; ++i)
-            if (i < *nreq) req[i - 1] = req[i];
-        --*nreq;
+    const unsigned cnt = __popc(ma) + __popc(mb);
+    unsigned x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (unsigned)o) x += y;
     }
-    if (lane == 0) atomicAdd(&c->outstanding, 1);
-    *keep = item;
+    const unsigned total = __shfl_sync(0xFFFFFFFFu, x, 31);
+    if (total == 0) return;
+    unsigned base = 0;
+    if (lane == 0) {
+        atomicAdd(&c->outstanding, (int)total);
+        base = atomicAdd(&c->t_tail, total);
+    }
+    base = __shfl_sync(0xFFFFFFFFu, base, 0) + (x - cnt);
+    if (cnt) __threadfence();
+#pragma unroll
+    for (unsigned r = 0; r < 4; ++r)
+        if (ma & (1u << r)) *(volatile unsigned long long*)&q.slots[(base + __popc(ma & ((1u << r) - 1u))) & q.mask] =
+            (unsigned long long)items_a[r];
+    base += __popc(ma);
+#pragma unroll
+    for (unsigned r = 0; r < 4; ++r)
+        if (mb & (1u << r)) *(volatile unsigned long long*)&q.slots[(base + __popc(mb & ((1u << r) - 1u))) & q.mask] =
+            (unsigned long long)items_b[r];
 }
 
-// After x dropped from cap to nv (value already written): counts the
-// neighbours of one list with value >= nv into *cnt (this lane's share) and
-// takes x's support away from neighbours whose level lies in (nv, cap]:
-// out-neighbours lose one unit of cnt_in (unstable below j), in-neighbours
-// one unit of cnt_out (unstable below their own value).  Four entries per
-// lane per step; stops like hist_pass2 on kmax-sorted lists.  Returns the
-// entries read.
-__device__ __forceinline__ int recount_pass(const Trans2Params& p, EngineCtl* c, const uint32_t* a, int n, int nv,
-                                            int cap, int j, bool out_list, int* cnt, uint32_t* keep) {
+// recount_pass over both lists at once with 16-byte id loads: counts the
+// neighbours with value >= nv into *cnt_o / *cnt_i (this lane's share) and
+// takes x's support away from the neighbours whose level lies in (nv, cap]
+// (out-neighbours lose a unit of cnt_in, in-neighbours one of cnt_out); a
+// step's counter decrements are all issued before any result is used.
+// Stops like hist_pass2v.  Returns the entries read.
+__device__ __forceinline__ int recount_pass2v(const Trans2Params& p, EngineCtl* c, uint32_t oo, int no, uint32_t io,
+                                              int ni, int nv, int cap, int j, int* cnt_o, int* cnt_i,
+                                              uint32_t* keep) {
     const unsigned lane = threadIdx.x & 31u;
-    int b = 0;
-    for (; b < n; b += 128) {
-        uint32_t u[4];
-        int cu[4];
+    const int so = (int)(oo & 3u), si = (int)(io & 3u), endo = so + no, endi = si + ni;
+    int entries = 0;
+    bool doneo = no <= 0, donei = ni <= 0;
+    for (int b = 0; !(doneo && donei); b += 128) {
+        uint32_t uo[4], ui[4];
+        load_ids4(p.out_nbr, oo, endo, b, !doneo, uo);
+        load_ids4(p.in_nbr, io, endi, b, !donei, ui);
+        const int t0 = b + 4 * (int)lane;
+        int co[4], ci[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            int e = b + r * 32 + (int)lane;
-            u[r] = e < n ? a[e] : 0u;
+        for (int q = 0; q < 4; ++q) {
+            const int t = t0 + q;
+            co[q] = (!doneo && t >= so && t < endo) ? ld_vol(&p.cur[uo[q]]) : -1;
+            ci[q] = (!donei && t >= si && t < endi) ? ld_vol(&p.cur[ui[q]]) : -1;
         }
+        int oldo[4], oldi[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            int e = b + r * 32 + (int)lane;
-            cu[r] = e < n ? ld_vol(&p.cur[u[r]]) : -1;
+        for (int q = 0; q < 4; ++q) {
+            *cnt_o += (co[q] >= nv);
+            *cnt_i += (ci[q] >= nv);
+            oldo[q] = (co[q] > nv && co[q] <= cap) ? atomicSub(&p.cnt_in[uo[q]], 1) : 0x7FFFFFFF;
+            oldi[q] = (ci[q] > nv && ci[q] <= cap) ? atomicSub(&p.cnt_out[ui[q]], 1) : 0x7FFFFFFF;
         }
-        uint32_t req[4];
-        unsigned nreq = 0;
+        unsigned ro = 0, ri = 0;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            int x = cu[r];
-            *cnt += (x >= nv);
-            if (x > nv && x <= cap) {
-                if (out_list) {
-                    int old = atomicSub(&p.cnt_in[u[r]], 1);
-                    if (old - 1 < j && mark_request(&p.mark[u[r]], c)) req[nreq++] = u[r];
-                } else {
-                    int old = atomicSub(&p.cnt_out[u[r]], 1);
-                    if (old - 1 < x && mark_request(&p.mark[u[r]], c)) req[nreq++] = u[r];
-                }
-            }
+        for (int q = 0; q < 4; ++q) {
+            if (oldo[q] != 0x7FFFFFFF && oldo[q] - 1 < j && mark_request(&p.mark[uo[q]], c)) ro |= 1u << q;
+            if (oldi[q] != 0x7FFFFFFF && oldi[q] - 1 < ci[q] && mark_request(&p.mark[ui[q]], c)) ri |= 1u << q;
         }
-        keep_one(c, keep, &nreq, req);
-        tq_push_warp4(c, p.q, nreq, req);
-        int last = min(b + 127, n - 1) - b;
-        int rr = last >> 5;
-        int mine = rr == 0 ? cu[0] : rr == 1 ? cu[1] : rr == 2 ? cu[2] : cu[3];
-        if (p.sorted && __shfl_sync(0xFFFFFFFFu, mine, last & 31) == -1) {
-            b += 128;
-            break;
+        keep_one(c, keep, &ro, uo);
+        keep_one(c, keep, &ri, ui);
+        tq_push_warp_mask8(c, p.q, ro, uo, ri, ui);
+        if (!doneo) {
+            const int last = min(b + 127, endo - 1);
+            entries += last + 1 - max(b, so);
+            const int lv = last_value(co, b, last);
+            if (b + 128 >= endo || (p.sorted && lv == -1)) doneo = true;
+        }
+        if (!donei) {
+            const int last = min(b + 127, endi - 1);
+            entries += last + 1 - max(b, si);
+            const int lv = last_value(ci, b, last);
+            if (b + 128 >= endi || (p.sorted && lv == -1)) donei = true;
         }
     }
-    return min(b, n);
+    return entries;
 }
 
-__global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
+#ifndef DC_TRANS2_MIN_BLOCKS
+#define DC_TRANS2_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(kThreads, DC_TRANS2_MIN_BLOCKS) k_trans2(Trans2Params p) {
     const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const unsigned gwarp = blockIdx.x * kWarpsPerBlock + wib;
     const unsigned nwarps = gridDim.x * kWarpsPerBlock;
@@ -817,14 +944,16 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
         if (lane == 0 && jmin != 0x7FFFFFFF) atomicMin(&c->next_min, jmin);
         block_producer_done(c, &s_prod);
 
-        // ---- drain: the warp's kept item first, else the queue
+        // ---- drain: the warp's kept item first, else the queue; finished
+        // items are counted off in batches (before the warp waits)
         unsigned long long item;
         uint32_t keep = kNoKeep;
+        unsigned done_pending = 0;
         for (;;) {
             if (keep != kNoKeep) {
                 item = keep;
                 keep = kNoKeep;
-            } else if (!tq_take_warp(c, p.q, &ticket, &item)) {
+            } else if (!tq_take_warp_lazy(c, p.q, &ticket, &item, &done_pending)) {
                 break;
             }
             const uint32_t x = (uint32_t)item;
@@ -837,7 +966,7 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
             if (p.kmax[x] < j || cap < 1) {
                 if (lane == 0) {
                     atomicExch(&p.mark[x], 0u);
-                    tq_finish(c, 1);
+                    ++done_pending;
                 }
                 continue;
             }
@@ -859,8 +988,8 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
                 hi_[lane] = 0;
                 hi_[lane + 32] = 0;
                 __syncwarp();
-                my_entries += hist_pass2(p.cur, p.out_nbr + oo, p.out_len[x], p.in_nbr + io, p.in_len[x], lo, hi, first,
-                                         p.sorted != 0, ho, hi_);
+                my_entries += hist_pass2v(p.cur, p.out_nbr, oo, p.out_len[x], p.in_nbr, io, p.in_len[x], lo, hi, first,
+                                          p.sorted != 0, ho, hi_);
                 __syncwarp();
                 int b0 = 2 * lane, b1 = 2 * lane + 1;
                 int o0 = ho[b0], o1 = ho[b1], i0 = hi_[b0], i1 = hi_[b1];
@@ -945,8 +1074,7 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
                 c_o = 0;
                 c_i = 0;
                 // out-neighbours z hold x in cnt_in; in-neighbours y hold x in cnt_out
-                my_entries += recount_pass(p, c, p.out_nbr + oo, p.out_len[x], nv, cap, j, true, &c_o, &keep);
-                my_entries += recount_pass(p, c, p.in_nbr + io, p.in_len[x], nv, cap, j, false, &c_i, &keep);
+                my_entries += recount_pass2v(p, c, oo, p.out_len[x], io, p.in_len[x], nv, cap, j, &c_o, &c_i, &keep);
 #pragma unroll
                 for (int s = 16; s; s >>= 1) {
                     c_o += __shfl_xor_sync(0xFFFFFFFFu, c_o, s);
@@ -971,7 +1099,7 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
                 }
             }
             tq_push_warp(c, p.q, requeue, x);
-            if (lane == 0) tq_finish(c, 1);
+            if (lane == 0) ++done_pending;
         }
         jprev = j;
         seed_out = false;
@@ -993,18 +1121,26 @@ __global__ void __launch_bounds__(kThreads) k_trans2(Trans2Params p) {
 // bitonic sort of (kmax, id) pairs in shared memory.  Long lists: one block,
 // counting sort by kmax through a scratch copy of the list.
 static constexpr int kSortShort = 32;
+static constexpr int kSortWarp = 256;
 static constexpr int kSortMid = 4096;
 
+// Lists of at most kSortShort entries are sorted here, one thread each;
+// longer ones are listed for the warp sort (up to kSortWarp), the block
+// sort (up to kSortMid) or the counting sort.
 __global__ void k_sort_short(uint32_t V, const uint32_t* off, const int32_t* len, uint32_t* nbr, const int32_t* kmax,
-                             uint32_t* mid_list, unsigned* mid_cnt, uint32_t* big_list, unsigned* big_cnt) {
+                             uint32_t* warp_list, uint32_t* mid_list, uint32_t* big_list, unsigned* cnt) {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
         int n = len[v];
         if (n > kSortMid) {
-            big_list[atomicAdd(big_cnt, 1u)] = (uint32_t)v;
+            big_list[atomicAdd(&cnt[2], 1u)] = (uint32_t)v;
+            continue;
+        }
+        if (n > kSortWarp) {
+            mid_list[atomicAdd(&cnt[1], 1u)] = (uint32_t)v;
             continue;
         }
         if (n > kSortShort) {
-            mid_list[atomicAdd(mid_cnt, 1u)] = (uint32_t)v;
+            warp_list[atomicAdd(&cnt[0], 1u)] = (uint32_t)v;
             continue;
         }
         if (n < 2) continue;
@@ -1031,42 +1167,107 @@ __global__ void k_sort_short(uint32_t V, const uint32_t* off, const int32_t* len
     }
 }
 
-__global__ void k_sort_mid(const uint32_t* off, const int32_t* len, uint32_t* nbr, const int32_t* kmax,
-                           const uint32_t* list, unsigned n_list) {
-    __shared__ unsigned long long sh[kSortMid];
-    for (unsigned li = blockIdx.x; li < n_list; li += gridDim.x) {
-        uint32_t v = list[li];
-        int n = len[v];
+// One warp per list of kSortShort+1 .. kSortWarp entries: the list and its
+// neighbours' kmax go to the warp's shared buffer, every entry's place is its
+// rank (entries with a larger kmax, or an equal kmax and a smaller index, go
+// before it), and the entries are written back at their places.  The list
+// count is read on the device (no host round trip).
+constexpr int kSortWarpThreads = 256;
+// Lane-strided entries i = lane + 32 t, t < T: rank among the n staged
+// entries, written to a[rank].  Staged keys are (kmax << 8) | (255 - index),
+// all distinct, so the rank (kmax descending, index ascending on ties) is the
+// number of larger keys.
+template <int T>
+__device__ __forceinline__ void warp_rank_place(const uint32_t* ids, const uint32_t* ks, int n, uint32_t* a) {
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t mk[T];
+    int rank[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        const int i = (int)lane + 32 * t;
+        mk[t] = i < n ? ks[i] : 0xFFFFFFFFu;
+        rank[t] = 0;
+    }
+    for (int j = 0; j < n; ++j) {
+        const uint32_t kj = ks[j];
+#pragma unroll
+        for (int t = 0; t < T; ++t) rank[t] += kj > mk[t];
+    }
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        const int i = (int)lane + 32 * t;
+        if (i < n) a[rank[t]] = ids[i];
+    }
+}
+__global__ void __launch_bounds__(kSortWarpThreads) k_sort_warp(const uint32_t* off, const int32_t* len,
+                                                                 uint32_t* nbr, const int32_t* kmax,
+                                                                 const uint32_t* list, const unsigned* n_list) {
+    constexpr int kW = kSortWarpThreads / 32;
+    static_assert(kSortWarp <= 256, "index part of the staged keys is 8 bits");
+    __shared__ uint32_t s_id[kW][kSortWarp];
+    __shared__ uint32_t s_k[kW][kSortWarp];
+    const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const unsigned nl = *n_list;
+    for (unsigned li = blockIdx.x * kW + w; li < nl; li += gridDim.x * kW) {
+        const uint32_t v = list[li];
+        const int n = len[v];
         uint32_t* a = nbr + off[v];
-        int p2 = 1;
-        while (p2 < n) p2 <<= 1;
-        for (int i = threadIdx.x; i < p2; i += blockDim.x) {
-            if (i < n) {
-                uint32_t u = a[i];
-                // ascending order of (~kmax) gives kmax descending
-                sh[i] = ((unsigned long long)(0x7FFFFFFF - kmax[u]) << 32) | u;
-            } else {
-                sh[i] = ~0ull;
-            }
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t u = a[i];
+            s_id[w][i] = u;
+            s_k[w][i] = ((uint32_t)kmax[u] << 8) | (uint32_t)(255 - i);
+        }
+        __syncwarp();
+        switch ((n + 31) >> 5) {  // chunks of 32 entries (uniform over the warp)
+            case 1: warp_rank_place<1>(s_id[w], s_k[w], n, a); break;
+            case 2: warp_rank_place<2>(s_id[w], s_k[w], n, a); break;
+            case 3: warp_rank_place<3>(s_id[w], s_k[w], n, a); break;
+            case 4: warp_rank_place<4>(s_id[w], s_k[w], n, a); break;
+            case 5: warp_rank_place<5>(s_id[w], s_k[w], n, a); break;
+            case 6: warp_rank_place<6>(s_id[w], s_k[w], n, a); break;
+            case 7: warp_rank_place<7>(s_id[w], s_k[w], n, a); break;
+            default: warp_rank_place<8>(s_id[w], s_k[w], n, a); break;
+        }
+        __syncwarp();
+    }
+}
+
+// One block per list of kSortWarp+1 .. kSortMid entries: a counting sort by
+// neighbour kmax in shared memory (K + 1 bins, the list staged in shared
+// memory), written back in place.  Entries of equal kmax keep no particular
+// order; only the kmax order matters to the readers.  Dynamic shared memory:
+// 4 (K + 1) + 8 kSortMid bytes.
+__global__ void k_sort_mid(const uint32_t* off, const int32_t* len, uint32_t* nbr, const int32_t* kmax, int K,
+                           const uint32_t* list, unsigned n_list) {
+    extern __shared__ unsigned s_mid[];
+    unsigned* bins = s_mid;                   // K + 1
+    uint32_t* ids = s_mid + (K + 1);          // kSortMid
+    int* ks = (int*)(ids + kSortMid);         // kSortMid
+    for (unsigned li = blockIdx.x; li < n_list; li += gridDim.x) {
+        const uint32_t v = list[li];
+        const int n = len[v];
+        uint32_t* a = nbr + off[v];
+        for (int i = threadIdx.x; i <= K; i += blockDim.x) bins[i] = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t u = a[i];
+            const int k = kmax[u];
+            ids[i] = u;
+            ks[i] = k;
+            atomicAdd(&bins[K - k], 1u);
         }
         __syncthreads();
-        for (int kk = 2; kk <= p2; kk <<= 1) {
-            for (int jj = kk >> 1; jj > 0; jj >>= 1) {
-                for (int i = threadIdx.x; i < p2; i += blockDim.x) {
-                    int ixj = i ^ jj;
-                    if (ixj > i) {
-                        bool up = (i & kk) == 0;
-                        unsigned long long x = sh[i], y = sh[ixj];
-                        if ((x > y) == up) {
-                            sh[i] = y;
-                            sh[ixj] = x;
-                        }
-                    }
-                }
-                __syncthreads();
-            }
+        unsigned long long carry = 0;
+        for (int b0 = 0; b0 <= K; b0 += blockDim.x) {
+            const int b = b0 + threadIdx.x;
+            const unsigned long long x = b <= K ? bins[b] : 0ull;
+            unsigned long long tot;
+            const unsigned long long ex = block_excl_scan64(x, &tot);
+            if (b <= K) bins[b] = (unsigned)(ex + carry);
+            carry += tot;
+            __syncthreads();
         }
-        for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = (uint32_t)sh[i];
+        for (int i = threadIdx.x; i < n; i += blockDim.x) a[atomicAdd(&bins[K - ks[i]], 1u)] = ids[i];
         __syncthreads();
     }
 }
@@ -1541,7 +1742,11 @@ static int finish_build(dc_graph* h, uint32_t V, uint64_t E, const uint32_t* d_s
             return set_error(DC_ERR_CAPACITY, "adjacency with slack exceeds 2^32 entries (u32 offsets)");
         uint32_t** off = side == 0 ? &g.out_off : &g.in_off;
         uint32_t** nbr = side == 0 ? &g.out_nbr : &g.in_nbr;
-        if (dmalloc(h->stream, off, (uint64_t)V + 1) || dmalloc(h->stream, nbr, total)) return DC_ERR_NOMEM;
+        // four spare entries: the row kernel's 16-byte id loads read whole
+        // aligned windows, the last one may reach past the last list
+        if (dmalloc(h->stream, off, (uint64_t)V + 1) || dmalloc(h->stream, nbr, total + 4)) return DC_ERR_NOMEM;
+        if ((uintptr_t)*nbr & 15u)
+            return set_error(DC_ERR_CUDA, "adjacency array not 16-byte aligned (vector loads need it)");
         ++g_launches;
         k_off_to_u32<<<grid_for(h, (uint64_t)V + 1), kThreads, 0, h->stream>>>(V, (unsigned long long*)s->tmp64, *off);
         if (side == 0) g.out_cap = total;
@@ -1957,19 +2162,25 @@ static int sort_lists_by_kmax(dc_graph* h, int32_t K, int* sorted) {
         uint32_t* nbr = side == 0 ? g.out_nbr : g.in_nbr;
         uint64_t cap = side == 0 ? g.out_cap : g.in_cap;
         unsigned* cnt = s->cursor;
-        DC_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), h->stream));
+        DC_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned), h->stream));
         ++g_launches;
-        k_sort_short<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, off, len, nbr, h->d.kmax_v, s->rem0, &cnt[0],
-                                                                  s->rem1, &cnt[1]);
-        unsigned hc[2] = {0, 0};
+        k_sort_short<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, off, len, nbr, h->d.kmax_v, s->rem0, s->rem2,
+                                                                  s->rem1, cnt);
+        // most lists go to the warp sort, which reads its count on the device
+        ++g_launches;
+        k_sort_warp<<<h->geom.sms * 8, kSortWarpThreads, 0, h->stream>>>(off, len, nbr, h->d.kmax_v, s->rem0, &cnt[0]);
+        unsigned hc[3] = {0, 0, 0};
         DC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, h->stream));
         DC_CUDA(cudaStreamSynchronize(h->stream));
-        if (hc[0]) {
-            int blocks = (int)std::min<unsigned>(hc[0], (unsigned)h->geom.sms * 8);
-            ++g_launches;
-            k_sort_mid<<<blocks, 256, 0, h->stream>>>(off, len, nbr, h->d.kmax_v, s->rem0, hc[0]);
-        }
         if (hc[1]) {
+            const size_t shm = 4ull * (K + 1) + 8ull * kSortMid;
+            static_assert(4ull * kSortBigBins + 8ull * kSortMid <= 227ull * 1024, "mid-list sort shared memory");
+            DC_CUDA(cudaFuncSetAttribute(k_sort_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+            int blocks = (int)std::min<unsigned>(hc[1], (unsigned)h->geom.sms * 8);
+            ++g_launches;
+            k_sort_mid<<<blocks, 256, shm, h->stream>>>(off, len, nbr, h->d.kmax_v, K, s->rem2, hc[1]);
+        }
+        if (hc[2]) {
             uint32_t*& tmp = side == 0 ? s->w_out_nbr : s->w_in_nbr;
             uint64_t& tcap = side == 0 ? s->w_out_cap : s->w_in_cap;
             if (tcap < cap || !tmp) {
@@ -1977,9 +2188,9 @@ static int sort_lists_by_kmax(dc_graph* h, int32_t K, int* sorted) {
                 if (dmalloc(h->stream, &tmp, cap)) return DC_ERR_NOMEM;
                 tcap = cap;
             }
-            int blocks = (int)std::min<unsigned>(hc[1], (unsigned)h->geom.sms * 2);
+            int blocks = (int)std::min<unsigned>(hc[2], (unsigned)h->geom.sms * 2);
             ++g_launches;
-            k_sort_big<<<blocks, 512, 0, h->stream>>>(off, len, nbr, tmp, h->d.kmax_v, K, s->rem1, hc[1]);
+            k_sort_big<<<blocks, 512, 0, h->stream>>>(off, len, nbr, tmp, h->d.kmax_v, K, s->rem1, hc[2]);
         }
         DC_CUDA(cudaGetLastError());
     }
@@ -2107,7 +2318,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
         k_preleft_cur<<<grid_for(h, V), kThreads, 0, st>>>(V, d.kmax_v, s->row0, a, cur);
         ++g_launches;
         k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, st>>>(
-            V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, cur, co, ci);
+            V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, cur, co, ci, sorted);
         DC_CUDA(cudaMemsetAsync(mark, 0, sizeof(uint32_t) * V, st));
         DC_CUDA(cudaMemsetAsync(stamp, 0xFF, sizeof(int32_t) * V, st));
         return DC_OK;
