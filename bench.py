@@ -280,6 +280,37 @@ def check_parity(g, res, chunk=32):
             "rows_checked": K + 1, "values_checked": int((K + 1) * len(res["kmaxes"]) + len(res["kmaxes"]))}
 
 
+def check_against_oracle(g, V, s, d, chunk=32):
+    """kmax, lmax, every kmax value and every row of the engine's current
+    decomposition against the oracle's decomposition of the edge list
+    (s, d), computed a chunk of rows at a time so that large graphs fit in
+    host memory (checkDCore's criterion, main.cu:276-293).  Raises on any
+    difference."""
+    from oracle import oracle
+    t0 = time.perf_counter()
+    og = oracle.BuiltGraph(V, s, d)
+    K, okmaxes = og.kmax()
+    info = g.decomp_info()
+    if info["kmax"] != K:
+        raise RuntimeError(f"parity: kmax {info['kmax']} != oracle {K}")
+    if not np.array_equal(g.kmaxes(), okmaxes):
+        raise RuntimeError("parity: kmax values differ from the oracle")
+    lmax = 0
+    buf = None
+    for k0 in range(0, K + 1, chunk):
+        k1 = min(K + 1, k0 + chunk)
+        want = og.rows(okmaxes, k0, k1, out=buf)
+        buf = want.base if want.base is not None else want
+        lmax = max(lmax, int(want.max()) if want.size else 0)
+        if not np.array_equal(g.rows(k0, k1 - k0), want):
+            raise RuntimeError(f"parity: rows {k0}..{k1 - 1} differ from the oracle")
+    og.close()
+    if info["lmax"] != lmax:
+        raise RuntimeError(f"parity: lmax {info['lmax']} != oracle {lmax}")
+    return {"vs": "oracle (CPU restatement, oracle/dcore_oracle.c)", "exact": True, "kmax": K,
+            "rows_checked": K + 1, "values_checked": int((K + 2) * V), "oracle_s": time.perf_counter() - t0}
+
+
 def run_reference(args, w, rank, world):
     """The reference arm: the oracle's CPU restatement of the reference's
     decomposition (the reference has no CPU implementation of the path) on
@@ -409,6 +440,13 @@ def run_maintenance(args, w, rank, world, local):
                              "rows_repaired_in_place": local_rows}
     clocks = sampler.stop()
     launches = dc.launch_count() - launches0
+    parity = None
+    if rank == 0 and not args.no_oracle:
+        # the maintained decomposition after the whole stream against the
+        # oracle's decomposition of the final edge set
+        fs, fd = _final_edges(s, d, u[:pos], v[:pos], dl[:pos])
+        parity = check_against_oracle(g, V, fs, fd)
+        parity["after"] = f"{pos} updates in {sum(x['batches'] for x in per_size.values())} batches"
     head = per_size.get("10000") or per_size[max(per_size, key=lambda k: int(k))]
     line = {"metric": METRIC_MAINT, "value": head["updates_per_s"], "unit": "updates/s", "n_gpus": world,
             "steps": sum(x["batches"] for x in per_size.values()), "warmup": 1,
@@ -416,10 +454,9 @@ def run_maintenance(args, w, rank, world, local):
             "dtype": "int32", "data": "synthetic",
             "config": {"workload": args.workload, "graph": w["desc"], "V": V, "E": int(len(s)),
                        "headline": "batches of 10,000 updates", "per_batch_size": per_size,
-                       "exactness": "each batch leaves kmaxes and rows equal to a full recomputation",
                        "method": {0: "scheduler", 1: "local", 2: "re-peel"}[args.maint_method],
                        "row_repair": bool(args.row_repair), "tuning": dict(tuning, source=tune_src)},
-            "gpu_launches": int(launches), "clocks": clocks}
+            "gpu_launches": int(launches), "parity": parity, "clocks": clocks}
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.free()
@@ -528,14 +565,14 @@ def run_serve(args, w, rank, world, local):
     order = np.argsort([len(g[1]) for g in graphs])
     mid = [int(i) for i in order if scales[i] <= 19][-1:]
     checked = []
+    from oracle import oracle
     for i in list(order[:3]) + mid:
         V, s, d, u, v, dl = graphs[i]
         km, rows = srv.result(ids[i], V)
-        fs, fd = _final_edges(s, d, u, v, dl)
-        with dc.Graph.from_edges(V, fs, fd, device=local) as g:
-            g.decompose()
-            if not (np.array_equal(g.kmaxes(), km) and np.array_equal(g.rows(), rows)):
-                raise RuntimeError(f"graph {i}: served result differs from a fresh decomposition")
+        fs, fd = _final_edges(s, d, u[:pos[i]], v[:pos[i]], dl[:pos[i]])
+        okm, olm, okmaxes, orows = oracle.dcore(V, fs, fd)
+        if not (np.array_equal(okmaxes, km) and np.array_equal(orows, rows)):
+            raise RuntimeError(f"graph {i}: served result differs from the oracle's decomposition")
         checked.append(int(i))
     srv.free()
     value = sat_phase["updates_per_s"]
@@ -549,7 +586,7 @@ def run_serve(args, w, rank, world, local):
                        "scales": scales.tolist(), "edge_factors": efs.tolist(), "workers": workers,
                        "budget_gb": w["budget_gb"], "method": {0: "scheduler", 1: "local", 2: "re-peel"}[
                            args.maint_method],
-                       "gen_s": t_gen, "admit_s": t_admit, "exact_checked_graphs": checked,
+                       "gen_s": t_gen, "admit_s": t_admit,
                        "step": "one request (submission to completion)",
                        "value": "updates/s of the saturation phase; ms_per_step = p50 latency below capacity"},
             "latency_phase": dict(lat_phase, offered_req_s=phases[0][3], clocks=lat_clocks),
@@ -560,7 +597,10 @@ def run_serve(args, w, rank, world, local):
                     "h2d_bytes_per_step": float(9 * sat_phase["updates"] / sat_phase["requests"]),
                     "d2h_bytes_per_step": 0,
                     "timing": "wall clock through dc_server_submit/drain with host request buffers"},
-            "gpu_launches": sat_phase["gpu_launches"], "clocks": clocks}
+            "gpu_launches": sat_phase["gpu_launches"],
+            "parity": {"vs": "oracle (CPU restatement, oracle/dcore_oracle.c)", "exact": True,
+                       "graphs_checked": checked, "what": "kmax values and every dense row after all requests"},
+            "clocks": clocks}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -647,18 +687,6 @@ def run_row_sharded(args, w, rank, world, local, dist):
     g.free()
 
 
-def _same_decomposition(a, b, chunk=32):
-    """kmaxes and every dense row equal, compared a chunk of rows at a time."""
-    ka, kb = a.decomp_info()["kmax"], b.decomp_info()["kmax"]
-    if ka != kb or not np.array_equal(a.kmaxes(), b.kmaxes()):
-        return False
-    for k0 in range(0, ka + 1, chunk):
-        n = min(chunk, ka + 1 - k0)
-        if not np.array_equal(a.rows(k0, n), b.rows(k0, n)):
-            return False
-    return True
-
-
 def _stream_times(dc, g, u, v, dl, sizes, method):
     pos, ms, methods = 0, [], []
     for bs in sizes:
@@ -736,12 +764,11 @@ def run_sched(args, w, rank, world, local):
     launches = dc.launch_count() - launches0
     clocks = sampler.stop()
     fs, fd = _final_edges(s, d, u, v, dl)
-    with dc.Graph.from_edges(V, fs, fd, device=local) as fresh:
-        fresh.decompose()
-        for name in res:
-            if not _same_decomposition(res[name]["graph"], fresh):
-                raise RuntimeError(f"{name}: maintained result differs from a fresh decomposition")
-            res[name]["graph"].free()
+    parity = {}
+    for name in res:
+        if not args.no_oracle:
+            parity[name] = check_against_oracle(res[name]["graph"], V, fs, fd)
+        res[name]["graph"].free()
     L, Rr = res["learned"], res["rule"]
     updates = int(ev_sizes.sum())
     value = updates / L["wall_s"]
@@ -756,9 +783,8 @@ def run_sched(args, w, rank, world, local):
                                            "fresh seeds",
                                  "batches": int(w["train_batches"]) * len(w["train_scales"]),
                                  "max_batch": w["train_max"],
-                                 "final_loss": float(loss), "seconds": t_train},
-                       "exactness": "both runs end with kmaxes and every row equal to a fresh "
-                                    "decomposition of the final graph"},
+                                 "final_loss": float(loss), "seconds": t_train}},
+            "parity": parity or None,
             "scheduler": {"learned_wall_s": L["wall_s"], "rule_wall_s": Rr["wall_s"],
                           "gain_wall": Rr["wall_s"] / L["wall_s"],
                           "learned_device_ms": L["device_ms"], "rule_device_ms": Rr["device_ms"],

@@ -166,6 +166,37 @@ extern "C" int dc_graph_load(const char* path, int prune, const dc_graph_opts* o
     return dc_graph_create(V, s.size(), s.data(), d.data(), o, out);
 }
 
+extern "C" int dc_graph_load_text_device(const char* path, int prune, const dc_graph_opts* opts, dc_graph** out) {
+    if (!path || !out) return set_error(DC_ERR_INVALID, "dc_graph_load_text_device: null argument");
+    dc_graph* h = nullptr;
+    if (int rc = new_handle(opts, &h)) return rc;
+    uint32_t V = 0;
+    uint64_t E = 0;
+    uint32_t *src = nullptr, *dst = nullptr;
+    int rc = parse_text_graph_device(path, prune, h->stream, h->geom.sms, &V, &E, &src, &dst);
+    if (rc == DC_OK) rc = build_from_device_edges(h, V, E, src, dst);
+    if (src) cudaFreeAsync(src, h->stream);
+    if (dst) cudaFreeAsync(dst, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (rc == DC_OK && e != cudaSuccess) rc = set_error(DC_ERR_CUDA, "graph build: %s", cudaGetErrorString(e));
+    if (rc != DC_OK) {
+        dc_graph_free(h);
+        return rc;
+    }
+    *out = h;
+    return DC_OK;
+}
+
+extern "C" int dc_write_decomp_cpu_device(dc_graph* h, const char* path) {
+    if (!h || !path) return set_error(DC_ERR_INVALID, "null argument");
+    if (!h->d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
+    if (!h->d.full())
+        return set_error(DC_ERR_STATE, "the decomposition holds row 0 and rows %d..%d only (dc_decompose_rows)",
+                         h->d.row_lo, h->d.row_hi);
+    API_CUDA(cudaSetDevice(h->device));
+    return write_decomp_cpu_device(h, path);
+}
+
 extern "C" int dc_set_trace(dc_graph* h, uint32_t max_steps, dc_trace_fn fn, void* user) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");
     if (h->trace_dev) cudaFree(h->trace_dev);

@@ -104,6 +104,12 @@ int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del);
 int kmax_edge_batches_device(dc_graph* h, uint64_t B, const uint32_t* d_from, const uint32_t* d_to,
                              int64_t* d_batch_of, int64_t* n_batches);
 
+// Text graph parsed on the device into device edge arrays allocated on st
+// (dc_parse.cu); .decompCPU formatted on the device.
+int parse_text_graph_device(const char* path, int prune, cudaStream_t st, int sms, uint32_t* V_out, uint64_t* E_out,
+                            uint32_t** d_src_out, uint32_t** d_dst_out);
+int write_decomp_cpu_device(dc_graph* h, const char* path);
+
 // Full decomposition; method 0 = incremental rows, 1 = per-row peel.
 int decompose(dc_graph* h, int method, int materialize_rows);
 // Rows K0..Kstop from row 0 (in the scratch row0) and kmax; corners left in

@@ -158,6 +158,8 @@ SIGNATURES = {
     "dc_set_wait_limit": [vp, ctypes.c_uint64],
     "dc_test_withhold_barrier": [vp, ctypes.c_int32],
     "dc_graph_kmax_edge_batches": [vp, ctypes.c_uint64, vp, vp, vp, ctypes.POINTER(ctypes.c_int64)],
+    "dc_graph_load_text_device": [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(GraphOpts), ctypes.POINTER(vp)],
+    "dc_write_decomp_cpu_device": [vp, ctypes.c_char_p],
     "dc_kmax_noalloc": [ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp, vp, i32p, vp],
     "dc_plan_row_cuts": [i32p, f32p, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, i32p, f32p],
     "dc_launch_count": [u64p],
@@ -390,6 +392,14 @@ class Graph:
         return cls(h.value)
 
     @classmethod
+    def load_text_device(cls, path, prune=True, gap_min=1, gap_div=0, device=-1):
+        """Text graph parsed on the GPU (dc_graph_load_text_device)."""
+        h = vp()
+        o = cls._opts(gap_min, gap_div, device)
+        _check(lib().dc_graph_load_text_device(path.encode(), int(prune), ctypes.byref(o), ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
     def load(cls, path, prune=True, gap_min=1, gap_div=0, device=-1):
         h = vp()
         o = cls._opts(gap_min, gap_div, device)
@@ -604,6 +614,9 @@ class Graph:
         _check(lib().dc_graph_kmax_edge_batches(self._h, int(B), vp(d_from_ptr), vp(d_to_ptr), vp(d_batch_of_ptr),
                                                 ctypes.byref(n)))
         return n.value
+
+    def write_decomp_cpu_device(self, path):
+        _check(lib().dc_write_decomp_cpu_device(self._h, path.encode()))
 
     def set_wait_limit(self, ns):
         """Limit of every bounded device wait (ns; 0 = the 4 s default)."""

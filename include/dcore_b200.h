@@ -135,6 +135,12 @@ int dc_graph_create_device(uint32_t V, uint64_t E, const uint32_t* d_src, const 
  * when present (or `path` itself when it names such a file), else parses the
  * text file (prune as in dc_text_read_edges). */
 int dc_graph_load(const char* path, int prune, const dc_graph_opts* opts, dc_graph** out);
+/* Graph::readFile (src/graph.cpp:146-250) with the parse on the GPU: the
+ * file's bytes are copied to the device once and split into lines, parsed,
+ * compacted and (prune != 0) pruned and renumbered there, then built into
+ * the device CSR/CSC.  Same graph, same errors as dc_text_read_edges +
+ * dc_graph_create (lines of at most 511 bytes). */
+int dc_graph_load_text_device(const char* path, int prune, const dc_graph_opts* opts, dc_graph** out);
 int dc_graph_free(dc_graph* g);
 int dc_graph_info(const dc_graph* g, uint32_t* V, uint64_t* E);
 /* Live in/out degrees (host arrays of V). */
@@ -201,6 +207,10 @@ int dc_get_skyline(dc_graph* g, uint32_t* off, int32_t* ks, int32_t* ls, uint64_
 /* writeDecompFile / writeDecompFileCPU of the current decomposition. */
 int dc_write_decomp(dc_graph* g, const char* path);
 int dc_write_decomp_cpu(dc_graph* g, const char* path);
+/* writeDecompFileCPU (src/utils.h:110-124) with the text formatted on the
+ * GPU from the device skyline and copied to the host once; byte-identical to
+ * dc_write_decomp_cpu. */
+int dc_write_decomp_cpu_device(dc_graph* g, const char* path);
 
 /* ---- maintenance ------------------------------------------------------- */
 

@@ -485,3 +485,64 @@ int or_max_threads(void) {
     return 1;
 #endif
 }
+
+/*
+ * A built graph kept between calls, for checking a large decomposition a few
+ * rows at a time (dense rows of a scale-24 graph do not fit in host memory at
+ * once): or_graph_new builds the CSR/CSC once, or_graph_rows computes rows
+ * k0 .. k1-1 (dcore's per-row pass, main.cu:236-243, rows in parallel) into
+ * out[(k1 - k0) * V] from the given kmax values, or_graph_kmax the kmax
+ * pass.  The rows are those of or_dcore.
+ */
+void* or_graph_new(uint32_t V, uint64_t E, const uint32_t* src, const uint32_t* dst) {
+    or_graph* g = (or_graph*)malloc(sizeof(or_graph));
+    if (!g) return NULL;
+    if (or_graph_build(V, E, src, dst, g) != OR_OK) { free(g); return NULL; }
+    return g;
+}
+
+void or_graph_delete(void* gp) {
+    if (!gp) return;
+    or_graph_free((or_graph*)gp);
+    free(gp);
+}
+
+int32_t or_graph_kmax(void* gp, int32_t* kmaxes) {
+    or_graph* g = (or_graph*)gp;
+    or_scratch s;
+    if (scratch_init(&s, g->V, max_list(g->V, g->in_off)) != OR_OK) { scratch_free(&s); return -2; }
+    int32_t km = g->V ? or_bz_pass(g->V, g->in_off, g->in_nbr, g->out_off, g->out_nbr, NULL, 0, kmaxes, &s) : 0;
+    scratch_free(&s);
+    return km;
+}
+
+int or_graph_rows(void* gp, int threads, const int32_t* kmaxes, int32_t k0, int32_t k1, int32_t* out) {
+    or_graph* g = (or_graph*)gp;
+    const uint32_t V = g->V;
+    uint64_t mo = max_list(V, g->out_off);
+    int nt = threads;
+#ifdef _OPENMP
+    if (nt <= 0) nt = omp_get_max_threads();
+#else
+    nt = 1;
+#endif
+    if (k1 <= k0) return OR_OK;
+    if (nt > k1 - k0) nt = k1 - k0;
+    int failed = 0;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nt) reduction(| : failed)
+#endif
+    {
+        or_scratch s;
+        if (scratch_init(&s, V, mo) != OR_OK) failed = 1;
+        else {
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+            for (int32_t k = k0; k < k1; ++k)
+                or_bz_pass(V, g->out_off, g->out_nbr, g->in_off, g->in_nbr, kmaxes, k, out + (uint64_t)(k - k0) * V, &s);
+        }
+        scratch_free(&s);
+    }
+    return failed ? OR_ERR_NOMEM : OR_OK;
+}

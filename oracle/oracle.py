@@ -123,6 +123,51 @@ def dcore_timed(V, src, dst, threads=0, rows=None):
     return K, lm.value, kmaxes[:V], out, secs.value, nt
 
 
+class BuiltGraph:
+    """The oracle's CSR/CSC of one graph, built once, for checking a large
+    decomposition a chunk of rows at a time (or_graph_new / or_graph_rows)."""
+
+    def __init__(self, V, src, dst):
+        L = lib()
+        L.or_graph_new.argtypes = [ctypes.c_uint32, ctypes.c_uint64, u32p, u32p]
+        L.or_graph_new.restype = ctypes.c_void_p
+        L.or_graph_delete.argtypes = [ctypes.c_void_p]
+        L.or_graph_delete.restype = None
+        L.or_graph_kmax.argtypes = [ctypes.c_void_p, i32p]
+        L.or_graph_kmax.restype = ctypes.c_int32
+        L.or_graph_rows.argtypes = [ctypes.c_void_p, ctypes.c_int, i32p, ctypes.c_int32, ctypes.c_int32, i32p]
+        L.or_graph_rows.restype = ctypes.c_int
+        src, dst = _u32(src), _u32(dst)
+        self.V = V
+        self._g = L.or_graph_new(V, len(src), _ptr(src, u32p), _ptr(dst, u32p))
+        if not self._g:
+            raise RuntimeError("oracle or_graph_new failed")
+
+    def kmax(self):
+        out = np.empty(max(self.V, 1), np.int32)
+        km = lib().or_graph_kmax(self._g, _ptr(out, i32p))
+        return km, out[:self.V]
+
+    def rows(self, kmaxes, k0, k1, threads=0, out=None):
+        """Rows k0..k1-1 as an array [(k1 - k0), V]."""
+        kmaxes = np.ascontiguousarray(kmaxes, np.int32)
+        n = max(k1 - k0, 0)
+        if out is None or out.size < n * max(self.V, 1):
+            out = np.empty(n * max(self.V, 1), np.int32)
+        rc = lib().or_graph_rows(self._g, threads, _ptr(kmaxes, i32p), k0, k1, out.ctypes.data_as(i32p))
+        if rc:
+            raise RuntimeError(f"oracle or_graph_rows failed: {rc}")
+        return out[:n * max(self.V, 1)].reshape(n, max(self.V, 1))[:, :self.V]
+
+    def close(self):
+        if self._g:
+            lib().or_graph_delete(self._g)
+            self._g = None
+
+    def __del__(self):
+        self.close()
+
+
 def kmax(V, src, dst):
     src, dst = _u32(src), _u32(dst)
     out = np.empty(max(V, 1), np.int32)
