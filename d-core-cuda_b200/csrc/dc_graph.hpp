@@ -35,6 +35,10 @@ struct DevGraph {
     int32_t* in_len = nullptr;
     uint32_t* in_nbr = nullptr;
     uint64_t out_cap = 0, in_cap = 0;
+    // allocations behind out_nbr / in_nbr (the lists start at the first
+    // 16-byte boundary inside them: the row kernel reads ids 16 bytes at a time)
+    uint32_t* out_nbr_alloc = nullptr;
+    uint32_t* in_nbr_alloc = nullptr;
     bool sorted_kmax = false;  // lists ordered by neighbour kmax of the current graph
 };
 

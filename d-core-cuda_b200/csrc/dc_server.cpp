@@ -21,6 +21,7 @@
 // No counterpart in the reference (its driver handles one graph,
 // main.cu:1784-2218).
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -221,6 +222,9 @@ void worker(dc_server* s) {
                                    std::make_move_iterator(g.pending.end()));
         g.pending.clear();
         int rc = admit(s, g, lk);
+        if (rc != DC_OK)
+            fprintf(stderr, "dc_server: admitting graph %u failed (%d): %s\n", batch.front().graph, rc,
+                    dc_last_error());
         // one maintenance batch for all coalesced requests
         std::vector<uint32_t> pairs;
         std::vector<uint8_t> del;
@@ -235,6 +239,9 @@ void worker(dc_server* s) {
             grow_charge(s, g, n_ins, lk);
             lk.unlock();
             rc = dc_maintain(g.h, pairs.data(), del.data(), updates, s->method, nullptr);
+            if (rc != DC_OK)  // the worker's error message is thread-local: report it here
+                fprintf(stderr, "dc_server: batch of %llu updates on graph %u failed (%d): %s\n",
+                        (unsigned long long)updates, batch.front().graph, rc, dc_last_error());
             uint64_t bytes = 0, E = 0;
             dc_graph_device_bytes(g.h, &bytes);
             dc_graph_info(g.h, nullptr, &E);
