@@ -566,7 +566,7 @@ struct Trans2Params {
     int preleft;
     int32_t Kstop;  // last row to compute (rows above stay untouched)
     int sorted;     // lists ordered by neighbour kmax, descending
-    const uint32_t* order;
+    const uint32_t* order;  // C_k = order[0 .. ck[k]); nullptr: the graph is relabeled, C_k = ids 0 .. ck[k]-1
     const uint32_t* ck;
     int32_t* cur;
     int32_t* cnt_out;  // #{u in N_out(v) : cur[u] >= cur[v]}  (never above the truth)
@@ -888,7 +888,7 @@ __global__ void __launch_bounds__(kThreads, DC_TRANS2_MIN_BLOCKS) k_trans2(Trans
         // ---- vertices leaving C_j: value -1; neighbours they supported lose one count
         int lmin = 0x7FFFFFFF;  // bound on the next row that can need work (see hook)
         for (uint32_t i = vj + gwarp; i < vprev; i += nwarps) {
-            uint32_t x = p.order[i];
+            uint32_t x = p.order ? p.order[i] : i;
             int a = ld_vol(&p.cur[x]);
             __syncwarp();
             if (lane == 0) {
@@ -948,7 +948,7 @@ __global__ void __launch_bounds__(kThreads, DC_TRANS2_MIN_BLOCKS) k_trans2(Trans
             bool req = false;
             uint32_t v = 0;
             if (i < vj) {
-                v = p.order[i];
+                v = p.order ? p.order[i] : i;
                 const int cv = ld_vol(&p.cur[v]);
                 if (cv >= 1) {
                     int ci = ld_vol(&p.cnt_in[v]);
@@ -1143,11 +1143,25 @@ static constexpr int kSortShort = 32;
 static constexpr int kSortWarp = 256;
 static constexpr int kSortMid = 4096;
 
+// Where the entries of list i come from: the list itself (sorted in place),
+// or, when the relabeled graph is built, list order[i] of the handle's graph
+// with every entry renamed by pos (copy, rename and sort in one pass).
+struct ListSrc {
+    const uint32_t* off;
+    const uint32_t* nbr;
+    const uint32_t* order;  // nullptr: in place
+    const uint32_t* pos;
+};
+__device__ __forceinline__ const uint32_t* src_list(const ListSrc& s, uint32_t i, const uint32_t* own) {
+    return s.order ? s.nbr + s.off[s.order[i]] : own;
+}
+__device__ __forceinline__ uint32_t src_id(const ListSrc& s, uint32_t u) { return s.order ? s.pos[u] : u; }
+
 // Lists of at most kSortShort entries are sorted here, one thread each;
 // longer ones are listed for the warp sort (up to kSortWarp), the block
 // sort (up to kSortMid) or the counting sort.
 __global__ void k_sort_short(uint32_t V, const uint32_t* off, const int32_t* len, uint32_t* nbr, const int32_t* kmax,
-                             uint32_t* warp_list, uint32_t* mid_list, uint32_t* big_list, unsigned* cnt) {
+                             uint32_t* warp_list, uint32_t* mid_list, uint32_t* big_list, unsigned* cnt, ListSrc src) {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
         int n = len[v];
         if (n > kSortMid) {
@@ -1162,12 +1176,16 @@ __global__ void k_sort_short(uint32_t V, const uint32_t* off, const int32_t* len
             warp_list[atomicAdd(&cnt[0], 1u)] = (uint32_t)v;
             continue;
         }
-        if (n < 2) continue;
         uint32_t* a = nbr + off[v];
+        const uint32_t* in = src_list(src, (uint32_t)v, a);
+        if (n < 2) {
+            if (n == 1 && src.order) a[0] = src_id(src, in[0]);
+            continue;
+        }
         uint32_t ids[kSortShort];
         int ks[kSortShort];
         for (int i = 0; i < n; ++i) {
-            ids[i] = a[i];
+            ids[i] = src_id(src, in[i]);
             ks[i] = kmax[ids[i]];
         }
         for (int i = 1; i < n; ++i) {
@@ -1220,7 +1238,8 @@ __device__ __forceinline__ void warp_rank_place(const uint32_t* ids, const uint3
 }
 __global__ void __launch_bounds__(kSortWarpThreads) k_sort_warp(const uint32_t* off, const int32_t* len,
                                                                  uint32_t* nbr, const int32_t* kmax,
-                                                                 const uint32_t* list, const unsigned* n_list) {
+                                                                 const uint32_t* list, const unsigned* n_list,
+                                                                 ListSrc src) {
     constexpr int kW = kSortWarpThreads / 32;
     static_assert(kSortWarp <= 256, "index part of the staged keys is 8 bits");
     __shared__ uint32_t s_id[kW][kSortWarp];
@@ -1231,8 +1250,9 @@ __global__ void __launch_bounds__(kSortWarpThreads) k_sort_warp(const uint32_t* 
         const uint32_t v = list[li];
         const int n = len[v];
         uint32_t* a = nbr + off[v];
+        const uint32_t* in = src_list(src, v, a);
         for (int i = lane; i < n; i += 32) {
-            const uint32_t u = a[i];
+            const uint32_t u = src_id(src, in[i]);
             s_id[w][i] = u;
             s_k[w][i] = ((uint32_t)kmax[u] << 8) | (uint32_t)(255 - i);
         }
@@ -1257,7 +1277,7 @@ __global__ void __launch_bounds__(kSortWarpThreads) k_sort_warp(const uint32_t* 
 // order; only the kmax order matters to the readers.  Dynamic shared memory:
 // 4 (K + 1) + 8 kSortMid bytes.
 __global__ void k_sort_mid(const uint32_t* off, const int32_t* len, uint32_t* nbr, const int32_t* kmax, int K,
-                           const uint32_t* list, unsigned n_list) {
+                           const uint32_t* list, unsigned n_list, ListSrc src) {
     extern __shared__ unsigned s_mid[];
     unsigned* bins = s_mid;                   // K + 1
     uint32_t* ids = s_mid + (K + 1);          // kSortMid
@@ -1266,10 +1286,11 @@ __global__ void k_sort_mid(const uint32_t* off, const int32_t* len, uint32_t* nb
         const uint32_t v = list[li];
         const int n = len[v];
         uint32_t* a = nbr + off[v];
+        const uint32_t* in = src_list(src, v, a);
         for (int i = threadIdx.x; i <= K; i += blockDim.x) bins[i] = 0;
         __syncthreads();
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const uint32_t u = a[i];
+            const uint32_t u = src_id(src, in[i]);
             const int k = kmax[u];
             ids[i] = u;
             ks[i] = k;
@@ -1294,16 +1315,18 @@ __global__ void k_sort_mid(const uint32_t* off, const int32_t* len, uint32_t* nb
 // bins = K + 1 counters in shared memory (K < kSortBigBins)
 static constexpr int kSortBigBins = 11264;
 __global__ void k_sort_big(const uint32_t* off, const int32_t* len, uint32_t* nbr, uint32_t* tmp, const int32_t* kmax,
-                           int K, const uint32_t* list, unsigned n_list) {
+                           int K, const uint32_t* list, unsigned n_list, ListSrc src) {
     __shared__ unsigned bins[kSortBigBins];
     for (unsigned li = blockIdx.x; li < n_list; li += gridDim.x) {
         uint32_t v = list[li];
         const int n = len[v];
         uint32_t* a = nbr + off[v];
-        uint32_t* t = tmp + off[v];
+        // in place: staged through tmp; from a source list: straight into a
+        uint32_t* t = src.order ? a : tmp + off[v];
+        const uint32_t* in = src_list(src, v, a);
         for (int i = threadIdx.x; i <= K; i += blockDim.x) bins[i] = 0;
         __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&bins[K - kmax[a[i]]], 1u);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&bins[K - kmax[src_id(src, in[i])]], 1u);
         __syncthreads();
         // exclusive scan of bins (K+1 values), chunked by blockDim
         unsigned long long carry = 0;
@@ -1317,12 +1340,13 @@ __global__ void k_sort_big(const uint32_t* off, const int32_t* len, uint32_t* nb
             __syncthreads();
         }
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            uint32_t u = a[i];
+            uint32_t u = src_id(src, in[i]);
             unsigned pos = atomicAdd(&bins[K - kmax[u]], 1u);
             t[pos] = u;
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = t[i];
+        if (!src.order)
+            for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = t[i];
         __syncthreads();
     }
 }
@@ -1681,6 +1705,14 @@ void free_scratch(dc_graph* h) {
     dfree(h->stream, s->w_in_nbr);
     dfree(h->stream, s->kmax_old);
     dfree(h->stream, s->row0_old);
+    dfree(h->stream, s->pos);
+    dfree(h->stream, s->kmax_r);
+    dfree(h->stream, s->row0_r);
+    for (int i = 0; i < 2; ++i) {
+        dfree(h->stream, s->r_off[i]);
+        dfree(h->stream, s->r_len[i]);
+        dfree(h->stream, s->r_nbr_alloc[i]);
+    }
     delete s;
     h->scratch = nullptr;
 }
@@ -2169,56 +2201,157 @@ int expand_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* d_dst) {
 // Orders every adjacency list by neighbour kmax, descending.  *sorted = 0
 // when kmax is too large for the long-list counting sort (lists then stay
 // in arbitrary order and evaluations read them whole).
+// Orders every list of one side by neighbour kmax, descending (kmax[u] of
+// each entry u of the graph the lists belong to).  cap = entries the lists'
+// array spans (the long-list sort stages through a scratch copy that size).
+static int sort_side(dc_graph* h, int32_t K, uint32_t V, const uint32_t* off, const int32_t* len, uint32_t* nbr,
+                     uint64_t cap, const int32_t* kmax, int side, ListSrc src) {
+    Scratch* s = h->scratch;
+    unsigned* cnt = s->cursor;
+    DC_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned), h->stream));
+    ++g_launches;
+    k_sort_short<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, off, len, nbr, kmax, s->rem0, s->rem2, s->rem1, cnt,
+                                                              src);
+    // most lists go to the warp sort, which reads its count on the device
+    ++g_launches;
+    k_sort_warp<<<h->geom.sms * 8, kSortWarpThreads, 0, h->stream>>>(off, len, nbr, kmax, s->rem0, &cnt[0], src);
+    unsigned hc[3] = {0, 0, 0};
+    DC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, h->stream));
+    DC_CUDA(cudaStreamSynchronize(h->stream));
+    if (hc[1]) {
+        const size_t shm = 4ull * (K + 1) + 8ull * kSortMid;
+        static_assert(4ull * kSortBigBins + 8ull * kSortMid <= 227ull * 1024, "mid-list sort shared memory");
+        DC_CUDA(cudaFuncSetAttribute(k_sort_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        int blocks = (int)std::min<unsigned>(hc[1], (unsigned)h->geom.sms * 8);
+        ++g_launches;
+        k_sort_mid<<<blocks, 256, shm, h->stream>>>(off, len, nbr, kmax, K, s->rem2, hc[1], src);
+    }
+    if (hc[2]) {
+        uint32_t*& tmp = side == 0 ? s->w_out_nbr : s->w_in_nbr;
+        uint64_t& tcap = side == 0 ? s->w_out_cap : s->w_in_cap;
+        if (!src.order && (tcap < cap || !tmp)) {  // in place: staging copy of the lists' span
+            dfree(h->stream, tmp);
+            if (dmalloc(h->stream, &tmp, cap)) return DC_ERR_NOMEM;
+            tcap = cap;
+        }
+        int blocks = (int)std::min<unsigned>(hc[2], (unsigned)h->geom.sms * 2);
+        ++g_launches;
+        k_sort_big<<<blocks, 512, 0, h->stream>>>(off, len, nbr, tmp, kmax, K, s->rem1, hc[2], src);
+    }
+    DC_CUDA(cudaGetLastError());
+    return DC_OK;
+}
+
+// Orders every adjacency list of the graph by neighbour kmax, descending.
+// *sorted = 0 when kmax is too large for the long-list counting sort (lists
+// then stay in arbitrary order and evaluations read them whole).
 static int sort_lists_by_kmax(dc_graph* h, int32_t K, int* sorted) {
     DevGraph& g = h->g;
-    Scratch* s = h->scratch;
-    const uint32_t V = g.V;
     *sorted = 0;
     if (g.sorted_kmax) {
         *sorted = 1;
         return DC_OK;
     }
     if (K + 1 > kSortBigBins) return DC_OK;
-    for (int side = 0; side < 2; ++side) {
-        const uint32_t* off = side == 0 ? g.out_off : g.in_off;
-        const int32_t* len = side == 0 ? g.out_len : g.in_len;
-        uint32_t* nbr = side == 0 ? g.out_nbr : g.in_nbr;
-        uint64_t cap = side == 0 ? g.out_cap : g.in_cap;
-        unsigned* cnt = s->cursor;
-        DC_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned), h->stream));
-        ++g_launches;
-        k_sort_short<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, off, len, nbr, h->d.kmax_v, s->rem0, s->rem2,
-                                                                  s->rem1, cnt);
-        // most lists go to the warp sort, which reads its count on the device
-        ++g_launches;
-        k_sort_warp<<<h->geom.sms * 8, kSortWarpThreads, 0, h->stream>>>(off, len, nbr, h->d.kmax_v, s->rem0, &cnt[0]);
-        unsigned hc[3] = {0, 0, 0};
-        DC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, h->stream));
-        DC_CUDA(cudaStreamSynchronize(h->stream));
-        if (hc[1]) {
-            const size_t shm = 4ull * (K + 1) + 8ull * kSortMid;
-            static_assert(4ull * kSortBigBins + 8ull * kSortMid <= 227ull * 1024, "mid-list sort shared memory");
-            DC_CUDA(cudaFuncSetAttribute(k_sort_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-            int blocks = (int)std::min<unsigned>(hc[1], (unsigned)h->geom.sms * 8);
-            ++g_launches;
-            k_sort_mid<<<blocks, 256, shm, h->stream>>>(off, len, nbr, h->d.kmax_v, K, s->rem2, hc[1]);
-        }
-        if (hc[2]) {
-            uint32_t*& tmp = side == 0 ? s->w_out_nbr : s->w_in_nbr;
-            uint64_t& tcap = side == 0 ? s->w_out_cap : s->w_in_cap;
-            if (tcap < cap || !tmp) {
-                dfree(h->stream, tmp);
-                if (dmalloc(h->stream, &tmp, cap)) return DC_ERR_NOMEM;
-                tcap = cap;
-            }
-            int blocks = (int)std::min<unsigned>(hc[2], (unsigned)h->geom.sms * 2);
-            ++g_launches;
-            k_sort_big<<<blocks, 512, 0, h->stream>>>(off, len, nbr, tmp, h->d.kmax_v, K, s->rem1, hc[2]);
-        }
-        DC_CUDA(cudaGetLastError());
-    }
+    for (int side = 0; side < 2; ++side)
+        if (int rc = sort_side(h, K, g.V, side == 0 ? g.out_off : g.in_off, side == 0 ? g.out_len : g.in_len,
+                               side == 0 ? g.out_nbr : g.in_nbr, side == 0 ? g.out_cap : g.in_cap, h->d.kmax_v, side,
+                               ListSrc{nullptr, nullptr, nullptr, nullptr}))
+            return rc;
     g.sorted_kmax = true;
     *sorted = 1;
+    return DC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the graph relabeled in kmax order for the row kernel
+// ---------------------------------------------------------------------------
+// New id i = position of a vertex in kmax-descending order (s->order), so
+// C_k = {new ids < |C_k|} is a prefix of the id space: the row kernel's scans
+// of C_k read its state contiguously, and the dense core's state (the
+// vertices of the heavy rows) packs into a small range that stays in the
+// SMs' caches.  Lists hold new ids, ordered by neighbour kmax.
+__global__ void k_relabel_gather(uint32_t V, const uint32_t* order, const int32_t* kmax, const int32_t* row0,
+                                 const int32_t* out_len, const int32_t* in_len, uint32_t* pos, int32_t* kmax_r,
+                                 int32_t* row0_r, int32_t* len_o, int32_t* len_i) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = order[i];
+        pos[v] = (uint32_t)i;
+        kmax_r[i] = kmax[v];
+        row0_r[i] = row0[v];
+        len_o[i] = out_len[v];
+        len_i[i] = in_len[v];
+    }
+}
+
+__global__ void k_len_to_u64e(uint32_t V, const int32_t* len, unsigned long long* out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = (unsigned long long)len[i];
+}
+
+// corner records of the relabeled run back to original ids
+__global__ void k_unlabel_log(uint64_t n, const uint32_t* order, uint32_t* log_v) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        log_v[i] = order[log_v[i]];
+}
+
+// Builds the relabeled graph (s->order must hold the kmax order of the
+// current kmax) with its lists sorted by neighbour kmax, plus kmax and row 0
+// by new id.
+static int build_relabeled(dc_graph* h, int32_t K) {
+    DevGraph& g = h->g;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    const uint64_t n = (uint64_t)V + 1;
+    if (s->r_cap_V < V || !s->pos) {
+        dfree(h->stream, s->pos);
+        dfree(h->stream, s->kmax_r);
+        dfree(h->stream, s->row0_r);
+        for (int i = 0; i < 2; ++i) {
+            dfree(h->stream, s->r_off[i]);
+            dfree(h->stream, s->r_len[i]);
+        }
+        s->r_cap_V = 0;
+        if (dmalloc(h->stream, &s->pos, n) || dmalloc(h->stream, &s->kmax_r, n) || dmalloc(h->stream, &s->row0_r, n) ||
+            dmalloc(h->stream, &s->r_off[0], n) || dmalloc(h->stream, &s->r_off[1], n) ||
+            dmalloc(h->stream, &s->r_len[0], n) || dmalloc(h->stream, &s->r_len[1], n))
+            return DC_ERR_NOMEM;
+        s->r_cap_V = V;
+    }
+    // list arrays: three spare entries in front for the 16-byte alignment of
+    // the array start, four at the end for the last 16-byte id group
+    const uint64_t cap = g.E + 8;
+    if (s->r_cap < cap || !s->r_nbr_alloc[0]) {
+        for (int i = 0; i < 2; ++i) {
+            dfree(h->stream, s->r_nbr_alloc[i]);
+            s->r_nbr[i] = nullptr;
+        }
+        s->r_cap = 0;
+        const uint64_t want = cap + cap / 8;  // headroom for later, larger graphs of the handle
+        for (int i = 0; i < 2; ++i) {
+            if (dmalloc(h->stream, &s->r_nbr_alloc[i], want + 7)) return DC_ERR_NOMEM;
+            s->r_nbr[i] = (uint32_t*)(((uintptr_t)s->r_nbr_alloc[i] + 15u) & ~(uintptr_t)15u);
+        }
+        s->r_cap = want;
+    }
+    ++g_launches;
+    k_relabel_gather<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, s->order, h->d.kmax_v, s->row0, g.out_len,
+                                                                  g.in_len, s->pos, s->kmax_r, s->row0_r, s->r_len[0],
+                                                                  s->r_len[1]);
+    for (int side = 0; side < 2; ++side) {
+        ++g_launches;
+        k_len_to_u64e<<<grid_for(h, V), kThreads, 0, h->stream>>>(V, s->r_len[side], (unsigned long long*)s->tmp64);
+        if (int rc = scan_tmp64(h, V)) return rc;
+        ++g_launches;
+        k_off_to_u32<<<grid_for(h, n), kThreads, 0, h->stream>>>(V, (unsigned long long*)s->tmp64, s->r_off[side]);
+    }
+    // every relabeled list is read from its original list, renamed and
+    // sorted by neighbour kmax in one pass
+    for (int side = 0; side < 2; ++side) {
+        const ListSrc src{side == 0 ? g.out_off : g.in_off, side == 0 ? g.out_nbr : g.in_nbr, s->order, s->pos};
+        if (int rc = sort_side(h, K, V, s->r_off[side], s->r_len[side], s->r_nbr[side], s->r_cap, s->kmax_r, side, src))
+            return rc;
+    }
     return DC_OK;
 }
 
@@ -2328,20 +2461,41 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
         s->log_cap = cap;
     }
     if (nseg == 1) capn[0] = s->log_cap;
-    // adjacency lists ordered by neighbour kmax (kept until the graph changes)
+    // The graph the row kernel reads: where sorting is allowed, the graph
+    // relabeled in kmax order with kmax-sorted lists (C_k a prefix of the
+    // ids); else the handle's own lists (kmax-sorted when they still are from
+    // an earlier run) with C_k listed by `order`.
     int sorted = 0;
-    if (allow_sort || g.sorted_kmax)
+    const bool relabel = allow_sort && K + 1 <= kSortBigBins;
+    const uint32_t *G_out_off = g.out_off, *G_in_off = g.in_off, *G_order = s->order;
+    int32_t *G_out_len = g.out_len, *G_in_len = g.in_len;
+    uint32_t *G_out_nbr = g.out_nbr, *G_in_nbr = g.in_nbr;
+    const int32_t *G_kmax = d.kmax_v, *G_row0 = s->row0;
+    if (relabel) {
+        if (int rc = build_relabeled(h, K)) return rc;
+        sorted = 1;
+        G_out_off = s->r_off[0];
+        G_in_off = s->r_off[1];
+        G_out_len = s->r_len[0];
+        G_in_len = s->r_len[1];
+        G_out_nbr = s->r_nbr[0];
+        G_in_nbr = s->r_nbr[1];
+        G_kmax = s->kmax_r;
+        G_row0 = s->row0_r;
+        G_order = nullptr;
+    } else if (g.sorted_kmax) {
         if (int rc = sort_lists_by_kmax(h, K, &sorted)) return rc;
+    }
     // starting values and counters of a run that starts at row a: row 0
     // inside C_a with the vertices outside already left (for a = 1 those of
     // kmax 0), so the run's first step has no leaving pass
     auto start_state = [&](cudaStream_t st, int32_t a, int32_t* cur, int32_t* co, int32_t* ci, uint32_t* mark,
                            int32_t* stamp) -> int {
         ++g_launches;
-        k_preleft_cur<<<grid_for(h, V), kThreads, 0, st>>>(V, d.kmax_v, s->row0, a, cur);
+        k_preleft_cur<<<grid_for(h, V), kThreads, 0, st>>>(V, G_kmax, G_row0, a, cur);
         ++g_launches;
         k_counters_init<<<grid_for(h, (uint64_t)V * 32), kThreads, 0, st>>>(
-            V, g.out_off, g.out_len, g.out_nbr, g.in_off, g.in_len, g.in_nbr, cur, co, ci, sorted);
+            V, G_out_off, G_out_len, G_out_nbr, G_in_off, G_in_len, G_in_nbr, cur, co, ci, sorted);
         DC_CUDA(cudaMemsetAsync(mark, 0, sizeof(uint32_t) * V, st));
         DC_CUDA(cudaMemsetAsync(stamp, 0xFF, sizeof(int32_t) * V, st));
         return DC_OK;
@@ -2350,15 +2504,15 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     if (int rc = ensure_tring(h, 2ull * V + (uint64_t)h->geom.sms * 64 + 4096)) return rc;
     Trans2Params tp[kMaxRowSegments];
     tp[0].V = V;
-    tp[0].out_off = g.out_off; tp[0].out_len = g.out_len; tp[0].out_nbr = g.out_nbr;
-    tp[0].in_off = g.in_off; tp[0].in_len = g.in_len; tp[0].in_nbr = g.in_nbr;
-    tp[0].kmax = d.kmax_v;
+    tp[0].out_off = G_out_off; tp[0].out_len = G_out_len; tp[0].out_nbr = G_out_nbr;
+    tp[0].in_off = G_in_off; tp[0].in_len = G_in_len; tp[0].in_nbr = G_in_nbr;
+    tp[0].kmax = G_kmax;
     tp[0].K = K;
     tp[0].K0 = k0;
     tp[0].preleft = 1;
     tp[0].Kstop = cut[0];
     tp[0].sorted = sorted;
-    tp[0].order = s->order;
+    tp[0].order = G_order;
     tp[0].ck = s->ck;
     tp[0].cur = s->cur;
     tp[0].cnt_out = s->cnt_out;
@@ -2463,6 +2617,13 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
                 h->seg_void[i - 1] = voids[i];
             }
         }
+        if (relabel)  // corner records back to original ids (the seam check above compares relabeled state)
+            for (int i = 0; i < nseg; ++i)
+                if (nseg_log[i]) {
+                    ++g_launches;
+                    k_unlabel_log<<<grid_for(h, nseg_log[i]), kThreads, 0, h->stream>>>(nseg_log[i], s->order,
+                                                                                       s->log_v + off[i]);
+                }
     }
     cudaEventRecord(h->ev[4], h->stream);
     *nlog_out = nlog;

@@ -67,6 +67,17 @@ struct Scratch {
     int32_t* row0_old = nullptr;  // [V]
     // row segments after the first (rows split over concurrent launches)
     RowSegment seg[kMaxRowSegments - 1];
+    // the graph relabeled in kmax-descending order for the row kernel:
+    // new id = position in `order`; lists of new ids sorted by neighbour kmax
+    uint32_t* pos = nullptr;                    // [V] new id of each vertex
+    int32_t* kmax_r = nullptr;                  // [V] kmax by new id
+    int32_t* row0_r = nullptr;                  // [V] row 0 by new id
+    uint32_t* r_off[2] = {nullptr, nullptr};    // out / in list starts [V+1]
+    int32_t* r_len[2] = {nullptr, nullptr};     // [V]
+    uint32_t* r_nbr_alloc[2] = {nullptr, nullptr};
+    uint32_t* r_nbr[2] = {nullptr, nullptr};    // 16-byte aligned inside r_nbr_alloc
+    uint32_t r_cap_V = 0;
+    uint64_t r_cap = 0;                         // list entries per side
 };
 
 // Allocation / release (all errors reported through set_error, return DC_*).
