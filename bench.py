@@ -427,17 +427,26 @@ def run_maintenance(args, w, rank, world, local):
         lat = []
         methods = []
         local_rows = 0
+        detail = []
         for _ in range(nb):
             st = g.maintain(u[pos:pos + bs], v[pos:pos + bs], dl[pos:pos + bs], args.maint_method)
             lat.append(st["total_ms"])
             methods.append(st["method"])
             local_rows += st["rows_local"]
+            # per batch: ms (apply, kmax/row-0 update, rows), rows recomputed
+            # or repaired, method, store rebuilt
+            detail.append([round(st["total_ms"], 2), round(st["apply_ms"], 2), round(st["core_ms"], 2),
+                           round(st["rows_ms"], 2), st["rows_recomputed"], st["rows_local"], st["method"],
+                           st["rebuilt"]])
             pos += bs
         lat = np.array(lat)
         per_size[str(bs)] = {"batches": nb, "updates_per_s": bs * nb / (lat.sum() / 1000.0),
                              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                              "methods": {"local": methods.count(1), "repeel": methods.count(2)},
-                             "rows_repaired_in_place": local_rows}
+                             "rows_repaired_in_place": local_rows,
+                             "batch_detail": {"fields": ["total_ms", "apply_ms", "core_ms", "rows_ms",
+                                                         "rows_recomputed", "rows_repaired", "method", "rebuilt"],
+                                              "batches": detail}}
     clocks = sampler.stop()
     launches = dc.launch_count() - launches0
     parity = None
@@ -905,7 +914,7 @@ def run_decomposition(args, w, rank, world, local, dist):
         hd[:] = d
         hk = dc.pinned_array(V, np.int32)
         hrows = dc.pinned_array((K + 1) * V, np.int32).reshape(K + 1, V)
-        et = []
+        et, ph = [], []
         for i in range(args.e2e_steps + 1):
             if dist:
                 dist.barrier()
@@ -914,19 +923,26 @@ def run_decomposition(args, w, rank, world, local, dist):
             g2 = dc.Graph.from_edges(V, hs, hd, device=local)
             g2.set_tuning(tuning["peel_blocks_per_sm"], tuning["rows_blocks_per_sm"], tuning["peel_chunk"],
                           tuning["rows_split_permille"])
+            t1 = time.perf_counter()
             k2, _ = g2.decompose(dc.METHOD_INCREMENTAL)
+            t2 = time.perf_counter()
             g2.kmaxes(out=hk)
             g2.rows(0, k2 + 1, out=hrows[:k2 + 1])
+            t3 = time.perf_counter()
             g2.free()
             torch.cuda.synchronize()
+            t4 = time.perf_counter()
             if i > 0:  # first call is a warm-up
-                et.append(time.perf_counter() - t0)
+                et.append(t4 - t0)
+                ph.append([t1 - t0, t2 - t1, t3 - t2, t4 - t3])
         te = torch.tensor([float(np.mean(et))], dtype=torch.float64, device=dev)
         if dist:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         e2e = {"value": world * E / float(te.item()), "unit": "edges/s", "h2d_bytes_per_step": 8 * E,
                "d2h_bytes_per_step": 4 * V * (K + 2), "timing": "wall clock, synchronized, mean of steps",
-               "steps": len(et)}
+               "steps": len(et),
+               "phases_ms": dict(zip(["create_and_upload", "decompose", "download", "free"],
+                                     (1000.0 * np.mean(ph, 0)).round(3).tolist()))}
 
     # ---- oracle: full decomposition on the host cores (CPU baseline) and
     # the parity check of the last timed step and of the e2e output

@@ -1616,10 +1616,13 @@ int check_ctl_on(EngineCtl* ctl, cudaStream_t st, EngineCtl* hc, const char* wha
 
 int init_handle(dc_graph* h) {
     DC_CUDA(cudaGetDevice(&h->device));
-    cudaDeviceProp prop;
-    DC_CUDA(cudaGetDeviceProperties(&prop, h->device));
-    if (!prop.cooperativeLaunch) return set_error(DC_ERR_NO_DEVICE, "device lacks cooperative launch");
-    h->geom.sms = prop.multiProcessorCount;
+    // two attributes, not the whole property set (cudaGetDeviceProperties is
+    // slow, and every handle pays this)
+    int coop = 0, sms = 0;
+    DC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->device));
+    DC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    if (!coop) return set_error(DC_ERR_NO_DEVICE, "device lacks cooperative launch");
+    h->geom.sms = sms;
     h->geom.threads = kThreads;
     DC_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     // Freed blocks stay in the device's default pool for reuse instead of
@@ -1757,6 +1760,8 @@ uint64_t device_footprint(const dc_graph* h) {
         b += 4ull * s->ck_cap + 12 * s->log_cap + 8 * s->tring_cap;
         b += 4 * (s->w_out_cap + s->w_in_cap);
         if (s->kmax_old) b += 8 * n;
+        if (s->pos) b += 4 * 7 * ((uint64_t)s->r_cap_V + 1);     // relabeled graph: ids, kmax, row 0, offsets, lengths
+        if (s->r_nbr_alloc[0]) b += 2 * 4 * (s->r_cap + 7);     // its lists
     }
     return b;
 }
@@ -2360,7 +2365,8 @@ static int build_relabeled(dc_graph* h, int32_t K) {
 // row-to-row kernel.  Corners of rows 1..Kstop are left in the scratch log
 // (*nlog entries).  allow_sort: order adjacency lists by neighbour kmax
 // first (otherwise lists are read whole).
-int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out, int32_t K0) {
+int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out, int32_t K0,
+                   bool allow_relabel) {
     DevGraph& g = h->g;
     Decomp& d = h->d;
     Scratch* s = h->scratch;
@@ -2466,7 +2472,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
     // ids); else the handle's own lists (kmax-sorted when they still are from
     // an earlier run) with C_k listed by `order`.
     int sorted = 0;
-    const bool relabel = allow_sort && K + 1 <= kSortBigBins;
+    const bool relabel = allow_sort && allow_relabel && K + 1 <= kSortBigBins;
     const uint32_t *G_out_off = g.out_off, *G_in_off = g.in_off, *G_order = s->order;
     int32_t *G_out_len = g.out_len, *G_in_len = g.in_len;
     uint32_t *G_out_nbr = g.out_nbr, *G_in_nbr = g.in_nbr;
@@ -2483,7 +2489,7 @@ int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint6
         G_kmax = s->kmax_r;
         G_row0 = s->row0_r;
         G_order = nullptr;
-    } else if (g.sorted_kmax) {
+    } else if (allow_sort || g.sorted_kmax) {
         if (int rc = sort_lists_by_kmax(h, K, &sorted)) return rc;
     }
     // starting values and counters of a run that starts at row a: row 0

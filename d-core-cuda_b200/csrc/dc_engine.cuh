@@ -128,7 +128,11 @@ int decompose(dc_graph* h, int method, int materialize_rows);
 // step is the fixpoint of row K0 below row 0, so the corners it logs at K0
 // are relative to row 0 and rows 1..K0-1 of the resulting skyline are not
 // meaningful.
-int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out, int32_t K0 = 1);
+// allow_relabel: with sorting allowed, run on the graph relabeled in kmax
+// order (whole decompositions and row ranges); else sort the handle's lists
+// in place (maintenance recomputations, whose graph changes every batch).
+int rows_from_row0(dc_graph* h, int32_t K, int32_t Kstop, bool allow_sort, uint64_t* nlog_out, int32_t K0 = 1,
+                   bool allow_relabel = true);
 // kmax and row 0 (fused peel) when k_first <= 0 or not current, then rows
 // max(k_first, 1)..min(k_last, kmax) only; the decomposition then holds row 0
 // and that range.

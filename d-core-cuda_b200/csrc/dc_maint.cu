@@ -1068,7 +1068,7 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
         // ---- rows 0..R from the new row 0, rows above R from the old skyline
         MT_CUDA(cudaMemcpyAsync(s->row0, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
         uint64_t nlog = 0;
-        if ((rc = rows_from_row0(h, Knew, R, R > 48, &nlog))) goto out;
+        if ((rc = rows_from_row0(h, Knew, R, R > 48, &nlog, 1, false))) goto out;
         uint32_t* o_off = d.sky_off;
         int32_t* o_k = d.sky_k;
         int32_t* o_l = d.sky_l;

@@ -105,6 +105,7 @@ uint64_t footprint_bound(uint64_t V, uint64_t E, uint64_t sms) {
     b += 12 * (E + V + 1);
     b += 16 * (2 * V + 2 * cap / 32 + sms * 64 + 4096);
     b += 8 * E + 2 * 4 * cap;
+    b += 4 * 7 * (V + 1) + 2 * 4 * ((E + 8) + (E + 8) / 8 + 7);  // the row kernel's relabeled graph
     return b + (1ull << 20);
 }
 
