@@ -1648,6 +1648,40 @@ void free_graph_arrays(DevGraph& g, cudaStream_t st) {
     g.out_cap = g.in_cap = 0;
 }
 
+int sky_take_spare(dc_graph* h, int slot, uint64_t n, uint32_t** off, int32_t** k, int32_t** l, uint64_t* cap) {
+    Decomp& d = h->d;
+    if (d.spare_cap[slot] < n || !d.spare_k[slot]) {
+        dfree(h->stream, d.spare_k[slot]);
+        dfree(h->stream, d.spare_l[slot]);
+        d.spare_cap[slot] = 0;
+        const uint64_t want = n + n / 4 + 1;
+        if (dmalloc(h->stream, &d.spare_k[slot], want) || dmalloc(h->stream, &d.spare_l[slot], want))
+            return DC_ERR_NOMEM;
+        d.spare_cap[slot] = want;
+    }
+    if (!d.spare_off[slot] && dmalloc(h->stream, &d.spare_off[slot], (uint64_t)h->g.V + 1)) return DC_ERR_NOMEM;
+    *off = d.spare_off[slot];
+    *k = d.spare_k[slot];
+    *l = d.spare_l[slot];
+    *cap = d.spare_cap[slot];
+    d.spare_off[slot] = nullptr;
+    d.spare_k[slot] = nullptr;
+    d.spare_l[slot] = nullptr;
+    d.spare_cap[slot] = 0;
+    return DC_OK;
+}
+
+void sky_put_spare(dc_graph* h, int slot, uint32_t* off, int32_t* k, int32_t* l, uint64_t cap) {
+    Decomp& d = h->d;
+    dfree(h->stream, d.spare_off[slot]);
+    dfree(h->stream, d.spare_k[slot]);
+    dfree(h->stream, d.spare_l[slot]);
+    d.spare_off[slot] = off;
+    d.spare_k[slot] = k;
+    d.spare_l[slot] = l;
+    d.spare_cap[slot] = (k && l) ? cap : 0;
+}
+
 void free_decomp(Decomp& d, cudaStream_t st) {
     dfree(st, d.kmax_v);
     dfree(st, d.row0);
@@ -1655,6 +1689,12 @@ void free_decomp(Decomp& d, cudaStream_t st) {
     dfree(st, d.sky_k);
     dfree(st, d.sky_l);
     dfree(st, d.rows);
+    for (int i = 0; i < 2; ++i) {
+        dfree(st, d.spare_off[i]);
+        dfree(st, d.spare_k[i]);
+        dfree(st, d.spare_l[i]);
+        d.spare_cap[i] = 0;
+    }
     d.rows_cap = 0;
     d.corner_cap = 0;
     d.valid = false;
@@ -1753,6 +1793,7 @@ uint64_t device_footprint(const dc_graph* h) {
     uint64_t b = sizeof(EngineCtl);
     if (g.out_off) b += 2 * 4 * (2 * V1) + 4 * (g.out_cap + g.in_cap);
     if (d.kmax_v) b += 4 * (3 * V1) + 8 * d.corner_cap;
+    for (int i = 0; i < 2; ++i) b += 8 * d.spare_cap[i] + (d.spare_off[i] ? 4 * V1 : 0);
     b += 4 * d.rows_cap;
     if (const Scratch* s = h->scratch) {
         uint64_t n = (uint64_t)s->cap_V + 1;
@@ -2160,11 +2201,14 @@ int build_skyline_from_log(dc_graph* h, uint64_t nlog) {
         k_sky_count<<<grid_for(h, n[r]), kThreads, 0, h->stream>>>(V, n[r], s->log_v + lo[r], s->log_k + lo[r], cnt);
     }
     if (int rc = scan_tmp64(h, V)) return rc;
-    if (d.corner_cap < total) {
+    if (d.corner_cap < total || !d.sky_k) {
+        // a quarter of headroom: maintenance batches rarely grow it again
         dfree(h->stream, d.sky_k);
         dfree(h->stream, d.sky_l);
-        if (dmalloc(h->stream, &d.sky_k, total) || dmalloc(h->stream, &d.sky_l, total)) return DC_ERR_NOMEM;
-        d.corner_cap = total;
+        d.corner_cap = 0;
+        const uint64_t want = total + total / 4 + 1;
+        if (dmalloc(h->stream, &d.sky_k, want) || dmalloc(h->stream, &d.sky_l, want)) return DC_ERR_NOMEM;
+        d.corner_cap = want;
     }
     if (!d.sky_off && dmalloc(h->stream, &d.sky_off, (uint64_t)V + 1)) return DC_ERR_NOMEM;
     ++g_launches;

@@ -164,6 +164,12 @@ int scan_tmp64(dc_graph* h, uint64_t n);
 // row segment ran, [off2, off2 + n2).
 int build_skyline_from_log(dc_graph* h, uint64_t nlog);
 int prepare_row_segments(dc_graph* h);
+// Spare skyline buffers (slot 0 or 1): take hands over the slot's buffers with
+// room for at least n corners and V + 1 offsets (allocated or grown with a
+// quarter of headroom; the slot is left empty); put returns buffers to a slot
+// (freeing what it held).
+int sky_take_spare(dc_graph* h, int slot, uint64_t n, uint32_t** off, int32_t** k, int32_t** l, uint64_t* cap);
+void sky_put_spare(dc_graph* h, int slot, uint32_t* off, int32_t* k, int32_t* l, uint64_t cap);
 // kmax (in-degree peel) and row 0 (out-degree peel) of the current graph into
 // d.kmax_v and the scratch row 0; reports the largest values.
 int peel_kmax_row0(dc_graph* h, int32_t* kmax, int32_t* lmax);

@@ -67,6 +67,12 @@ struct Decomp {
     bool rows_valid = false;
     bool peel_valid = false;  // kmax_v and row0 match the current graph
     int32_t row_lo = 1, row_hi = -1;  // rows held besides row 0 (all: 1..kmax)
+    // spare skyline buffers that maintenance rotates through (a batch's
+    // partial and merged skylines), so steady-state batches allocate nothing
+    uint32_t* spare_off[2] = {nullptr, nullptr};
+    int32_t* spare_k[2] = {nullptr, nullptr};
+    int32_t* spare_l[2] = {nullptr, nullptr};
+    uint64_t spare_cap[2] = {0, 0};
     bool full() const { return valid && row_lo <= 1 && row_hi >= kmax; }
     // every row of [k0, k0 + n) is held (row 0 always is)
     bool holds(uint64_t k0, uint64_t n) const {

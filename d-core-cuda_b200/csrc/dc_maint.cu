@@ -1069,14 +1069,16 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
         MT_CUDA(cudaMemcpyAsync(s->row0, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
         uint64_t nlog = 0;
         if ((rc = rows_from_row0(h, Knew, R, R > 48, &nlog, 1, false))) goto out;
+        // the old skyline stays readable while rows 0..R are assembled in
+        // spare slot 0 and merged into spare slot 1; then the merged one is
+        // current and the other two go back to the slots (no allocation
+        // once the slots have grown to the graph's size)
         uint32_t* o_off = d.sky_off;
         int32_t* o_k = d.sky_k;
         int32_t* o_l = d.sky_l;
-        d.sky_off = nullptr;
-        d.sky_k = nullptr;
-        d.sky_l = nullptr;
-        d.corner_cap = 0;
-        rc = build_skyline_from_log(h, nlog);
+        const uint64_t o_cap = d.corner_cap;
+        if ((rc = sky_take_spare(h, 0, 0, &d.sky_off, &d.sky_k, &d.sky_l, &d.corner_cap)) == DC_OK)
+            rc = build_skyline_from_log(h, nlog);
         if (rc == DC_OK) {
             unsigned long long* cnt = (unsigned long long*)s->tmp64;
             ++g_launches;
@@ -1090,29 +1092,22 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
             }
             uint32_t* m_off = nullptr;
             int32_t *m_k = nullptr, *m_l = nullptr;
-            if (rc == DC_OK && (mt_malloc(h->stream, &m_off, (uint64_t)V + 1) || mt_malloc(h->stream, &m_k, total) || mt_malloc(h->stream, &m_l, total))) {
-                rc = DC_ERR_NOMEM;
-            }
+            uint64_t m_cap = 0;
+            if (rc == DC_OK) rc = sky_take_spare(h, 1, total, &m_off, &m_k, &m_l, &m_cap);
             if (rc == DC_OK) {
                 ++g_launches;
                 k_merge_fill<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, R, d.kmax_v, d.sky_off, d.sky_k, d.sky_l,
                                                                        o_off, o_k, o_l, cnt, m_k, m_l, m_off);
                 cudaStreamSynchronize(h->stream);
-                mt_free(h->stream, d.sky_off);
-                mt_free(h->stream, d.sky_k);
-                mt_free(h->stream, d.sky_l);
+                sky_put_spare(h, 0, d.sky_off, d.sky_k, d.sky_l, d.corner_cap);
                 d.sky_off = m_off;
                 d.sky_k = m_k;
                 d.sky_l = m_l;
-                d.corner_cap = total;
+                d.corner_cap = m_cap;
                 d.n_corners = total;
-            } else {
-                mt_free(h->stream, m_off); mt_free(h->stream, m_k); mt_free(h->stream, m_l);
             }
         }
-        mt_free(h->stream, o_off);
-        mt_free(h->stream, o_k);
-        mt_free(h->stream, o_l);
+        sky_put_spare(h, 1, o_off, o_k, o_l, o_cap);
         if (rc != DC_OK) {
             d.valid = false;
             goto out;

@@ -650,16 +650,13 @@ int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_
     if (hc.error) return DC_OK;  // capacity: the caller recomputes the rows
     const uint64_t nlog = hc.log_count;
     // per-vertex change lists
+    // the change lists go to spare skyline slot 0 and the merged skyline to
+    // slot 1 (no allocation once the slots have grown to the graph's size)
     unsigned long long* cnt = (unsigned long long*)s->tmp64;
     uint32_t *coff = nullptr, *fill = s->cursor, *noff = nullptr;
     int32_t *ck = nullptr, *cl = nullptr, *nk = nullptr, *nl = nullptr;
-    int rc = DC_OK;
-    if (cudaMallocAsync((void**)&coff, 4ull * (V + 1), h->stream) != cudaSuccess ||
-        cudaMallocAsync((void**)&ck, 4ull * (nlog ? nlog : 1), h->stream) != cudaSuccess ||
-        cudaMallocAsync((void**)&cl, 4ull * (nlog ? nlog : 1), h->stream) != cudaSuccess) {
-        cudaGetLastError();
-        rc = set_error(DC_ERR_NOMEM, "row repair: change list allocation failed");
-    }
+    uint64_t ccap = 0, ncap = 0;
+    int rc = sky_take_spare(h, 0, nlog, &coff, &ck, &cl, &ccap);
     unsigned long long total = 0;
     if (rc == DC_OK) {
         cudaMemsetAsync(cnt, 0, 8ull * (V + 1), h->stream);
@@ -685,35 +682,25 @@ int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_
             rc = set_error(DC_ERR_CUDA, "row repair: corner count download failed");
         }
     }
-    if (rc == DC_OK && (cudaMallocAsync((void**)&noff, 4ull * (V + 1), h->stream) != cudaSuccess ||
-                        cudaMallocAsync((void**)&nk, 4ull * (total ? total : 1), h->stream) != cudaSuccess ||
-                        cudaMallocAsync((void**)&nl, 4ull * (total ? total : 1), h->stream) != cudaSuccess)) {
-        cudaGetLastError();
-        rc = set_error(DC_ERR_NOMEM, "row repair: skyline allocation failed");
-    }
+    if (rc == DC_OK) rc = sky_take_spare(h, 1, total, &noff, &nk, &nl, &ncap);
     if (rc == DC_OK) {
         ++g_launches;
         k_rep_merge<true><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
                                                                     coff, ck, cl, cnt, nk, nl, noff);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(DC_ERR_CUDA, "row repair: merge launch failed");
     }
-    cudaFreeAsync(coff, h->stream);
-    cudaFreeAsync(ck, h->stream);
-    cudaFreeAsync(cl, h->stream);
+    if (coff || ck) sky_put_spare(h, 0, coff, ck, cl, ccap);
     if (rc != DC_OK) {
-        if (noff) cudaFreeAsync(noff, h->stream);
-        if (nk) cudaFreeAsync(nk, h->stream);
-        if (nl) cudaFreeAsync(nl, h->stream);
+        if (noff || nk) sky_put_spare(h, 1, noff, nk, nl, ncap);
         return rc;
     }
-    cudaFreeAsync(d.sky_off, h->stream);
-    cudaFreeAsync(d.sky_k, h->stream);
-    cudaFreeAsync(d.sky_l, h->stream);
+    // the old skyline becomes the spare of slot 1
+    sky_put_spare(h, 1, d.sky_off, d.sky_k, d.sky_l, d.corner_cap);
     d.sky_off = noff;
     d.sky_k = nk;
     d.sky_l = nl;
     d.n_corners = total;
-    d.corner_cap = total;
+    d.corner_cap = ncap;
     *applied = true;
     return DC_OK;
 }

@@ -99,7 +99,7 @@ uint64_t footprint_bound(uint64_t V, uint64_t E, uint64_t sms) {
     const uint64_t cap = E + E / 8 + 2 * V + 64;
     uint64_t b = 2 * 4 * cap * 2;
     b += 4 * 4 * (V + 1);
-    b += 4 * 3 * (V + 1) + 2 * (8 * (E + 2 * V) + 4 * (V + 1));
+    b += 4 * 3 * (V + 1) + 3 * (8 * (E + 2 * V) + 4 * (V + 1));  // skyline and its two spares
     b += 4 * 20 * (V + 2) + 8 * (V + 2) + 8 * (sms * 64 + 64);
     b += 8 * (V + sms * 64 * 32 + 64);
     b += 12 * (E + V + 1);
