@@ -2269,8 +2269,12 @@ static int sort_side(dc_graph* h, int32_t K, uint32_t V, const uint32_t* off, co
     DC_CUDA(cudaStreamSynchronize(h->stream));
     if (hc[1]) {
         const size_t shm = 4ull * (K + 1) + 8ull * kSortMid;
-        static_assert(4ull * kSortBigBins + 8ull * kSortMid <= 227ull * 1024, "mid-list sort shared memory");
-        DC_CUDA(cudaFuncSetAttribute(k_sort_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        // the kernel's limit is set to its largest need, the same value on
+        // every call: handles sorting on other threads at the same time
+        // (the serving loop) must never see it lowered below their launch
+        constexpr size_t kMidMax = 4ull * kSortBigBins + 8ull * kSortMid;
+        static_assert(kMidMax <= 227ull * 1024, "mid-list sort shared memory");
+        DC_CUDA(cudaFuncSetAttribute(k_sort_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMidMax));
         int blocks = (int)std::min<unsigned>(hc[1], (unsigned)h->geom.sms * 8);
         ++g_launches;
         k_sort_mid<<<blocks, 256, shm, h->stream>>>(off, len, nbr, kmax, K, s->rem2, hc[1], src);
