@@ -440,7 +440,8 @@ __device__ __forceinline__ bool tq_take_warp(EngineCtl* c, TicketQueue q, unsign
         if (*ticket == kNoTicket) *ticket = atomicAdd(&c->t_head, 1u);
         volatile unsigned long long* s = &q.slots[*ticket & q.mask];
         unsigned long long t0 = 0;
-        unsigned spins = 0;
+        unsigned spins = 0, seen_tail = 0;
+        int seen_out = 0;
         for (;;) {
             it = *s;
             if (it != kEmptyItem) {
@@ -456,12 +457,26 @@ __device__ __forceinline__ bool tq_take_warp(EngineCtl* c, TicketQueue q, unsign
                 state = 2;
                 break;
             }
-            if (++spins == 64) t0 = gtimer();
-            if (spins > 64 && (spins & 63) == 0 && gtimer() - t0 > wait_limit(c)) {
-                set_dev_error(c, DC_DEV_ERR_TIMEOUT, 5);
-                *ticket = kNoTicket;
-                state = 2;
-                break;
+            if (++spins == 64) {
+                t0 = gtimer();
+                seen_tail = ld_vol(&c->t_tail);
+                seen_out = ld_vol(&c->outstanding);
+            }
+            // the limit bounds a wait without progress: while the phase's
+            // other warps still push or finish items the clock restarts
+            if (spins > 64 && (spins & 63) == 0) {
+                const unsigned tl = ld_vol(&c->t_tail);
+                const int ou = ld_vol(&c->outstanding);
+                if (tl != seen_tail || ou != seen_out) {
+                    seen_tail = tl;
+                    seen_out = ou;
+                    t0 = gtimer();
+                } else if (gtimer() - t0 > wait_limit(c)) {
+                    set_dev_error(c, DC_DEV_ERR_TIMEOUT, 5);
+                    *ticket = kNoTicket;
+                    state = 2;
+                    break;
+                }
             }
             if (spins > 16) __nanosleep(spins > 256 ? 256 : 32);
         }
