@@ -1511,6 +1511,45 @@ __global__ void k_sky_sort(uint32_t V, const unsigned long long* off, int32_t* s
 }
 
 // Dense rows [k0, k0+n): rows[(k-k0)*V + v]
+// Four consecutive vertices per thread and one 16-byte streaming store per
+// row (V a multiple of 4, so every row starts 16-byte aligned); the output is
+// far larger than L2, hence the streaming (evict-first) stores.
+__global__ void k_expand4(uint32_t V, uint32_t k0, uint32_t n, const int32_t* kmax, const uint32_t* sky_off,
+                          const int32_t* sky_k, const int32_t* sky_l, int32_t* rows) {
+    const uint32_t V4 = V / 4;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < V4; t += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t ci[4], b[4];
+        int val[4], nextk[4], km[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t v = 4 * (uint32_t)t + q;
+            const uint32_t a = sky_off[v];
+            b[q] = sky_off[v + 1];
+            km[q] = kmax[v];
+            uint32_t c = a;
+            while (c + 1 < b[q] && (uint32_t)sky_k[c + 1] <= k0) ++c;
+            ci[q] = c;
+            val[q] = sky_l[c];
+            nextk[q] = (c + 1 < b[q]) ? sky_k[c + 1] : 0x7FFFFFFF;
+        }
+        int4* out = reinterpret_cast<int4*>(rows) + t;
+        for (uint32_t r = 0; r < n; ++r) {
+            const int k = (int)(k0 + r);
+            int o[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                while (k >= nextk[q]) {
+                    ++ci[q];
+                    val[q] = sky_l[ci[q]];
+                    nextk[q] = (ci[q] + 1 < b[q]) ? sky_k[ci[q] + 1] : 0x7FFFFFFF;
+                }
+                o[q] = (k <= km[q]) ? val[q] : 0;
+            }
+            __stcs(out + (uint64_t)r * V4, make_int4(o[0], o[1], o[2], o[3]));
+        }
+    }
+}
+
 __global__ void k_expand(uint32_t V, uint32_t k0, uint32_t n, const int32_t* kmax, const uint32_t* sky_off,
                          const int32_t* sky_k, const int32_t* sky_l, int32_t* rows) {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
@@ -2241,8 +2280,12 @@ int expand_rows(dc_graph* h, uint32_t k0, uint32_t n, int32_t* d_dst) {
     if (!d.valid) return set_error(DC_ERR_STATE, "no decomposition on this graph");
     if (n == 0) return DC_OK;
     ++g_launches;
-    k_expand<<<grid_for(h, h->g.V), kThreads, 0, h->stream>>>(h->g.V, k0, n, d.kmax_v, d.sky_off, d.sky_k, d.sky_l,
-                                                               d_dst);
+    if (h->g.V % 4 == 0 && ((uintptr_t)d_dst & 15u) == 0)
+        k_expand4<<<grid_for(h, h->g.V / 4), kThreads, 0, h->stream>>>(h->g.V, k0, n, d.kmax_v, d.sky_off, d.sky_k,
+                                                                         d.sky_l, d_dst);
+    else
+        k_expand<<<grid_for(h, h->g.V), kThreads, 0, h->stream>>>(h->g.V, k0, n, d.kmax_v, d.sky_off, d.sky_k,
+                                                                   d.sky_l, d_dst);
     DC_CUDA(cudaGetLastError());
     return DC_OK;
 }
