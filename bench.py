@@ -427,25 +427,29 @@ def run_maintenance(args, w, rank, world, local):
         lat = []
         methods = []
         local_rows = 0
+        local_ins = 0
         detail = []
         for _ in range(nb):
             st = g.maintain(u[pos:pos + bs], v[pos:pos + bs], dl[pos:pos + bs], args.maint_method)
             lat.append(st["total_ms"])
             methods.append(st["method"])
-            local_rows += st["rows_local"]
+            local_rows += st["rows_local"] & 1
+            local_ins += (st["rows_local"] >> 1) & 1
             # per batch: ms (apply, kmax/row-0 update, rows), rows recomputed
             # or repaired, method, store rebuilt
             detail.append([round(st["total_ms"], 2), round(st["apply_ms"], 2), round(st["core_ms"], 2),
                            round(st["rows_ms"], 2), st["rows_recomputed"], st["rows_local"], st["method"],
-                           st["rebuilt"]])
+                           st["rebuilt"], round(st["del_repair_ms"], 2), round(st["ins_repair_ms"], 2),
+                           st["ins_scanned"]])
             pos += bs
         lat = np.array(lat)
         per_size[str(bs)] = {"batches": nb, "updates_per_s": bs * nb / (lat.sum() / 1000.0),
                              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                              "methods": {"local": methods.count(1), "repeel": methods.count(2)},
-                             "rows_repaired_in_place": local_rows,
+                             "rows_repaired_in_place": {"deletions": local_rows, "insertions": local_ins},
                              "batch_detail": {"fields": ["total_ms", "apply_ms", "core_ms", "rows_ms",
-                                                         "rows_recomputed", "rows_repaired", "method", "rebuilt"],
+                                                         "rows_recomputed", "rows_repaired", "method", "rebuilt",
+                                                         "del_repair_ms", "ins_repair_ms", "ins_scanned"],
                                               "batches": detail}}
     clocks = sampler.stop()
     launches = dc.launch_count() - launches0
@@ -697,13 +701,16 @@ def run_row_sharded(args, w, rank, world, local, dist):
 
 
 def _stream_times(dc, g, u, v, dl, sizes, method):
-    pos, ms, methods = 0, [], []
+    """Per batch: device ms, method, rows repaired in place (bit 0
+    deletions, bit 1 insertions)."""
+    pos, ms, methods, local = 0, [], [], []
     for bs in sizes:
         st = g.maintain(u[pos:pos + bs], v[pos:pos + bs], dl[pos:pos + bs], method)
         ms.append(st["total_ms"])
         methods.append(st["method"])
+        local.append(st["rows_local"])
         pos += bs
-    return np.array(ms), np.array(methods)
+    return np.array(ms), np.array(methods), np.array(local)
 
 
 def _hot_stream(dc, V, s, d, sizes, hot_frac, rng, seed):
@@ -716,13 +723,15 @@ def _hot_stream(dc, V, s, d, sizes, hot_frac, rng, seed):
 
 
 def run_sched(args, w, rank, world, local):
-    """Learned scheduler against the rule of thumb.  Training: a fresh R-MAT
-    graph, a log-uniform batch stream (10% hot) applied to two copies, one
-    per method, logging features and device times; the network learns
-    log(time - row recompute) of each method.  Evaluation: a fresh R-MAT 23
-    graph and stream applied to two copies, one with the network attached,
-    one with the rule of thumb; both must end equal to a fresh
-    decomposition of the final edge set."""
+    """Learned scheduler against the rule of thumb.  Training: fresh R-MAT
+    graphs, log-uniform batch streams (10% hot) applied to two copies, one
+    per path -- incremental (local kmax / row-0 update, rows repaired in
+    place wherever the batch fits) and full (fused re-peel, rows
+    recomputed) -- logging features and device times; the network learns
+    log(time) of each path.  Evaluation: a fresh R-MAT 23 graph and stream
+    applied to two copies, one with the network attached, one with the rule
+    of thumb (method by batch size, rows by the default row mode); both must
+    end equal to the oracle's decomposition of the final edge set."""
     import torch
     import dcore_b200 as dc
     torch.cuda.set_device(local)
@@ -736,16 +745,16 @@ def run_sched(args, w, rank, world, local):
         tr_sizes = _log_uniform(rng, w["train_batches"], w["train_max"])
         u, v, dl, _ = _hot_stream(dc, V, s, d, tr_sizes, w["hot_frac"], rng, w["seed"] + 200 + j)
         logs = []
-        for method in (dc.MAINT_LOCAL, dc.MAINT_REPEEL):
+        for method, mode in ((dc.MAINT_LOCAL, 3), (dc.MAINT_REPEEL, 0)):
             with dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16) as g:
-                g.set_row_repair(0)  # identical batches (and row work) on both copies
+                g.set_row_repair(mode)
                 g.decompose()
                 g.maint_log(True)
                 _stream_times(dc, g, u, v, dl, tr_sizes, method)
                 logs.append(g.maint_log())
         (X, _, ta), (_, _, tb) = logs
         Xs.append(X)
-        Ts.append(np.log(np.stack([ta[:, 0] - ta[:, 2], tb[:, 0] - tb[:, 2]], 1).clip(1e-3) + 1e-2))
+        Ts.append(np.log(np.stack([ta[:, 0], tb[:, 0]], 1).clip(1e-3)))
     X = np.concatenate(Xs).astype(np.float32)
     T = np.concatenate(Ts).astype(np.float32)
     sched = dc.Scheduler(seed=w["seed"])
@@ -762,14 +771,14 @@ def run_sched(args, w, rank, world, local):
     launches0 = dc.launch_count()
     for name, sch in (("learned", sched), ("rule", None)):
         g = dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16)
-        g.set_row_repair(0)  # both policies do the same row work; only the method differs
-        g.decompose()
+        g.decompose()  # default row mode: the rule's rows; the network sets the path per batch
         g.set_scheduler(sch)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ms, methods = _stream_times(dc, g, u, v, dl, ev_sizes, dc.MAINT_AUTO)
+        ms, methods, rows_local = _stream_times(dc, g, u, v, dl, ev_sizes, dc.MAINT_AUTO)
         wall = time.perf_counter() - t0
-        res[name] = {"wall_s": wall, "device_ms": float(ms.sum()), "ms": ms, "methods": methods, "graph": g}
+        res[name] = {"wall_s": wall, "device_ms": float(ms.sum()), "ms": ms, "methods": methods,
+                     "rows_local": rows_local, "graph": g}
     launches = dc.launch_count() - launches0
     clocks = sampler.stop()
     fs, fd = _final_edges(s, d, u, v, dl)
@@ -781,7 +790,7 @@ def run_sched(args, w, rank, world, local):
     L, Rr = res["learned"], res["rule"]
     updates = int(ev_sizes.sum())
     value = updates / L["wall_s"]
-    diff = L["methods"] != Rr["methods"]
+    diff = (L["methods"] != Rr["methods"]) | (L["rows_local"] != Rr["rows_local"])
     line = {"metric": METRIC_MAINT, "value": value, "unit": "updates/s", "n_gpus": world,
             "steps": int(len(ev_sizes)), "warmup": 1, "ms_per_step": float(np.median(L["ms"])),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
@@ -804,7 +813,15 @@ def run_sched(args, w, rank, world, local):
                           "learned_methods": {"local": int((L["methods"] == 1).sum()),
                                               "repeel": int((L["methods"] == 2).sum())},
                           "rule_methods": {"local": int((Rr["methods"] == 1).sum()),
-                                           "repeel": int((Rr["methods"] == 2).sum())}},
+                                           "repeel": int((Rr["methods"] == 2).sum())},
+                          "batch_detail": {"fields": ["updates", "hot", "learned_ms", "learned_method",
+                                                      "learned_rows_in_place", "rule_ms", "rule_method",
+                                                      "rule_rows_in_place"],
+                                           "batches": [[int(ev_sizes[i]), int(hot_batch[i]),
+                                                        round(float(L["ms"][i]), 2), int(L["methods"][i]),
+                                                        int(L["rows_local"][i]), round(float(Rr["ms"][i]), 2),
+                                                        int(Rr["methods"][i]), int(Rr["rows_local"][i])]
+                                                       for i in range(len(ev_sizes))]}},
             "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": float(9 * updates / len(ev_sizes)),
                     "d2h_bytes_per_step": 0, "timing": "wall clock of dc_maintain calls with host batches"},
             "gpu_launches": int(launches), "clocks": clocks}

@@ -346,7 +346,7 @@ extern "C" int dc_maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is
 
 extern "C" int dc_set_row_repair(dc_graph* h, int on) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");
-    if (on < 0 || on > 2) return set_error(DC_ERR_INVALID, "dc_set_row_repair: mode must be 0, 1 or 2");
+    if (on < 0 || on > 3) return set_error(DC_ERR_INVALID, "dc_set_row_repair: mode must be 0, 1, 2 or 3");
     h->row_repair = on;
     return DC_OK;
 }

@@ -2032,6 +2032,42 @@ static int persistent_grid(dc_graph* h, const void* fn, int bps, int* blocks) {
     return DC_OK;
 }
 
+// A control block as persistent_launch prepares it (no trace, no test
+// hook), written by the device: usable inside a captured CUDA graph.
+__global__ void k_ctl_init(EngineCtl* c, unsigned long long wait_ns) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(c);
+    for (uint32_t i = threadIdx.x; i < sizeof(EngineCtl) / 4; i += blockDim.x) w[i] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c->step = -1;
+        c->wait_ns = wait_ns;
+    }
+}
+
+int ctl_init_enqueue(dc_graph* h, EngineCtl* ctl, cudaStream_t st) {
+    ++g_launches;
+    k_ctl_init<<<1, 256, 0, st>>>(ctl, h->wait_ns);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DC_OK : set_error(DC_ERR_CUDA, "control block init: %s", cudaGetErrorString(e));
+}
+
+// Capture-safe persistent launch: the control block is initialised by a
+// kernel and nothing is waited for (the caller reads the block's status
+// later).
+int persistent_enqueue(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* ctl, cudaStream_t st,
+                       int bps) {
+    int blocks = 0;
+    if (int rc = persistent_grid(h, fn, bps, &blocks)) return rc;
+    if (int rc = ctl_init_enqueue(h, ctl, st)) return rc;
+    ++g_launches;
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kThreads), args, 0, st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(DC_ERR_CUDA, "%s: cooperative launch failed (%s)", name, cudaGetErrorString(e));
+    }
+    return DC_OK;
+}
+
 // Initialises a control block (on stream st) and launches a persistent
 // kernel there without waiting.  The handle's own block carries the trace.
 static int persistent_launch(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* ctl,
@@ -2810,6 +2846,7 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
         h->times.row0_ms = 0;
         cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]);
         h->times.trans_ms = ms;
+        h->full_rows_ms = ms;
         cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
         h->times.sky_ms = ms;
         h->times.expand_ms = 0;
@@ -2836,6 +2873,7 @@ int decompose(dc_graph* h, int method, int materialize_rows) {
     h->times.row0_ms = ms;
     cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
     h->times.trans_ms = ms;
+    h->full_rows_ms = ms;
     cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]);
     h->times.sky_ms = ms;
     cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]);

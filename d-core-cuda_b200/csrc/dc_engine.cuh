@@ -98,15 +98,28 @@ int build_from_host_csr(dc_graph* h, uint32_t V, uint64_t E, const int32_t* in_d
 
 // Batch maintenance (dc_maint.cu).
 int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t b, int method, dc_maint_stats* st);
-// Rows 1..R repaired in place after a deletion-only batch (dc_repair.cu);
-// *applied = false when the caller must recompute them instead.
-int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_dv, uint32_t n_del, bool* applied);
+// Rows 1..R repaired in place after a deletion-only batch (dc_repair.cu),
+// giving up after deadline_ns (0: no limit); *applied = false when the caller
+// must recompute them instead.
+int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_dv, uint32_t n_del,
+                unsigned long long deadline_ns, bool* applied);
 // Deletions per batch below which maintenance splits a mixed batch to repair
 // its rows in place.
 uint32_t row_repair_max_deletions();
 // Whether a row repair after deleting these (device) edges is expected to
 // beat recomputing the rows (uses the graph before the deletions).
 bool row_repair_worthwhile(dc_graph* h, const uint32_t* d_u, const uint32_t* d_v, uint32_t n);
+// Rows 1..R repaired in place after an insertion-only batch (dc_repair.cu),
+// giving up after deadline_ns (0: no limit); *applied = false when the caller
+// must recompute them instead.
+int rows_repair_ins(dc_graph* h, int32_t R, const uint32_t* d_iu, const uint32_t* d_iv, uint32_t n_ins,
+                    unsigned long long deadline_ns, bool* applied, unsigned long long* scanned);
+// Insertions per batch below which maintenance repairs rows in place.
+uint32_t row_repair_max_insertions();
+// New skyline from the current one, the updated row 0 and kmax, and the first
+// nlog entries of the scratch change log (dc_repair.cu); nlog = 0 when no row
+// above 0 changed.
+int apply_change_log(dc_graph* h, uint64_t nlog, bool* applied);
 // Maintenance method for a batch (rule of thumb or the learned scheduler).
 int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del);
 
@@ -158,6 +171,11 @@ int ensure_tring(dc_graph* h, uint64_t need);
 int check_ctl_on(EngineCtl* ctl, cudaStream_t st, EngineCtl* hc, const char* what);
 // bps: blocks per SM for this kernel (0 = the handle's blocks_per_sm, else 2).
 int run_persistent(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* out, int bps = 0);
+// Capture-safe forms (no host memory, no waiting): a control block reset by a
+// kernel, and a persistent launch after such a reset.
+int ctl_init_enqueue(dc_graph* h, EngineCtl* ctl, cudaStream_t st);
+int persistent_enqueue(dc_graph* h, const void* fn, void** args, const char* name, EngineCtl* ctl, cudaStream_t st,
+                       int bps = 0);
 int check_ctl(dc_graph* h, EngineCtl* hc, const char* what);
 int scan_tmp64(dc_graph* h, uint64_t n);
 // Skyline from row 0 and the corner log: entries [0, nlog) and, when a second

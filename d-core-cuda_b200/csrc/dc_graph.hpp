@@ -130,6 +130,7 @@ struct dc_graph {
              seg_void[dc::kMaxRowSegments - 1] = {};
     uint64_t stat_evals = 0, stat_drops = 0, stat_entries = 0;
     uint64_t full_work = 0;  // sum over vertices of degree x kmax at the last full decomposition
+    float full_rows_ms = 0;  // rows phase (rows 1..kmax) of the last full decomposition
     // limit of one bounded device wait in ns (0: the default, dc::kWaitNs)
     uint64_t wait_ns = 0;
     // failure-detection tests: block of the next persistent launch that

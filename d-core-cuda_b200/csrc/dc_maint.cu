@@ -100,8 +100,11 @@ __global__ void k_del_validate(uint32_t n, const uint32_t* du, const uint32_t* d
 // Warp per list: removes the listed neighbours (one occurrence each, in
 // order) by swapping with the last live entry.  All deletions of one list
 // are in one group, so no two warps touch the same list.
+// run: nullptr, or a device flag that must be nonzero for the kernel to act
+// (a captured batch skips its updates when the batch failed validation).
 __global__ void k_del_apply(uint32_t ngroups, const uint32_t* gvert, const uint32_t* goff, const uint32_t* gnbr,
-                            const uint32_t* off, int32_t* len, uint32_t* nbr, EngineCtl* c) {
+                            const uint32_t* off, int32_t* len, uint32_t* nbr, EngineCtl* c, const int* run) {
+    if (run && !*run) return;
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -150,7 +153,8 @@ __global__ void k_ins_fits(uint32_t V, const uint32_t* out_off, const int32_t* o
 // Appends each edge to the free slots of both lists (capacity checked).
 __global__ void k_ins_apply(uint32_t n, const uint32_t* iu, const uint32_t* iv, const uint32_t* out_off,
                             int32_t* out_len, uint32_t* out_nbr, const uint32_t* in_off, int32_t* in_len,
-                            uint32_t* in_nbr) {
+                            uint32_t* in_nbr, const int* run) {
+    if (run && !*run) return;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t u = iu[i], v = iv[i];
         int po = atomicAdd(&out_len[u], 1);
@@ -212,6 +216,7 @@ struct CoreParams {
     int32_t b;  // an insert batch raises no value by more than b
     TicketQueue q;
     EngineCtl* ctl;
+    const int* run;  // nullptr, or a device flag that must be nonzero for the kernel to act
 };
 
 __device__ __forceinline__ bool core_request(uint32_t* m, EngineCtl* c) {
@@ -258,6 +263,7 @@ __device__ __forceinline__ void core_block_done(EngineCtl* c, unsigned* s_cnt) {
 }
 
 __global__ void __launch_bounds__(kMThreads) k_core_local(CoreParams p) {
+    if (p.run && !*(const volatile int*)p.run) return;  // every block returns: no barrier is entered
     const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const unsigned gwarp = blockIdx.x * kMWarps + wib;
     const unsigned nwarps = gridDim.x * kMWarps;
@@ -455,12 +461,13 @@ __global__ void __launch_bounds__(kMThreads) k_core_local(CoreParams p) {
 // batch features for the scheduler
 // ---------------------------------------------------------------------------
 // acc: [0] sum log2(1+deg) over endpoints, [1] sum min-kmax, [2] dense-core
-// edges, [3] sum row-0 value over endpoints (floats); iacc: [0] max deg,
-// [1] max min-kmax (ints)
+// edges, [3] sum row-0 value over endpoints, [4] sum of degree x kmax over
+// endpoints (the list entries a row repair scans at least once; floats);
+// iacc: [0] max deg, [1] max min-kmax (ints)
 __global__ void k_batch_features(uint32_t n, const uint32_t* u, const uint32_t* v, const int32_t* kmax,
                                  const int32_t* row0, const int32_t* in_len, const int32_t* out_len, int K, float* acc,
                                  int* iacc) {
-    float a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    float a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0;
     int m0 = 0, m1 = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t x = u[i], y = v[i];
@@ -470,6 +477,7 @@ __global__ void k_batch_features(uint32_t n, const uint32_t* u, const uint32_t* 
         a1 += mk;
         a2 += (2 * mk >= K) ? 1.f : 0.f;
         a3 += row0[x] + row0[y];
+        a4 += (float)dx * (float)max(kmax[x], 0) + (float)dy * (float)max(kmax[y], 0);
         m0 = max(m0, max(dx, dy));
         m1 = max(m1, mk);
     }
@@ -479,6 +487,7 @@ __global__ void k_batch_features(uint32_t n, const uint32_t* u, const uint32_t* 
         a1 += __shfl_xor_sync(0xFFFFFFFFu, a1, s);
         a2 += __shfl_xor_sync(0xFFFFFFFFu, a2, s);
         a3 += __shfl_xor_sync(0xFFFFFFFFu, a3, s);
+        a4 += __shfl_xor_sync(0xFFFFFFFFu, a4, s);
         m0 = max(m0, __shfl_xor_sync(0xFFFFFFFFu, m0, s));
         m1 = max(m1, __shfl_xor_sync(0xFFFFFFFFu, m1, s));
     }
@@ -487,6 +496,7 @@ __global__ void k_batch_features(uint32_t n, const uint32_t* u, const uint32_t* 
         atomicAdd(&acc[1], a1);
         atomicAdd(&acc[2], a2);
         atomicAdd(&acc[3], a3);
+        atomicAdd(&acc[4], a4);
         atomicMax(&iacc[0], m0);
         atomicMax(&iacc[1], m1);
     }
@@ -656,10 +666,13 @@ int sched_choose(dc_sched* s, const float* feat);
 // row 0 grows with the batch (its bound on how far a value can rise is the
 // number of inserted edges), the fused peel is a fixed pass over the graph.
 static constexpr uint64_t kSchedLocalMax = 1ull << 16;
+// Row mode 1 repairs rows in place for batches of at most this many net
+// updates (the rule of thumb's local-method limit too).
+static constexpr uint64_t kRuleRepairMax = 64;
 
 int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del) {
     (void)h;
-    return (n_ins + n_del <= 64) ? DC_MAINT_LOCAL : DC_MAINT_REPEEL;
+    return (n_ins + n_del <= kRuleRepairMax) ? DC_MAINT_LOCAL : DC_MAINT_REPEEL;
 }
 
 // The 16 scheduler features of a net batch against the current graph and
@@ -671,7 +684,7 @@ static int batch_features(dc_graph* h, const NetBatch& nb, float* f) {
     u.insert(u.end(), nb.ins_u.begin(), nb.ins_u.end());
     v.insert(v.end(), nb.ins_v.begin(), nb.ins_v.end());
     const uint64_t n = u.size();
-    float acc[4] = {0, 0, 0, 0};
+    float acc[5] = {0, 0, 0, 0, 0};
     int iacc[2] = {0, 0};
     if (n) {
         uint32_t *du = nullptr, *dv = nullptr;
@@ -681,12 +694,12 @@ static int batch_features(dc_graph* h, const NetBatch& nb, float* f) {
             return DC_ERR_NOMEM;
         }
         float* dacc = (float*)h->scratch->tmp64;
-        int* diacc = (int*)(dacc + 4);
+        int* diacc = (int*)(dacc + 6);
         MT_CUDA(cudaMemsetAsync(dacc, 0, 32, h->stream));
         ++g_launches;
         k_batch_features<<<mgrid(h, n), kMThreads, 0, h->stream>>>((uint32_t)n, du, dv, d.kmax_v, d.row0, g.in_len,
                                                                    g.out_len, d.kmax, dacc, diacc);
-        MT_CUDA(cudaMemcpyAsync(acc, dacc, 16, cudaMemcpyDeviceToHost, h->stream));
+        MT_CUDA(cudaMemcpyAsync(acc, dacc, 20, cudaMemcpyDeviceToHost, h->stream));
         MT_CUDA(cudaMemcpyAsync(iacc, diacc, 8, cudaMemcpyDeviceToHost, h->stream));
         MT_CUDA(cudaStreamSynchronize(h->stream));
         mt_free(h->stream, du);
@@ -708,7 +721,9 @@ static int batch_features(dc_graph* h, const NetBatch& nb, float* f) {
     f[12] = (float)std::log2(1.0 + (double)d.n_corners / (g.V ? g.V : 1));
     f[13] = (float)((double)nb.n_ins / (double)std::max<uint64_t>(1, nb.n_ins + nb.n_del));
     f[14] = (float)std::log2(1.0 + n);
-    f[15] = 1.0f;
+    // expected work of an in-place row repair against a recomputation
+    // (the rule of thumb repairs below 1/160 of the graph's degree x kmax)
+    f[15] = (float)std::log2(1.0 + 160.0 * acc[4] / (double)std::max<uint64_t>(1, h->full_work));
     return DC_OK;
 }
 
@@ -771,7 +786,7 @@ static int apply_deletions(dc_graph* h, const NetBatch& nb) {
         ++g_launches;
         k_del_apply<<<mgrid(h, gvert.size() * 32), kMThreads, 0, h->stream>>>(
             (uint32_t)gvert.size(), d_gv, d_go, d_gn, side == 0 ? g.out_off : g.in_off,
-            side == 0 ? g.out_len : g.in_len, side == 0 ? g.out_nbr : g.in_nbr, h->ctl);
+            side == 0 ? g.out_len : g.in_len, side == 0 ? g.out_nbr : g.in_nbr, h->ctl, nullptr);
         cudaError_t e = cudaStreamSynchronize(h->stream);
         mt_free(h->stream, d_gv);
         mt_free(h->stream, d_go);
@@ -856,7 +871,7 @@ static int apply_insertions(dc_graph* h, const NetBatch& nb, uint32_t** d_iu_out
     } else if (rc == DC_OK) {
         ++g_launches;
         k_ins_apply<<<mgrid(h, n), kMThreads, 0, h->stream>>>(n, iu, iv, g.out_off, g.out_len, g.out_nbr, g.in_off,
-                                                              g.in_len, g.in_nbr);
+                                                              g.in_len, g.in_nbr, nullptr);
         g.E += n;
     }
     if (rc != DC_OK) {
@@ -896,6 +911,7 @@ static int core_local(dc_graph* h, int which, int32_t* val, const int32_t* old, 
     p.n_seeds = n_seeds;
     p.insert_mode = insert_mode;
     p.b = b;
+    p.run = nullptr;
     if (int rc = ensure_tring(h, 2ull * g.V + (uint64_t)h->geom.sms * 64 + 4096)) return rc;
     p.q.slots = s->tring;
     p.q.mask = (unsigned)(s->tring_cap - 1);
@@ -908,7 +924,33 @@ static int core_local(dc_graph* h, int which, int32_t* val, const int32_t* old, 
     return DC_OK;
 }
 
-int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t b, int method, dc_maint_stats* st) {
+// Appends one record of the maintenance log (scheduler training data).
+static void log_batch(dc_graph* h, const float* feat, const dc_maint_stats* st) {
+    MaintLogRec r;
+    memcpy(r.feat, feat, sizeof(r.feat));
+    r.method = st->method;
+    r.total_ms = st->total_ms;
+    r.core_ms = st->core_ms;
+    r.rows_ms = st->rows_ms;
+    h->maint_log.push_back(r);
+}
+
+// Time limit of an in-place row repair of rows 1..R: what recomputing them
+// is expected to cost (the rows phase of the last full decomposition, scaled
+// by R / kmax, plus the recomputation's fixed passes over C_1), so that a
+// repair that turns out larger than expected gives up in time.  Row mode 2
+// (repair whenever the batch fits) sets no limit.
+static unsigned long long repair_deadline_ns(const dc_graph* h, int32_t R, int rmode) {
+    if (rmode == 2) return 0;
+    const double K = std::max<int32_t>(1, h->d.kmax);
+    const double ms = 2.0 + h->full_rows_ms * std::min(1.0, (double)R / K) + 0.1 * h->full_rows_ms;
+    return (unsigned long long)(ms * 1e6);
+}
+
+// repair_mode: the row maintenance mode of this batch (-1: the handle's);
+// nested: a part of a split batch (no features, no log record).
+static int maintain_impl(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t b, int method,
+                         int repair_mode, bool nested, dc_maint_stats* st) {
     DevGraph& g = h->g;
     Decomp& d = h->d;
     const uint32_t V = g.V;
@@ -923,17 +965,60 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
         if (int rc = decompose(h, 0, 0)) return rc;
     NetBatch nb;
     if (int rc = net_batch(V, pairs, is_del, b, nb)) return rc;
+    // features of the batch against the decomposition before it
+    float feat[16];
+    const bool want_feat = !nested && (h->log_maint || (method == DC_MAINT_AUTO && h->sched));
+    if (want_feat)
+        if (int rc = batch_features(h, nb, feat)) return rc;
+    int rmode = repair_mode >= 0 ? repair_mode : h->row_repair;
+    bool by_rule = false;  // method picked by the rule of thumb (halves of a split batch pick their own)
+    if (method == DC_MAINT_AUTO) {
+        // the network picks the incremental path (local kmax / row-0 update,
+        // rows repaired in place wherever the batch fits, within the time
+        // limit: row mode 3) or the full one
+        // (fused re-peel, rows recomputed) where both are practical; past
+        // kSchedLocalMax net updates the local update's region covers most
+        // of the graph and the full path is taken without asking.  Without
+        // a network the rule of thumb picks the method and the handle's mode
+        // the rows.
+        int m = !nested && h->sched && nb.n_ins + nb.n_del <= kSchedLocalMax ? sched_choose(h->sched, feat) : -1;
+        if (m == DC_MAINT_LOCAL) {
+            method = DC_MAINT_LOCAL;
+            rmode = 3;
+        } else if (m == DC_MAINT_REPEEL) {
+            method = DC_MAINT_REPEEL;
+            rmode = 0;
+        } else {
+            method = choose_method(h, nb.n_ins, nb.n_del);
+            by_rule = true;
+        }
+    }
+    // the rule's row mode repairs small batches only: past kRuleRepairMax net
+    // updates the expected-work estimate misses the cascades that deletions
+    // near the dense core start, and a recomputation is the safer bet
+    if (rmode == 1 && nb.n_ins + nb.n_del > kRuleRepairMax) rmode = 0;
     bool repair_del = false;  // rows of the deletions repaired in place
-    if (h->row_repair && !nb.del_u.empty() && nb.del_u.size() <= row_repair_max_deletions() && d.kmax_v) {
+    if (rmode && !nb.del_u.empty() && nb.del_u.size() <= row_repair_max_deletions() && d.kmax_v) {
         uint32_t *eu = nullptr, *ev = nullptr;
         if (upload(h, &eu, nb.del_u) == DC_OK && upload(h, &ev, nb.del_v) == DC_OK)
-            repair_del = h->row_repair == 2 || row_repair_worthwhile(h, eu, ev, (uint32_t)nb.del_u.size());
+            repair_del = rmode >= 2 || row_repair_worthwhile(h, eu, ev, (uint32_t)nb.del_u.size());
+        mt_free(h->stream, eu);
+        mt_free(h->stream, ev);
+    }
+    bool repair_ins = false;  // rows of the insertions repaired in place
+    if (rmode && !nb.ins_u.empty() && nb.ins_u.size() <= row_repair_max_insertions() && d.kmax_v) {
+        uint32_t *eu = nullptr, *ev = nullptr;
+        if (upload(h, &eu, nb.ins_u) == DC_OK && upload(h, &ev, nb.ins_v) == DC_OK)
+            repair_ins = rmode >= 2 || row_repair_worthwhile(h, eu, ev, (uint32_t)nb.ins_u.size());
         mt_free(h->stream, eu);
         mt_free(h->stream, ev);
     }
     if (repair_del && !nb.ins_u.empty()) {
-        // deletions first (their rows are repaired in place), then the
-        // insertions: the net effect per edge makes the two commute
+        // deletions first (their rows repaired in place), then the
+        // insertions with their own row maintenance: the net effect per edge
+        // makes the two commute.  (Insertions repaired in place after
+        // deletions that recompute rows 1..R would only add to that
+        // recomputation, so they split the batch only with the deletions.)
         std::vector<uint32_t> pd(2 * nb.del_u.size()), pi(2 * nb.ins_u.size());
         for (size_t i = 0; i < nb.del_u.size(); ++i) {
             pd[2 * i] = nb.del_u[i];
@@ -945,33 +1030,29 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
         }
         std::vector<uint8_t> ones(nb.del_u.size(), 1);
         dc_maint_stats a, c;
-        if (int rc = maintain(h, pd.data(), ones.data(), nb.del_u.size(), method, &a)) return rc;
-        if (int rc = maintain(h, pi.data(), nullptr, nb.ins_u.size(), method, &c)) return rc;
+        const int half = by_rule ? DC_MAINT_AUTO : method;
+        if (int rc = maintain_impl(h, pd.data(), ones.data(), nb.del_u.size(), half, rmode, true, &a)) return rc;
+        if (int rc = maintain_impl(h, pi.data(), nullptr, nb.ins_u.size(), half, rmode, true, &c)) return rc;
         *st = c;
         st->deleted = a.deleted;
         st->rows_recomputed = std::max(a.rows_recomputed, c.rows_recomputed);
         st->rebuilt = a.rebuilt | c.rebuilt;
-        st->rows_local = a.rows_local;
+        st->rows_local = a.rows_local | c.rows_local;
+        st->del_repair_ms = a.del_repair_ms;
+        st->ins_repair_ms = c.ins_repair_ms;
+        st->ins_scanned = c.ins_scanned;
         st->region = a.region + c.region;
         st->apply_ms = a.apply_ms + c.apply_ms;
         st->core_ms = a.core_ms + c.core_ms;
         st->rows_ms = a.rows_ms + c.rows_ms;
         st->total_ms = a.total_ms + c.total_ms;
+        st->method = method;
+        h->mtimes.total_ms = st->total_ms;
+        if (h->log_maint && want_feat) log_batch(h, feat, st);
         return DC_OK;
     }
     st->deleted = nb.n_del;
     st->inserted = nb.n_ins;
-    float feat[16];
-    const bool want_feat = h->log_maint || (method == DC_MAINT_AUTO && h->sched);
-    if (want_feat)
-        if (int rc = batch_features(h, nb, feat)) return rc;
-    if (method == DC_MAINT_AUTO) {
-        // the network decides where both methods are practical; past
-        // kSchedLocalMax net updates the local update's region covers most
-        // of the graph and the fused re-peel is taken without asking
-        int m = h->sched && nb.n_ins + nb.n_del <= kSchedLocalMax ? sched_choose(h->sched, feat) : -1;
-        method = m > 0 ? m : choose_method(h, nb.n_ins, nb.n_del);
-    }
     st->method = method;
     cudaEvent_t* ev = h->ev;
     cudaEventRecord(ev[0], h->stream);
@@ -1050,12 +1131,55 @@ int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t
             st->lmax = d.lmax;
             goto timing;
         }
+        // ---- no row above 0 can change: only row 0's corners are new
+        if (R == 0) {
+            bool applied = false;
+            if ((rc = apply_change_log(h, 0, &applied))) goto out;
+            if (applied) {
+                d.kmax = Knew;
+                d.lmax = res[2];
+                d.rows_valid = false;
+                d.valid = true;
+                st->kmax = d.kmax;
+                st->lmax = d.lmax;
+                goto timing;
+            }
+        }
         // ---- deletions only: repair rows 1..R in place
         if (repair_del && nb.ins_u.empty()) {
             bool applied = false;
-            if ((rc = rows_repair(h, R, d_du, d_dv, (uint32_t)nb.del_u.size(), &applied))) goto out;
+            cudaEventRecord(ev[4], h->stream);
+            if ((rc = rows_repair(h, R, d_du, d_dv, (uint32_t)nb.del_u.size(), repair_deadline_ns(h, R, rmode),
+                                  &applied)))
+                goto out;
+            cudaEventRecord(ev[5], h->stream);
+            cudaEventSynchronize(ev[5]);
+            cudaEventElapsedTime(&st->del_repair_ms, ev[4], ev[5]);
             if (applied) {
                 st->rows_local = 1;
+                d.kmax = Knew;
+                d.lmax = res[2];
+                d.rows_valid = false;
+                d.valid = true;
+                st->kmax = d.kmax;
+                st->lmax = d.lmax;
+                goto timing;
+            }
+        }
+        // ---- insertions only: repair rows 1..R in place
+        if (repair_ins && nb.del_u.empty()) {
+            bool applied = false;
+            unsigned long long scanned = 0;
+            cudaEventRecord(ev[4], h->stream);
+            if ((rc = rows_repair_ins(h, R, d_iu, d_iv, (uint32_t)nb.ins_u.size(), repair_deadline_ns(h, R, rmode), &applied,
+                                      &scanned)))
+                goto out;
+            cudaEventRecord(ev[5], h->stream);
+            cudaEventSynchronize(ev[5]);
+            cudaEventElapsedTime(&st->ins_repair_ms, ev[4], ev[5]);
+            st->ins_scanned = scanned;
+            if (applied) {
+                st->rows_local = 2;
                 d.kmax = Knew;
                 d.lmax = res[2];
                 d.rows_valid = false;
@@ -1136,15 +1260,7 @@ timing:
     }
     st->kmax = d.kmax;
     st->lmax = d.lmax;
-    if (h->log_maint && want_feat) {
-        MaintLogRec r;
-        memcpy(r.feat, feat, sizeof(feat));
-        r.method = st->method;
-        r.total_ms = st->total_ms;
-        r.core_ms = st->core_ms;
-        r.rows_ms = st->rows_ms;
-        h->maint_log.push_back(r);
-    }
+    if (h->log_maint && want_feat) log_batch(h, feat, st);
 out:
     mt_free(h->stream, d_du);
     mt_free(h->stream, d_dv);
@@ -1158,6 +1274,10 @@ out:
         d.row_hi = d.kmax;
     }
     return rc;
+}
+
+int maintain(dc_graph* h, const uint32_t* pairs, const uint8_t* is_del, uint64_t b, int method, dc_maint_stats* st) {
+    return maintain_impl(h, pairs, is_del, b, method, -1, false, st);
 }
 
 }  // namespace dc

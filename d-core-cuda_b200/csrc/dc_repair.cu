@@ -64,12 +64,19 @@ struct RepairParams {
     const uint32_t* sky_off;  // old skyline
     const int32_t* sky_k;
     const int32_t* sky_l;
-    const uint32_t* del_u;  // deleted edges u -> v
+    const uint32_t* del_u;  // deleted edges u -> v (insertions: inserted edges)
     const uint32_t* del_v;
     uint32_t n_del;
-    const uint32_t* leave;  // vertices whose kmax fell
+    const uint32_t* leave;  // vertices whose kmax fell (insertions: rose)
     uint32_t n_leave;
+    const int32_t* row0_new;  // insertions: row 0 after the batch
+    unsigned long long deadline_ns;  // a block still busy this long after its start gives up (0: never)
     int32_t R;
+    // captured batches: R and the vertex count of `leave` read on the device
+    // when set, and a flag that must be nonzero for the kernel to act
+    const int32_t* R_dev;
+    const unsigned* n_leave_dev;
+    const int* run;
     uint32_t* log_v;
     int32_t* log_k;
     int32_t* log_l;
@@ -77,17 +84,19 @@ struct RepairParams {
     EngineCtl* ctl;  // level = row counter, log_count, error
 };
 
-struct RowState {
+template <int NW>
+struct RowStateT {
     uint32_t key[kHash];
     int cur[kHash];
     unsigned st[kHash];  // 0 idle, 1 queued or being evaluated, 2 re-run requested
     uint32_t ring[kHash];
     unsigned qhead, qtail, used;
     int out;    // queued + running items
-    int abort;  // table full, or a wait ran out
+    int abort;  // table full, a wait ran out, or (insertions) the scan budget is spent
     int k;
-    int hist[kRWarps][2][kRWin];
+    int hist[NW][2][kRWin];
 };
+using RowState = RowStateT<kRWarps>;
 
 __device__ __forceinline__ int vld(const int* p) { return *(const volatile int*)p; }
 __device__ __forceinline__ unsigned vldu(const unsigned* p) { return *(const volatile unsigned*)p; }
@@ -111,7 +120,8 @@ __device__ __forceinline__ int sky_at(const RepairParams& p, uint32_t v, int k) 
 __device__ __forceinline__ unsigned hslot0(uint32_t v) { return (v * 2654435761u) >> (32 - kHashBits); }
 
 // Table slot of v (inserting it when asked); -1 when absent / table full.
-__device__ int h_slot(RowState& S, uint32_t v, bool insert) {
+template <class St>
+__device__ int h_slot(St& S, uint32_t v, bool insert) {
     unsigned i = hslot0(v) & (kHash - 1);
     for (int probe = 0; probe < kHash; ++probe) {
         uint32_t key = vldu(&S.key[i]);
@@ -132,7 +142,8 @@ __device__ int h_slot(RowState& S, uint32_t v, bool insert) {
 }
 
 // Row-k value of w: -1 outside C_k, else the override or the old value.
-__device__ __forceinline__ int rv(const RepairParams& p, RowState& S, uint32_t w, int k) {
+template <class St>
+__device__ __forceinline__ int rv(const RepairParams& p, St& S, uint32_t w, int k) {
     if (p.kmax_new[w] < k) return -1;
     int i = h_slot(S, w, false);
     if (i >= 0) {
@@ -142,7 +153,8 @@ __device__ __forceinline__ int rv(const RepairParams& p, RowState& S, uint32_t w
     return sky_at(p, w, k);
 }
 
-__device__ __forceinline__ void enqueue(RowState& S, unsigned slot) {
+template <class St>
+__device__ __forceinline__ void enqueue(St& S, unsigned slot) {
     atomicAdd(&S.out, 1);
     unsigned pos = atomicAdd(&S.qtail, 1u);
     __threadfence_block();
@@ -150,7 +162,8 @@ __device__ __forceinline__ void enqueue(RowState& S, unsigned slot) {
 }
 
 // Any thread: asks for an evaluation of w at this row.
-__device__ __forceinline__ void push(RowState& S, uint32_t w) {
+template <class St>
+__device__ __forceinline__ void push(St& S, uint32_t w) {
     int slot = h_slot(S, w, true);
     if (slot < 0) return;
     unsigned old = atomicCAS(&S.st[slot], 0u, 1u);
@@ -160,7 +173,8 @@ __device__ __forceinline__ void push(RowState& S, uint32_t w) {
 
 // Converged warp: one histogram pass over a list for the window [lo, hi];
 // values above hi land in the top bin on the first window only.
-__device__ __forceinline__ void r_hist(const RepairParams& p, RowState& S, const uint32_t* a, int n, int k, int lo,
+template <class St>
+__device__ __forceinline__ void r_hist(const RepairParams& p, St& S, const uint32_t* a, int n, int k, int lo,
                                        int hi, bool first, int* bins) {
     const unsigned lane = threadIdx.x & 31u;
     int top = 0;
@@ -180,7 +194,8 @@ __device__ __forceinline__ void r_hist(const RepairParams& p, RowState& S, const
 // how many neighbours hold at least nv, read after the write.  The recount
 // closes the race in which x and a neighbour drop at the same time and each
 // read the other's old value: whichever reads second sees the other's write.
-__device__ __forceinline__ int r_release(const RepairParams& p, RowState& S, const uint32_t* a, int n, int k, int nv,
+template <class St>
+__device__ __forceinline__ int r_release(const RepairParams& p, St& S, const uint32_t* a, int n, int k, int nv,
                                          int cap) {
     int support = 0;
     for (int e = (int)(threadIdx.x & 31u); e < n && !vld(&S.abort); e += 32) {
@@ -196,7 +211,8 @@ __device__ __forceinline__ int r_release(const RepairParams& p, RowState& S, con
 
 // Converged warp: takes a queued slot; false when the row is finished or
 // abandoned.
-__device__ bool r_take(const RepairParams& p, RowState& S, unsigned* slot) {
+template <class St>
+__device__ bool r_take(const RepairParams& p, St& S, unsigned* slot) {
     const unsigned lane = threadIdx.x & 31u;
     int state = 0;
     unsigned got = 0;
@@ -233,9 +249,13 @@ __device__ bool r_take(const RepairParams& p, RowState& S, unsigned* slot) {
 }
 
 __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
+    if (p.run && !*p.run) return;
+    if (p.R_dev) p.R = *p.R_dev;
+    if (p.n_leave_dev) p.n_leave = *p.n_leave_dev;
     extern __shared__ __align__(16) unsigned char s_raw[];
     RowState& S = *reinterpret_cast<RowState*>(s_raw);
     const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const unsigned long long t_start = gtimer();
     int* ho = S.hist[wib][0];
     int* hi_ = S.hist[wib][1];
     for (;;) {
@@ -289,6 +309,7 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
             // ---- drain
             unsigned slot;
             while (r_take(p, S, &slot)) {
+                if (lane == 0 && p.deadline_ns && gtimer() - t_start > p.deadline_ns) atomicExch(&S.abort, 1);
                 const uint32_t x = vldu(&S.key[slot]);
                 int cap = vld(&S.cur[slot]);
                 if (cap == kUnset) cap = sky_at(p, x, k);
@@ -426,6 +447,356 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// insertions
+// ---------------------------------------------------------------------------
+// Inserting edges (and vertices joining C_k because their kmax rose) can only
+// raise row values.  Row k is repaired after row k-1 (one block takes the rows
+// in order), because the new row k-1 bounds the new row k from above:
+//
+//   region   grown from the seeds -- endpoints of inserted edges with both
+//            ends in C_k, and the vertices that joined C_k -- along edges
+//            (either direction) to every member w with
+//                old_k(w) < bound(x)   for a region vertex x next to it, and
+//                old_k(w) < new row_{k-1}(w)   (w could rise at all);
+//            each region vertex starts at its bound, new row_{k-1}
+//   refine   the greatest fixpoint below the bounds, as for deletions, with
+//            every vertex outside the region fixed at its old value
+//
+// Why the region holds every vertex that rises: let w rise to L > old_k(w).
+// In the new (k, L)-core, the vertices that were not in the old one split
+// into groups joined by edges; a group without a seed would, with the old
+// (k, L)-core, already satisfy the (k, L) conditions in the old graph (its
+// members' edges are all old and reach no other group), so it would have
+// been in the old core.  Hence a path of risen vertices joins w to a seed,
+// and every step of it passes the two conditions above (each of them ends at
+// or above L, started below L, and is bounded by its new row k-1).  The
+// refinement then starts at or above every new value and stops at the
+// greatest fixpoint, which is the new row.
+constexpr int kIThreads = 512;
+constexpr int kIWarps = kIThreads / 32;
+
+struct InsState {
+    RowStateT<kIWarps> S;
+    uint32_t pkey[kHash];  // the previous row's region (slots as S.key had them)
+    int pval[kHash];       // and its new values in that row
+    unsigned long long scanned;  // list entries read, all rows
+    unsigned pused;        // entries of the previous row's region
+};
+
+// New row-(k-1) value of a member w of C_k: the previous row's region holds
+// every value that rose there; row 0 is the updated row-0 array.
+__device__ __forceinline__ int prev_val(const RepairParams& p, const InsState& I, uint32_t w, int k) {
+    if (k == 1) return p.row0_new[w];
+    if (I.pused) {
+        unsigned i = hslot0(w) & (kHash - 1);
+        for (int probe = 0; probe < kHash; ++probe) {
+            const uint32_t key = I.pkey[i];
+            if (key == w) return I.pval[i];
+            if (key == kEmptyKey) break;
+            i = (i + 1) & (kHash - 1);
+        }
+    }
+    return sky_at(p, w, k - 1);
+}
+
+// Row-k value of w before the batch; -1 when w was outside C_k.
+__device__ __forceinline__ int old_val(const RepairParams& p, uint32_t w, int k) {
+    return p.kmax_old[w] >= k ? sky_at(p, w, k) : -1;
+}
+
+// Adds w to the region with bound u (once) and queues it for expansion.
+__device__ __forceinline__ void ins_add(InsState& I, uint32_t w, int u) {
+    auto& S = I.S;
+    const int slot = h_slot(S, w, true);
+    if (slot < 0) return;
+    if (atomicCAS(&S.st[slot], 0u, 1u) == 0u) {
+        atomicExch(&S.cur[slot], u);
+        __threadfence_block();
+        enqueue(S, (unsigned)slot);
+    }
+}
+
+// Converged warp, after x fell from cap to nv: queues the region members of
+// a list whose value lies in (nv, cap]; returns how many neighbours in C_k
+// hold at least nv (read after the write, as in r_release).
+template <class St>
+__device__ __forceinline__ int r_release_region(const RepairParams& p, St& S, const uint32_t* a, int n, int k, int nv,
+                                                int cap) {
+    int support = 0;
+    for (int e = (int)(threadIdx.x & 31u); e < n && !vld(&S.abort); e += 32) {
+        const uint32_t w = a[e];
+        if (p.kmax_new[w] < k) continue;
+        const int sl = h_slot(S, w, false);
+        int x = sl >= 0 ? vld(&S.cur[sl]) : kUnset;
+        if (x == kUnset) x = sky_at(p, w, k);
+        support += x >= nv;
+        if (sl >= 0 && x > nv && x <= cap) {
+            const unsigned o = atomicCAS(&S.st[sl], 0u, 1u);
+            if (o == 0u) enqueue(S, (unsigned)sl);
+            else if (o == 1u) atomicCAS(&S.st[sl], 1u, 2u);
+        }
+    }
+#pragma unroll
+    for (int s = 16; s; s >>= 1) support += __shfl_xor_sync(0xFFFFFFFFu, support, s);
+    return support;
+}
+
+// Converged warp: largest L <= cap with #{out-nbrs in C_k at >= L} >= L and
+// #{in-nbrs in C_k at >= L} >= k, by 64-value windows from the top.
+template <class St>
+__device__ int r_eval(const RepairParams& p, St& S, uint32_t x, int k, int cap, int* ho, int* hi_) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t* ao = p.out_nbr + p.out_off[x];
+    const uint32_t* ai = p.in_nbr + p.in_off[x];
+    const int no = p.out_len[x], ni = p.in_len[x];
+    int carry_o = 0, carry_i = 0, hi = cap;
+    bool first = true;
+    for (;;) {
+        const int lo = max(0, hi - (kRWin - 1));
+        ho[lane] = 0;
+        ho[lane + 32] = 0;
+        hi_[lane] = 0;
+        hi_[lane + 32] = 0;
+        __syncwarp();
+        r_hist(p, S, ao, no, k, lo, hi, first, ho);
+        r_hist(p, S, ai, ni, k, lo, hi, first, hi_);
+        __syncwarp();
+        int found = -1;
+        if (lane == 0) {
+            for (int L = hi; L >= lo; --L) {
+                carry_o += ho[L - lo];
+                carry_i += hi_[L - lo];
+                if (carry_o >= L && carry_i >= k) {
+                    found = L;
+                    break;
+                }
+            }
+        }
+        found = __shfl_sync(0xFFFFFFFFu, found, 0);
+        carry_o = __shfl_sync(0xFFFFFFFFu, carry_o, 0);
+        carry_i = __shfl_sync(0xFFFFFFFFu, carry_i, 0);
+        __syncwarp();
+        if (found >= 0) return found;
+        if (lo == 0) return 0;  // a member keeps at least 0
+        hi = lo - 1;
+        first = false;
+    }
+}
+
+__global__ void __launch_bounds__(kIThreads) k_row_repair_ins(RepairParams p) {
+    if (p.run && !*p.run) return;
+    if (p.R_dev) p.R = *p.R_dev;
+    if (p.n_leave_dev) p.n_leave = *p.n_leave_dev;
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    InsState& I = *reinterpret_cast<InsState*>(s_raw);
+    auto& S = I.S;
+    const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    int* ho = S.hist[wib][0];
+    int* hi_ = S.hist[wib][1];
+    const unsigned long long t_start = gtimer();
+    for (int i = threadIdx.x; i < kHash; i += kIThreads) {
+        S.key[i] = kEmptyKey;
+        S.cur[i] = kUnset;
+        S.st[i] = 0;
+        S.ring[i] = kEmptySlot;
+    }
+    if (threadIdx.x == 0) {
+        S.used = 0;
+        S.abort = 0;
+        I.scanned = 0;
+        I.pused = 0;
+    }
+    for (int k = 1; k <= p.R; ++k) {
+        __syncthreads();
+        if (threadIdx.x == 0 && ld_vol(&p.ctl->error)) S.abort = 1;
+        __syncthreads();
+        if (S.abort) break;
+        if (S.used) {  // the last row left entries: clear the table
+            __syncthreads();
+            for (int i = threadIdx.x; i < kHash; i += kIThreads) {
+                S.key[i] = kEmptyKey;
+                S.cur[i] = kUnset;
+                S.st[i] = 0;
+                S.ring[i] = kEmptySlot;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            S.qhead = S.qtail = S.used = 0;
+            S.out = 1;  // held by the seeding phase
+            S.k = k;
+        }
+        __syncthreads();
+        // ---- seeds: inserted edges inside C_k, vertices that joined C_k
+        for (uint32_t i = threadIdx.x; i < p.n_del && !vld(&S.abort); i += kIThreads) {
+            const uint32_t a = p.del_u[i], b = p.del_v[i];
+            if (p.kmax_new[a] < k || p.kmax_new[b] < k) continue;
+            int u = prev_val(p, I, a, k);
+            if (u > old_val(p, a, k)) ins_add(I, a, u);
+            u = prev_val(p, I, b, k);
+            if (u > old_val(p, b, k)) ins_add(I, b, u);
+        }
+        for (uint32_t i = threadIdx.x; i < p.n_leave && !vld(&S.abort); i += kIThreads) {
+            const uint32_t x = p.leave[i];
+            if (p.kmax_old[x] < k && p.kmax_new[x] >= k) ins_add(I, x, prev_val(p, I, x, k));
+        }
+        __syncthreads();
+        if (S.used == 0) {
+            // nothing can rise in this row; the next row reads the old row
+            if (threadIdx.x == 0) I.pused = 0;
+            continue;
+        }
+        // ---- region: expand from every queued vertex
+        if (threadIdx.x == 0) atomicSub(&S.out, 1);
+        __syncthreads();
+        unsigned slot;
+        while (r_take(p, S, &slot)) {
+            const uint32_t x = vldu(&S.key[slot]);
+            const int t = vld(&S.cur[slot]);
+            for (int side = 0; side < 2; ++side) {
+                const uint32_t* a = side ? p.in_nbr + p.in_off[x] : p.out_nbr + p.out_off[x];
+                const int n = side ? p.in_len[x] : p.out_len[x];
+                for (int e = (int)lane; e < n && !vld(&S.abort); e += 32) {
+                    const uint32_t w = a[e];
+                    if (p.kmax_new[w] < k || h_slot(S, w, false) >= 0) continue;
+                    const int o = old_val(p, w, k);
+                    if (o >= t) continue;
+                    const int u = prev_val(p, I, w, k);
+                    if (u > o) ins_add(I, w, u);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                atomicAdd(&I.scanned, (unsigned long long)(p.out_len[x] + p.in_len[x]));
+                if (p.deadline_ns && gtimer() - t_start > p.deadline_ns) atomicExch(&S.abort, 1);
+                __threadfence_block();
+                atomicSub(&S.out, 1);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        if (S.abort) break;
+        // ---- refinement from the bounds: queue the whole region
+        if (threadIdx.x == 0) {
+            S.qhead = S.qtail = 0;
+            S.out = 1;
+        }
+        for (int i = threadIdx.x; i < kHash; i += kIThreads) {
+            S.ring[i] = kEmptySlot;
+            S.st[i] = 0;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kHash; i += kIThreads)
+            if (S.key[i] != kEmptyKey) {
+                S.st[i] = 1u;
+                enqueue(S, (unsigned)i);
+            }
+        for (int sweep = 0;; ++sweep) {
+            __syncthreads();
+            if (threadIdx.x == 0) atomicSub(&S.out, 1);
+            __syncthreads();
+            while (r_take(p, S, &slot)) {
+                const uint32_t x = vldu(&S.key[slot]);
+                const int cap = vld(&S.cur[slot]);
+                const int nv = cap >= 1 ? r_eval(p, S, x, k, cap, ho, hi_) : cap;
+                if (nv < cap) {
+                    if (lane == 0) atomicExch(&S.cur[slot], nv);
+                    __syncwarp();
+                    __threadfence_block();
+                    const int so = r_release_region(p, S, p.out_nbr + p.out_off[x], p.out_len[x], k, nv, cap);
+                    const int si = r_release_region(p, S, p.in_nbr + p.in_off[x], p.in_len[x], k, nv, cap);
+                    if (lane == 0 && nv >= 1 && (so < nv || si < k)) atomicCAS(&S.st[slot], 1u, 2u);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    atomicAdd(&I.scanned, 2ull * (unsigned long long)(p.out_len[x] + p.in_len[x]));
+                    if (p.deadline_ns && gtimer() - t_start > p.deadline_ns) atomicExch(&S.abort, 1);
+                    if (atomicCAS(&S.st[slot], 1u, 0u) == 2u) {
+                        atomicExch(&S.st[slot], 1u);
+                        enqueue(S, slot);
+                    }
+                    __threadfence_block();
+                    atomicSub(&S.out, 1);
+                }
+                __syncwarp();
+            }
+            __syncthreads();
+            if (S.abort) break;
+            if (sweep == 32) {  // bounded: a row that keeps failing is recomputed
+                if (threadIdx.x == 0) S.abort = 1;
+                __syncthreads();
+                break;
+            }
+            // ---- the row is quiet: every region vertex must hold its value
+            // against the final values; queue any that does not, drain again
+            if (threadIdx.x == 0) {
+                S.qhead = S.qtail = 0;
+                S.out = 1;  // held by the sweep
+                S.k = 0;    // vertices found unstable
+            }
+            for (int i = threadIdx.x; i < kHash; i += kIThreads) S.ring[i] = kEmptySlot;
+            __syncthreads();
+            for (int i = wib; i < kHash; i += kIWarps) {
+                const uint32_t x = S.key[i];
+                if (x == kEmptyKey) continue;
+                const int val = S.cur[i];
+                if (val < 1) continue;
+                int so = 0, si = 0;
+                const uint32_t* ao = p.out_nbr + p.out_off[x];
+                const uint32_t* ai = p.in_nbr + p.in_off[x];
+                for (int e = (int)lane; e < p.out_len[x]; e += 32) so += rv(p, S, ao[e], k) >= val;
+                for (int e = (int)lane; e < p.in_len[x]; e += 32) si += rv(p, S, ai[e], k) >= val;
+#pragma unroll
+                for (int s = 16; s; s >>= 1) {
+                    so += __shfl_xor_sync(0xFFFFFFFFu, so, s);
+                    si += __shfl_xor_sync(0xFFFFFFFFu, si, s);
+                }
+                if (lane == 0 && (so < val || si < k)) {
+                    atomicAdd(&S.k, 1);
+                    const unsigned o = atomicCAS(&S.st[i], 0u, 1u);
+                    if (o == 0u) enqueue(S, (unsigned)i);
+                }
+            }
+            __syncthreads();
+            const bool again = S.k != 0;
+            __syncthreads();
+            if (threadIdx.x == 0) S.k = k;
+            if (!again) {
+                __syncthreads();
+                break;
+            }
+        }
+        __syncthreads();
+        if (S.abort) break;
+        // ---- values that differ from the old skyline's reading go to the
+        // log (a vertex that joined C_k is read as its last old corner,
+        // which is how the merged skyline reads rows above its old kmax);
+        // the region becomes the next row's "previous row"
+        for (int i = threadIdx.x; i < kHash; i += kIThreads) {
+            const uint32_t v = S.key[i];
+            const int c = S.cur[i];
+            I.pkey[i] = v;
+            I.pval[i] = c;
+            if (v == kEmptyKey || c == sky_at(p, v, k)) continue;
+            const unsigned long long li = atomicAdd(&p.ctl->log_count, 1u);
+            if (li < p.log_cap) {
+                p.log_v[li] = v;
+                p.log_k[li] = k;
+                p.log_l[li] = c;
+            } else {
+                set_dev_error(p.ctl, DC_DEV_ERR_CAPACITY, 45);
+            }
+        }
+        if (threadIdx.x == 0) I.pused = S.used;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (S.abort && !ld_vol(&p.ctl->error)) set_dev_error(p.ctl, DC_DEV_ERR_CAPACITY, 44);
+        p.ctl->edges_scanned = I.scanned;
+    }
+}
+
 // Work of a repair: sum over the endpoints x of the deleted edges of
 // deg(x) * kmax(x), the list entries a row-by-row repair scans at least once.
 __global__ void k_repair_work(uint32_t n, const uint32_t* u, const uint32_t* v, const int32_t* kmax,
@@ -441,19 +812,27 @@ __global__ void k_repair_work(uint32_t n, const uint32_t* u, const uint32_t* v, 
     if ((threadIdx.x & 31u) == 0) atomicAdd(acc, w);
 }
 
-// Vertices whose kmax fell (kmax_new < kmax_old), compacted.
-__global__ void k_collect_leave(uint32_t V, const int32_t* kold, const int32_t* knew, uint32_t* out, unsigned* n) {
+// Vertices whose kmax fell (rise = false) or rose (rise = true), compacted.
+__global__ void k_collect_leave(uint32_t V, const int32_t* kold, const int32_t* knew, uint32_t* out, unsigned* n,
+                                bool rise) {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
-        if (knew[v] < kold[v]) out[atomicAdd(n, 1u)] = (uint32_t)v;
+        if (rise ? knew[v] > kold[v] : knew[v] < kold[v]) out[atomicAdd(n, 1u)] = (uint32_t)v;
 }
 
-// Per-vertex change lists from the log: count, fill, sort by k.
-__global__ void k_chg_count(unsigned long long n, const uint32_t* lv, unsigned long long* cnt) {
+// Per-vertex change lists from the log: count, fill, sort by k.  Captured
+// batches read n on the device (n_dev) and act only while *run != 0.
+__global__ void k_chg_count(unsigned long long n, const uint32_t* lv, unsigned long long* cnt,
+                            const unsigned long long* n_dev, const int* run) {
+    if (run && !*run) return;
+    if (n_dev) n = *n_dev;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         atomicAdd(&cnt[lv[i]], 1ull);
 }
 __global__ void k_chg_fill(unsigned long long n, const uint32_t* lv, const int32_t* lk, const int32_t* ll,
-                           const unsigned long long* off, uint32_t* fill, int32_t* ck, int32_t* cl) {
+                           const unsigned long long* off, uint32_t* fill, int32_t* ck, int32_t* cl,
+                           const unsigned long long* n_dev, const int* run) {
+    if (run && !*run) return;
+    if (n_dev) n = *n_dev;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t v = lv[i];
         uint64_t o = off[v] + atomicAdd(&fill[v], 1u);
@@ -461,7 +840,9 @@ __global__ void k_chg_fill(unsigned long long n, const uint32_t* lv, const int32
         cl[o] = ll[i];
     }
 }
-__global__ void k_chg_sort(uint32_t V, const unsigned long long* off, int32_t* ck, int32_t* cl, uint32_t* off32) {
+__global__ void k_chg_sort(uint32_t V, const unsigned long long* off, int32_t* ck, int32_t* cl, uint32_t* off32,
+                           const int* run) {
+    if (run && !*run) return;
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t a = off[v], b = off[v + 1];
         for (uint64_t i = a + 1; i < b; ++i) {
@@ -488,7 +869,8 @@ template <bool FILL>
 __global__ void k_rep_merge(uint32_t V, const int32_t* kmax, const int32_t* row0, const uint32_t* ooff,
                             const int32_t* ok, const int32_t* ol, const uint32_t* coff, const int32_t* ck,
                             const int32_t* cl, unsigned long long* cnt_off, int32_t* nk, int32_t* nl,
-                            uint32_t* noff) {
+                            uint32_t* noff, const int* run) {
+    if (run && !*run) return;
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
         const int km = kmax[v];
         uint32_t i = ooff[v], ie = ooff[v + 1];
@@ -503,7 +885,9 @@ __global__ void k_rep_merge(uint32_t V, const int32_t* kmax, const int32_t* row0
         ++c;
         int oldv = (i < ie) ? ol[i] : 0;  // old row-0 corner
         ++i;
-        int after = 0x7FFFFFFF;  // row after a change run
+        // row after a change run; a changed row 0 is one (an unchanged row 1
+        // keeps its old value, which may now differ from row 0)
+        int after = oldv != last ? 1 : 0x7FFFFFFF;
         for (;;) {
             int kc = 0x7FFFFFFF;
             if (i < ie) kc = min(kc, ok[i]);
@@ -580,28 +964,10 @@ bool row_repair_worthwhile(dc_graph* h, const uint32_t* d_u, const uint32_t* d_v
         }                                                                                   \
     } while (0)
 
-// Rows 1..R after a deletion-only batch (graph, kmax and row 0 already
-// updated; kmax before the batch in scratch kmax_old).  Replaces the skyline
-// and sets *applied; leaves everything untouched with *applied = false when a
-// row touched more vertices than a block's table holds or the change log ran
-// out (the caller then recomputes the rows).
-int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_dv, uint32_t n_del, bool* applied) {
-    *applied = false;
-    DevGraph& g = h->g;
-    Decomp& d = h->d;
+// The change log of a repair: the scratch corner log (sized by the last
+// decomposition), at least 2^20 entries.
+static int ensure_change_log(dc_graph* h, uint64_t* cap_out) {
     Scratch* s = h->scratch;
-    const uint32_t V = g.V;
-    if (R < 1 || V == 0) return DC_OK;
-    if (2ull * n_del > kHashLimit) return DC_OK;  // the seeds alone overflow a row's table
-    unsigned* n_leave_d = (unsigned*)s->cursor;
-    RP_CUDA(cudaMemsetAsync(n_leave_d, 0, sizeof(unsigned), h->stream));
-    ++g_launches;
-    k_collect_leave<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, s->kmax_old, d.kmax_v, s->rem0, n_leave_d);
-    unsigned n_leave = 0;
-    RP_CUDA(cudaMemcpyAsync(&n_leave, n_leave_d, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
-    RP_CUDA(cudaStreamSynchronize(h->stream));
-    if (2ull * n_del + n_leave > kHashLimit) return DC_OK;
-    // change log: the scratch corner log (sized by the last decomposition)
     uint64_t cap = s->log_cap;
     if (cap < (1u << 20)) {
         cudaFreeAsync(s->log_v, h->stream);
@@ -620,35 +986,18 @@ int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_
         }
         s->log_cap = cap;
     }
-    RP_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
-    if (h->wait_ns)
-        RP_CUDA(cudaMemcpyAsync(&h->ctl->wait_ns, &h->wait_ns, sizeof(h->wait_ns), cudaMemcpyHostToDevice, h->stream));
-    RP_CUDA(cudaStreamSynchronize(h->stream));
-    RepairParams p;
-    p.V = V;
-    p.out_off = g.out_off; p.out_len = g.out_len; p.out_nbr = g.out_nbr;
-    p.in_off = g.in_off; p.in_len = g.in_len; p.in_nbr = g.in_nbr;
-    p.kmax_new = d.kmax_v;
-    p.kmax_old = s->kmax_old;
-    p.sky_off = d.sky_off; p.sky_k = d.sky_k; p.sky_l = d.sky_l;
-    p.del_u = d_du; p.del_v = d_dv; p.n_del = n_del;
-    p.leave = s->rem0; p.n_leave = n_leave;
-    p.R = R;
-    p.log_v = s->log_v; p.log_k = s->log_k; p.log_l = s->log_l; p.log_cap = cap;
-    p.ctl = h->ctl;
-    static_assert(sizeof(RowState) <= 200 * 1024, "row table exceeds shared memory");
-    RP_CUDA(cudaFuncSetAttribute(k_row_repair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RowState)));
-    const int blocks = std::max(1, std::min<int>(R, h->geom.sms));
-    ++g_launches;
-    k_row_repair<<<blocks, kRThreads, sizeof(RowState), h->stream>>>(p);
-    RP_CUDA(cudaGetLastError());
-    EngineCtl hc;
-    RP_CUDA(cudaMemcpyAsync(&hc, h->ctl, sizeof(EngineCtl), cudaMemcpyDeviceToHost, h->stream));
-    RP_CUDA(cudaStreamSynchronize(h->stream));
-    if (hc.error & DC_DEV_ERR_TIMEOUT)
-        return set_error(DC_ERR_TIMEOUT, "row repair: bounded device wait expired (site %u)", hc.err_where);
-    if (hc.error) return DC_OK;  // capacity: the caller recomputes the rows
-    const uint64_t nlog = hc.log_count;
+    *cap_out = cap;
+    return DC_OK;
+}
+
+// Merges the change log (v, k, new value) of a repair with the current
+// skyline into the new skyline (kmax and row 0 already updated) and makes it
+// current; *applied tells whether it did.
+int apply_change_log(dc_graph* h, uint64_t nlog, bool* applied) {
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
     // per-vertex change lists
     // the change lists go to spare skyline slot 0 and the merged skyline to
     // slot 1 (no allocation once the slots have grown to the graph's size)
@@ -662,17 +1011,18 @@ int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_
         cudaMemsetAsync(cnt, 0, 8ull * (V + 1), h->stream);
         cudaMemsetAsync(fill, 0, 4ull * V, h->stream);
         g_launches += 3;
-        if (nlog) k_chg_count<<<rgrid(h, nlog), kRThreads, 0, h->stream>>>(nlog, s->log_v, cnt);
+        if (nlog) k_chg_count<<<rgrid(h, nlog), kRThreads, 0, h->stream>>>(nlog, s->log_v, cnt, nullptr, nullptr);
         rc = scan_tmp64(h, V);
     }
     if (rc == DC_OK) {
         if (nlog)
             k_chg_fill<<<rgrid(h, nlog), kRThreads, 0, h->stream>>>(nlog, s->log_v, s->log_k, s->log_l, cnt, fill, ck,
-                                                                    cl);
-        k_chg_sort<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, cnt, ck, cl, coff);
+                                                                    cl, nullptr, nullptr);
+        k_chg_sort<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, cnt, ck, cl, coff, nullptr);
         // new skyline: count, scan, fill
         k_rep_merge<false><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
-                                                                     coff, ck, cl, cnt, nullptr, nullptr, nullptr);
+                                                                     coff, ck, cl, cnt, nullptr, nullptr, nullptr,
+                                                                     nullptr);
         rc = scan_tmp64(h, V);
     }
     if (rc == DC_OK) {
@@ -686,7 +1036,7 @@ int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_
     if (rc == DC_OK) {
         ++g_launches;
         k_rep_merge<true><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
-                                                                    coff, ck, cl, cnt, nk, nl, noff);
+                                                                    coff, ck, cl, cnt, nk, nl, noff, nullptr);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(DC_ERR_CUDA, "row repair: merge launch failed");
     }
     if (coff || ck) sky_put_spare(h, 0, coff, ck, cl, ccap);
@@ -703,6 +1053,128 @@ int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_
     d.corner_cap = ncap;
     *applied = true;
     return DC_OK;
+}
+
+// Rows 1..R after a deletion-only batch (graph, kmax and row 0 already
+// updated; kmax before the batch in scratch kmax_old).  Replaces the skyline
+// and sets *applied; leaves everything untouched with *applied = false when a
+// row touched more vertices than a block's table holds or the change log ran
+// out (the caller then recomputes the rows).
+int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_dv, uint32_t n_del,
+                unsigned long long deadline_ns, bool* applied) {
+    *applied = false;
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    if (R < 1 || V == 0) return DC_OK;
+    if (2ull * n_del > kHashLimit) return DC_OK;  // the seeds alone overflow a row's table
+    unsigned* n_leave_d = (unsigned*)s->cursor;
+    RP_CUDA(cudaMemsetAsync(n_leave_d, 0, sizeof(unsigned), h->stream));
+    ++g_launches;
+    k_collect_leave<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, s->kmax_old, d.kmax_v, s->rem0, n_leave_d, false);
+    unsigned n_leave = 0;
+    RP_CUDA(cudaMemcpyAsync(&n_leave, n_leave_d, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    RP_CUDA(cudaStreamSynchronize(h->stream));
+    if (2ull * n_del + n_leave > kHashLimit) return DC_OK;
+    uint64_t cap = 0;
+    if (int rc = ensure_change_log(h, &cap)) return rc;
+    RP_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
+    if (h->wait_ns)
+        RP_CUDA(cudaMemcpyAsync(&h->ctl->wait_ns, &h->wait_ns, sizeof(h->wait_ns), cudaMemcpyHostToDevice, h->stream));
+    RP_CUDA(cudaStreamSynchronize(h->stream));
+    RepairParams p;
+    p.V = V;
+    p.out_off = g.out_off; p.out_len = g.out_len; p.out_nbr = g.out_nbr;
+    p.in_off = g.in_off; p.in_len = g.in_len; p.in_nbr = g.in_nbr;
+    p.kmax_new = d.kmax_v;
+    p.kmax_old = s->kmax_old;
+    p.sky_off = d.sky_off; p.sky_k = d.sky_k; p.sky_l = d.sky_l;
+    p.del_u = d_du; p.del_v = d_dv; p.n_del = n_del;
+    p.leave = s->rem0; p.n_leave = n_leave;
+    p.row0_new = nullptr;
+    p.deadline_ns = deadline_ns;
+    p.R = R;
+    p.R_dev = nullptr;
+    p.n_leave_dev = nullptr;
+    p.run = nullptr;
+    p.log_v = s->log_v; p.log_k = s->log_k; p.log_l = s->log_l; p.log_cap = cap;
+    p.ctl = h->ctl;
+    static_assert(sizeof(RowState) <= 200 * 1024, "row table exceeds shared memory");
+    RP_CUDA(cudaFuncSetAttribute(k_row_repair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RowState)));
+    const int blocks = std::max(1, std::min<int>(R, h->geom.sms));
+    ++g_launches;
+    k_row_repair<<<blocks, kRThreads, sizeof(RowState), h->stream>>>(p);
+    RP_CUDA(cudaGetLastError());
+    EngineCtl hc;
+    RP_CUDA(cudaMemcpyAsync(&hc, h->ctl, sizeof(EngineCtl), cudaMemcpyDeviceToHost, h->stream));
+    RP_CUDA(cudaStreamSynchronize(h->stream));
+    if (hc.error & DC_DEV_ERR_TIMEOUT)
+        return set_error(DC_ERR_TIMEOUT, "row repair: bounded device wait expired (site %u)", hc.err_where);
+    if (hc.error) return DC_OK;  // capacity: the caller recomputes the rows
+    return apply_change_log(h, hc.log_count, applied);
+}
+
+// Largest insertion batch whose seeds fit a row's table.
+uint32_t row_repair_max_insertions() { return kHashLimit / 4; }
+
+// Rows 1..R after an insertion-only batch (graph, kmax and row 0 already
+// updated; kmax before the batch in scratch kmax_old).  Replaces the skyline
+// and sets *applied; leaves everything untouched with *applied = false when a
+// row's region outgrew the table, the repair ran past deadline_ns (the
+// recomputation is then expected to be cheaper), or the change log ran out.
+// *scanned: list entries the repair read.
+int rows_repair_ins(dc_graph* h, int32_t R, const uint32_t* d_iu, const uint32_t* d_iv, uint32_t n_ins,
+                    unsigned long long deadline_ns, bool* applied, unsigned long long* scanned) {
+    *applied = false;
+    *scanned = 0;
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    if (R < 1 || V == 0) return DC_OK;
+    if (2ull * n_ins > kHashLimit) return DC_OK;
+    unsigned* n_join_d = (unsigned*)s->cursor;
+    RP_CUDA(cudaMemsetAsync(n_join_d, 0, sizeof(unsigned), h->stream));
+    ++g_launches;
+    k_collect_leave<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, s->kmax_old, d.kmax_v, s->rem0, n_join_d, true);
+    unsigned n_join = 0;
+    RP_CUDA(cudaMemcpyAsync(&n_join, n_join_d, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    RP_CUDA(cudaStreamSynchronize(h->stream));
+    if (2ull * n_ins + n_join > kHashLimit) return DC_OK;
+    uint64_t cap = 0;
+    if (int rc = ensure_change_log(h, &cap)) return rc;
+    RP_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), h->stream));
+    if (h->wait_ns)
+        RP_CUDA(cudaMemcpyAsync(&h->ctl->wait_ns, &h->wait_ns, sizeof(h->wait_ns), cudaMemcpyHostToDevice, h->stream));
+    RepairParams p;
+    memset(&p, 0, sizeof(p));
+    p.V = V;
+    p.out_off = g.out_off; p.out_len = g.out_len; p.out_nbr = g.out_nbr;
+    p.in_off = g.in_off; p.in_len = g.in_len; p.in_nbr = g.in_nbr;
+    p.kmax_new = d.kmax_v;
+    p.kmax_old = s->kmax_old;
+    p.sky_off = d.sky_off; p.sky_k = d.sky_k; p.sky_l = d.sky_l;
+    p.del_u = d_iu; p.del_v = d_iv; p.n_del = n_ins;
+    p.leave = s->rem0; p.n_leave = n_join;
+    p.row0_new = d.row0;
+    p.deadline_ns = deadline_ns;
+    p.R = R;
+    p.log_v = s->log_v; p.log_k = s->log_k; p.log_l = s->log_l; p.log_cap = cap;
+    p.ctl = h->ctl;
+    static_assert(sizeof(InsState) <= 227 * 1024, "insertion repair state exceeds shared memory");
+    RP_CUDA(cudaFuncSetAttribute(k_row_repair_ins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InsState)));
+    ++g_launches;
+    k_row_repair_ins<<<1, kIThreads, sizeof(InsState), h->stream>>>(p);
+    RP_CUDA(cudaGetLastError());
+    EngineCtl hc;
+    RP_CUDA(cudaMemcpyAsync(&hc, h->ctl, sizeof(EngineCtl), cudaMemcpyDeviceToHost, h->stream));
+    RP_CUDA(cudaStreamSynchronize(h->stream));
+    *scanned = hc.edges_scanned;
+    if (hc.error & DC_DEV_ERR_TIMEOUT)
+        return set_error(DC_ERR_TIMEOUT, "row repair: bounded device wait expired (site %u)", hc.err_where);
+    if (hc.error) return DC_OK;  // capacity or budget: the caller recomputes the rows
+    return apply_change_log(h, hc.log_count, applied);
 }
 
 }  // namespace dc

@@ -57,7 +57,8 @@ class MaintStats(ctypes.Structure):
                 ("lmax", ctypes.c_int32), ("rows_recomputed", ctypes.c_int32), ("method", ctypes.c_int32),
                 ("rebuilt", ctypes.c_uint32), ("rows_local", ctypes.c_uint32), ("region", ctypes.c_uint64),
                 ("apply_ms", ctypes.c_float), ("core_ms", ctypes.c_float), ("rows_ms", ctypes.c_float),
-                ("total_ms", ctypes.c_float)]
+                ("total_ms", ctypes.c_float), ("del_repair_ms", ctypes.c_float), ("ins_repair_ms", ctypes.c_float),
+                ("ins_scanned", ctypes.c_uint64)]
 
 
 MAINT_AUTO, MAINT_LOCAL, MAINT_REPEEL = 0, 1, 2

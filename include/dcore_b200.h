@@ -224,9 +224,12 @@ typedef struct dc_maint_stats {
     int32_t rows_recomputed;    /* rows 0..R recomputed (R + 1); rows above kept      */
     int32_t method;             /* DC_MAINT_LOCAL or DC_MAINT_REPEEL                  */
     uint32_t rebuilt;           /* 1 when the adjacency store grew (slack exhausted)  */
-    uint32_t rows_local;        /* 1 when rows were repaired locally (deletions only) */
+    uint32_t rows_local;        /* rows repaired in place: bit 0 deletions, bit 1 insertions */
     uint64_t region;            /* vertices visited by the local kmax / row-0 update  */
     float apply_ms, core_ms, rows_ms, total_ms;
+    float del_repair_ms;        /* in-place row repair of the deletions (0: none ran) */
+    float ins_repair_ms;        /* in-place row repair of the insertions (0: none ran) */
+    uint64_t ins_scanned;       /* list entries the insertion repair read             */
 } dc_maint_stats;
 
 /* maintenanceFast (main.cu:1665-1751) / maintenance (main.cu:1536-1663):
@@ -242,26 +245,38 @@ int dc_maintain(dc_graph* g, const uint32_t* pairs, const uint8_t* is_delete, ui
                 dc_maint_stats* stats);
 /* Row maintenance mode (default 1).  Repair: the deletions of a batch are
  * applied first and rows 1..R are repaired in place from their old values,
- * touching only the vertices the deletions reach (a row that touches too many
- * falls back to recomputation); the insertions follow as a second batch whose
- * rows are recomputed from the new row 0.  1: repair when the batch's
- * deletions are few and the lists they touch are short enough that the
- * repair is expected to beat recomputation; 2: repair whenever the deletions
- * fit; 0: every batch recomputes rows 1..R from the new row 0.  Results are
- * identical.  No counterpart in the reference (it re-peels rows k <= M+1,
- * main.cu:1735-1743). */
+ * touching only the vertices the deletions reach; the insertions follow as a
+ * second batch whose rows are repaired in place row after row (values can
+ * only rise: a region grown from the inserted edges and the vertices that
+ * joined C_k, bounded by the new previous row, refined down to the new row).
+ * A repair falls back to recomputing rows 1..R from the new row 0 when a
+ * row's region outgrows a block's table or when it has run as long as that
+ * recomputation is expected to take (the rows phase of the last full
+ * decomposition scaled by R / kmax).  1: repair when the batch has at most
+ * 64 net updates and the lists they touch are short enough that the repair
+ * is expected to beat recomputation; 2: repair whenever the updates fit, with no time
+ * limit; 3: repair whenever the updates fit, within the time limit (the
+ * learned scheduler's incremental path); 0: every batch recomputes rows 1..R
+ * from the new row 0.  Results are identical.  The
+ * reference re-peels rows k <= M+1 (main.cu:1735-1743); its disabled exact
+ * l-list maintenance (kListFindUpperBound / kListRefineHIndex, main.cu:929-1242,
+ * hInIndex src/cuda_utils.cuh:68-77) is the specification this replaces. */
 int dc_set_row_repair(dc_graph* g, int on);
 
 /* ---- learned maintenance scheduler -------------------------------------- */
-/* A BF16 MLP (16 -> 64 -> 64 -> 2, ReLU) predicting the log of the wall time
- * of DC_MAINT_LOCAL (output 0) and DC_MAINT_REPEEL (output 1) from 16
- * features of a batch (dc_maint_log_get lists them); DC_MAINT_AUTO runs the
- * method with the smaller prediction for batches of at most 65,536 net
- * updates (larger ones always re-peel), the rule of thumb (at most 64 net
- * updates: local) when no network is attached.  Either method gives exact
- * results.  Training and inference run
- * in the engine's own CUDA kernels.  No reference counterpart (the reference
- * fixes its batching mode at compile time, src/common.h:18-19). */
+/* A BF16 MLP (16 -> 64 -> 64 -> 2, ReLU) predicting the log of the time of
+ * a batch on each of two paths from 16 features of the batch
+ * (dc_maint_log_get lists them): output 0 the incremental path
+ * (DC_MAINT_LOCAL with rows repaired in place wherever the batch fits, mode 3
+ * of dc_set_row_repair), output 1 the full path (DC_MAINT_REPEEL with rows
+ * 1..R recomputed, mode 0).  DC_MAINT_AUTO runs the path with the smaller
+ * prediction for batches of at most 65,536 net updates (larger ones always
+ * take the full path); with no network attached the rule of thumb decides
+ * (at most 64 net updates: local; rows by the graph's row mode).  Both paths
+ * give exact results.  Training and inference run in the engine's own CUDA
+ * kernels.  No reference counterpart (the reference fixes its batching mode
+ * at compile time, src/common.h:18-19, and always re-peels rows,
+ * main.cu:1735-1743). */
 typedef struct dc_sched dc_sched;
 int dc_sched_create(uint64_t seed, dc_sched** out);
 int dc_sched_free(dc_sched* s);

@@ -51,5 +51,8 @@ def test_delete_every_edge(dc, orc, gpu, mode):
 def test_row_repair_mode_validation(dc, gpu):
     V, s, d = dc.gen_rmat(8, 4, 1)
     with dc.Graph.from_edges(V, s, d) as g:
+        g.set_row_repair(3)  # modes 0..3
         with pytest.raises(dc.DCoreError):
-            g.set_row_repair(3)
+            g.set_row_repair(4)
+        with pytest.raises(dc.DCoreError):
+            g.set_row_repair(-1)

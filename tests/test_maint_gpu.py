@@ -233,3 +233,76 @@ def test_randomized_deletion_heavy_streams(dc, orc, gpu, seed):
             _apply(cnt, u[i:i + bs], v[i:i + bs], dl[i:i + bs])
             _check(orc, g, V, cnt)
             i += bs
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("scale,ef,seed", [(12, 16, 31), (14, 8, 32)])
+def test_insertion_stream_local_row_repair(dc, orc, gpu, method, scale, ef, seed):
+    # insertions only: rows are repaired in place row after row (values can
+    # only rise; the region grows from the inserted edges and the vertices
+    # that joined C_k), every batch checked against a recomputation
+    V, s, d = dc.gen_rmat(scale, ef, seed)
+    sizes = [1, 1, 2, 3, 10, 50, 200, 1000]
+    u, v, dl = dc.gen_updates(V, s, d, sum(sizes), 1.0, seed + 7)
+    assert not dl.any()
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    local = 0
+    with dc.Graph.from_edges(V, s, d) as g:
+        g.set_row_repair(2)  # in place whenever the insertions fit
+        g.decompose()
+        i = 0
+        for bs in sizes:
+            st = g.maintain(u[i:i + bs], v[i:i + bs], dl[i:i + bs], method)
+            local += (st["rows_local"] >> 1) & 1
+            _apply(cnt, u[i:i + bs], v[i:i + bs], dl[i:i + bs])
+            _check(orc, g, V, cnt)
+            i += bs
+    assert local >= len(sizes) // 2  # the in-place path ran
+
+
+def test_insertions_into_the_dense_core(dc, orc, gpu):
+    # edges between high-kmax vertices: kmax rises, vertices join C_k for
+    # high k, and the in-degree condition of whole rows moves
+    V, s, d = dc.gen_rmat(12, 16, 41)
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    km, kmaxes = orc.kmax(V, s, d)
+    top = np.argsort(-kmaxes, kind="stable")[:400].astype(np.uint32)
+    rng = np.random.default_rng(3)
+    pairs = []
+    while len(pairs) < 60:
+        a, b = (int(x) for x in rng.choice(top, 2, replace=False))
+        if (a, b) not in cnt and (a, b) not in pairs:
+            pairs.append((a, b))
+    local = 0
+    with dc.Graph.from_edges(V, s, d) as g:
+        g.set_row_repair(2)
+        g.decompose()
+        for i in range(0, len(pairs), 6):
+            u = np.array([p[0] for p in pairs[i:i + 6]], np.uint32)
+            v = np.array([p[1] for p in pairs[i:i + 6]], np.uint32)
+            z = np.zeros(len(u), np.uint8)
+            st = g.maintain(u, v, z, 1)
+            local += (st["rows_local"] >> 1) & 1
+            _apply(cnt, u, v, z)
+            _check(orc, g, V, cnt)
+    assert local > 0
+
+
+@pytest.mark.parametrize("seed", range(1, 13))
+def test_randomized_insertion_heavy_streams(dc, orc, gpu, seed):
+    # random graphs, batch sizes, methods and row modes, mostly insertions
+    rng = np.random.default_rng(100 + seed)
+    V, s, d = dc.gen_rmat(int(rng.integers(10, 14)), int(rng.choice([8, 16])), seed)
+    sizes = [int(x) for x in rng.integers(1, 400, 4)]
+    u, v, dl = dc.gen_updates(V, s, d, sum(sizes), float(rng.choice([1.0, 0.7])), seed + 60)
+    method = int(rng.choice(METHODS))
+    cnt = Counter(zip(s.tolist(), d.tolist()))
+    with dc.Graph.from_edges(V, s, d) as g:
+        g.set_row_repair(int(rng.choice([1, 2])))
+        g.decompose()
+        i = 0
+        for bs in sizes:
+            g.maintain(u[i:i + bs], v[i:i + bs], dl[i:i + bs], method)
+            _apply(cnt, u[i:i + bs], v[i:i + bs], dl[i:i + bs])
+            _check(orc, g, V, cnt)
+            i += bs
