@@ -428,6 +428,7 @@ def run_maintenance(args, w, rank, world, local):
         methods = []
         local_rows = 0
         local_ins = 0
+        captured = 0
         detail = []
         for _ in range(nb):
             st = g.maintain(u[pos:pos + bs], v[pos:pos + bs], dl[pos:pos + bs], args.maint_method)
@@ -440,16 +441,19 @@ def run_maintenance(args, w, rank, world, local):
             detail.append([round(st["total_ms"], 2), round(st["apply_ms"], 2), round(st["core_ms"], 2),
                            round(st["rows_ms"], 2), st["rows_recomputed"], st["rows_local"], st["method"],
                            st["rebuilt"], round(st["del_repair_ms"], 2), round(st["ins_repair_ms"], 2),
-                           st["ins_scanned"]])
+                           st["ins_scanned"], st["captured"]])
+            captured += st["captured"]
             pos += bs
         lat = np.array(lat)
         per_size[str(bs)] = {"batches": nb, "updates_per_s": bs * nb / (lat.sum() / 1000.0),
                              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                              "methods": {"local": methods.count(1), "repeel": methods.count(2)},
                              "rows_repaired_in_place": {"deletions": local_rows, "insertions": local_ins},
+                             "captured_graph_batches": captured,
                              "batch_detail": {"fields": ["total_ms", "apply_ms", "core_ms", "rows_ms",
                                                          "rows_recomputed", "rows_repaired", "method", "rebuilt",
-                                                         "del_repair_ms", "ins_repair_ms", "ins_scanned"],
+                                                         "del_repair_ms", "ins_repair_ms", "ins_scanned",
+                                                         "captured"],
                                               "batches": detail}}
     clocks = sampler.stop()
     launches = dc.launch_count() - launches0

@@ -224,6 +224,7 @@ extern "C" int dc_graph_free(dc_graph* h) {
     free_graph_arrays(h->g, h->stream);
     free_decomp(h->d, h->stream);
     free_scratch(h);
+    dc::free_captured_batches(h);
     if (h->ctl) cudaFreeAsync(h->ctl, h->stream);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& e : h->ev)
@@ -348,6 +349,12 @@ extern "C" int dc_set_row_repair(dc_graph* h, int on) {
     if (!h) return set_error(DC_ERR_INVALID, "null graph");
     if (on < 0 || on > 3) return set_error(DC_ERR_INVALID, "dc_set_row_repair: mode must be 0, 1, 2 or 3");
     h->row_repair = on;
+    return DC_OK;
+}
+
+extern "C" int dc_set_captured_batches(dc_graph* h, int on) {
+    if (!h) return set_error(DC_ERR_INVALID, "null graph");
+    h->captured_batches = on != 0;
     return DC_OK;
 }
 

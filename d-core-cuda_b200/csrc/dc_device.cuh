@@ -90,6 +90,26 @@ struct EngineCtl {
     int test_skip_block;
 };
 
+// Decisions and results of one maintenance batch run as a captured CUDA
+// graph: every branch the host-driven batch takes between its kernels is
+// taken on the device, by small kernels writing these fields, and the
+// kernels after a branch act only while their run flag is set.
+struct BatchStatus {
+    int run_apply;      // the batch is valid: no missing deletion, insertions fit their free slots
+    int run_repair;     // rows 1..R are repaired in place
+    int run_merge;      // a new skyline is merged (the repair's changes, or new row-0 corners only)
+    int fallback;       // rows 1..R must be recomputed (repair not expected to pay, or it gave up)
+    int merge_overflow; // the merged skyline outgrew its buffer: the host merges instead
+    int notfound;       // a deleted edge is not in the graph (nothing applied)
+    int need_rebuild;   // an inserted edge does not fit its list (nothing applied)
+    int R, Knew, lmax;  // row bound, kmax and lmax after the batch
+    unsigned err, err_where;  // device error bits of the persistent kernels
+    unsigned n_leave;   // vertices whose kmax fell (deletions) or rose (insertions)
+    unsigned pad;
+    unsigned long long nlog, total, cap, work, region, scanned;
+    unsigned long long deadline_ns;  // time limit of the repair (0: none)
+};
+
 __device__ __forceinline__ unsigned long long wait_limit(const EngineCtl* c) {
     const unsigned long long w = *reinterpret_cast<const volatile unsigned long long*>(&c->wait_ns);
     return w ? w : kWaitNs;

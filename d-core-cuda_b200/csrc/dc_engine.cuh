@@ -120,6 +120,18 @@ uint32_t row_repair_max_insertions();
 // nlog entries of the scratch change log (dc_repair.cu); nlog = 0 when no row
 // above 0 changed.
 int apply_change_log(dc_graph* h, uint64_t nlog, bool* applied);
+// Captured batches (dc_repair.cu): the row maintenance of a batch with its
+// decisions in a device status block, enqueued without waiting.
+int repair_prepare(dc_graph* h);
+int decide_enqueue(dc_graph* h, BatchStatus* st, const int* dbuf, int rmode, uint32_t n_edges, bool insertions);
+// Releases a handle's captured-batch graphs and staging buffers (dc_maint.cu).
+void free_captured_batches(dc_graph* h);
+int repair_enqueue(dc_graph* h, bool insertions, const uint32_t* d_u, const uint32_t* d_v, uint32_t n,
+                   uint64_t log_cap, BatchStatus* st);
+int merge_enqueue(dc_graph* h, BatchStatus* st, uint32_t* coff, int32_t* ck, int32_t* cl, uint32_t* noff,
+                  int32_t* nk, int32_t* nl);
+// Change-log capacity of a repair (at least 2^20 entries).
+int ensure_change_log(dc_graph* h, uint64_t* cap_out);
 // Maintenance method for a batch (rule of thumb or the learned scheduler).
 int choose_method(dc_graph* h, uint64_t n_ins, uint64_t n_del);
 

@@ -136,6 +136,13 @@ struct dc_graph {
     // failure-detection tests: block of the next persistent launch that
     // leaves at its first grid barrier without arriving (-1: none)
     int32_t barrier_fault_block = -1;
+    // maintenance batches as captured CUDA graphs (dc_maint.cu)
+    bool captured_batches = true;
+    uint32_t* cb_host = nullptr;           // pinned: batch arrays, then the status block
+    uint32_t* cb_dev = nullptr;            // device copy of the batch arrays
+    dc::BatchStatus* cb_status = nullptr;  // device status block
+    uint64_t cb_words = 0;                 // capacity of cb_host / cb_dev in words (status excluded)
+    cudaGraphExec_t cb_exec[2] = {};       // deletion / insertion batch graphs (updated per batch)
     dc::EngineCtl ctl_init{};
     dc::EngineCtl ctl_init_seg[dc::kMaxRowSegments - 1] = {};  // the other row segments'
     // optional per-step trace of persistent kernels (diagnostics)

@@ -542,6 +542,56 @@ __global__ void k_vmax(uint32_t V, const int32_t* a, int* out) {
 }
 
 // ---------------------------------------------------------------------------
+// decisions of a captured batch (BatchStatus, csrc/dc_device.cuh)
+// ---------------------------------------------------------------------------
+__global__ void k_gb_init(BatchStatus* st, unsigned long long cap, int* dbuf) {
+    BatchStatus z = {};
+    z.run_apply = 1;
+    z.cap = cap;
+    *st = z;
+    dbuf[0] = -1;  // row bound (max), kmax after the batch (max), lmax (max)
+    dbuf[1] = 0;
+    dbuf[2] = 0;
+}
+
+// After the deletion check or the insertion capacity check: a failed check
+// stops the batch before anything is applied.
+__global__ void k_gb_gate(const EngineCtl* c, BatchStatus* st) {
+    const unsigned e = c->error;
+    if (e & DC_DEV_ERR_NOTFOUND) st->notfound = 1;
+    if (e & DC_DEV_ERR_CAPACITY) st->need_rebuild = 1;
+    if (e) st->run_apply = 0;
+}
+
+// After a persistent kernel: its errors stop the batch (reported by the host).
+__global__ void k_gb_collect(const EngineCtl* c, BatchStatus* st, int count_region) {
+    if (!st->run_apply) return;
+    const unsigned e = c->error;
+    if (e) {
+        st->err |= e;
+        st->err_where = c->err_where;
+        st->run_apply = 0;
+        return;
+    }
+    if (count_region) st->region += c->log_count;
+}
+
+// Expected work of a row repair (row_repair_worthwhile's measure): sum over
+// the edges' endpoints of degree x kmax, before the batch.
+__global__ void k_gb_work(uint32_t n, const uint32_t* u, const uint32_t* v, const int32_t* kmax,
+                          const int32_t* in_len, const int32_t* out_len, BatchStatus* st) {
+    unsigned long long w = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = u[i], b = v[i];
+        w += (unsigned long long)(in_len[a] + out_len[a]) * (unsigned long long)max(kmax[a], 0);
+        w += (unsigned long long)(in_len[b] + out_len[b]) * (unsigned long long)max(kmax[b], 0);
+    }
+#pragma unroll
+    for (int s = 16; s; s >>= 1) w += __shfl_xor_sync(0xFFFFFFFFu, w, s);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(&st->work, w);
+}
+
+// ---------------------------------------------------------------------------
 // skyline merge: rows <= R from the fresh partial skyline, rows > R from the
 // previous one
 // ---------------------------------------------------------------------------
@@ -884,14 +934,13 @@ static int apply_insertions(dc_graph* h, const NetBatch& nb, uint32_t** d_iu_out
     return DC_OK;
 }
 
-// One local core update.  which: 0 = kmax (count list = in-list),
-// 1 = row 0 (count list = out-list).  insert_mode: roots + bound b.
-static int core_local(dc_graph* h, int which, int32_t* val, const int32_t* old, const uint32_t* d_seeds,
-                      uint32_t n_seeds, int insert_mode, int32_t b, uint64_t* region) {
+// Parameters of one local core update.  which: 0 = kmax (count list =
+// in-list), 1 = row 0 (count list = out-list).  insert_mode: roots + bound b.
+static int core_params(dc_graph* h, int which, int32_t* val, const int32_t* old, const uint32_t* d_seeds,
+                       uint32_t n_seeds, int insert_mode, int32_t b, CoreParams* out) {
     DevGraph& g = h->g;
     Scratch* s = h->scratch;
-    if (n_seeds == 0) return DC_OK;
-    CoreParams p;
+    CoreParams& p = *out;
     p.V = g.V;
     if (which == 0) {
         p.c_off = g.in_off; p.c_len = g.in_len; p.c_nbr = g.in_nbr;
@@ -916,7 +965,16 @@ static int core_local(dc_graph* h, int which, int32_t* val, const int32_t* old, 
     p.q.slots = s->tring;
     p.q.mask = (unsigned)(s->tring_cap - 1);
     p.ctl = h->ctl;
-    if (insert_mode) MT_CUDA(cudaMemsetAsync(s->stamp, 0xFF, 4ull * g.V, h->stream));
+    return DC_OK;
+}
+
+// One local core update, waited for.
+static int core_local(dc_graph* h, int which, int32_t* val, const int32_t* old, const uint32_t* d_seeds,
+                      uint32_t n_seeds, int insert_mode, int32_t b, uint64_t* region) {
+    if (n_seeds == 0) return DC_OK;
+    CoreParams p;
+    if (int rc = core_params(h, which, val, old, d_seeds, n_seeds, insert_mode, b, &p)) return rc;
+    if (insert_mode) MT_CUDA(cudaMemsetAsync(h->scratch->stamp, 0xFF, 4ull * h->g.V, h->stream));
     void* args[] = {&p};
     EngineCtl hc;
     if (int rc = run_persistent(h, (const void*)k_core_local, args, "core update", &hc)) return rc;
@@ -945,6 +1003,422 @@ static unsigned long long repair_deadline_ns(const dc_graph* h, int32_t R, int r
     const double K = std::max<int32_t>(1, h->d.kmax);
     const double ms = 2.0 + h->full_rows_ms * std::min(1.0, (double)R / K) + 0.1 * h->full_rows_ms;
     return (unsigned long long)(ms * 1e6);
+}
+
+// Rows 1..R recomputed from the new row 0 (kmax and row 0 already updated)
+// and merged with the old skyline above R; then the decomposition is current
+// with kmax Knew and lmax.  On failure the decomposition is marked invalid.
+static int recompute_rows(dc_graph* h, int32_t R, int32_t Knew, int32_t lmax) {
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    const uint32_t V = h->g.V;
+    MT_CUDA(cudaMemcpyAsync(s->row0, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
+    uint64_t nlog = 0;
+    int rc = rows_from_row0(h, Knew, R, R > 48, &nlog, 1, false);
+    if (rc != DC_OK) return rc;
+    // the old skyline stays readable while rows 0..R are assembled in
+    // spare slot 0 and merged into spare slot 1; then the merged one is
+    // current and the other two go back to the slots (no allocation
+    // once the slots have grown to the graph's size)
+    uint32_t* o_off = d.sky_off;
+    int32_t* o_k = d.sky_k;
+    int32_t* o_l = d.sky_l;
+    const uint64_t o_cap = d.corner_cap;
+    if ((rc = sky_take_spare(h, 0, 0, &d.sky_off, &d.sky_k, &d.sky_l, &d.corner_cap)) == DC_OK)
+        rc = build_skyline_from_log(h, nlog);
+    if (rc == DC_OK) {
+        unsigned long long* cnt = (unsigned long long*)s->tmp64;
+        ++g_launches;
+        k_merge_count<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, R, d.kmax_v, d.sky_off, d.sky_k, d.sky_l, o_off,
+                                                                o_k, o_l, cnt);
+        rc = scan_tmp64(h, V);
+        unsigned long long total = 0;
+        if (rc == DC_OK) {
+            cudaMemcpyAsync(&total, s->tmp64 + V, sizeof(total), cudaMemcpyDeviceToHost, h->stream);
+            cudaStreamSynchronize(h->stream);
+        }
+        uint32_t* m_off = nullptr;
+        int32_t *m_k = nullptr, *m_l = nullptr;
+        uint64_t m_cap = 0;
+        if (rc == DC_OK) rc = sky_take_spare(h, 1, total, &m_off, &m_k, &m_l, &m_cap);
+        if (rc == DC_OK) {
+            ++g_launches;
+            k_merge_fill<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, R, d.kmax_v, d.sky_off, d.sky_k, d.sky_l,
+                                                                   o_off, o_k, o_l, cnt, m_k, m_l, m_off);
+            cudaStreamSynchronize(h->stream);
+            sky_put_spare(h, 0, d.sky_off, d.sky_k, d.sky_l, d.corner_cap);
+            d.sky_off = m_off;
+            d.sky_k = m_k;
+            d.sky_l = m_l;
+            d.corner_cap = m_cap;
+            d.n_corners = total;
+        }
+    }
+    sky_put_spare(h, 1, o_off, o_k, o_l, o_cap);
+    if (rc != DC_OK) {
+        d.valid = false;
+        return rc;
+    }
+    d.kmax = Knew;
+    d.lmax = lmax;
+    d.rows_valid = false;
+    d.valid = true;
+    return DC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// a maintenance batch as one captured CUDA graph
+// ---------------------------------------------------------------------------
+// A batch of one kind of update (deletions or insertions) on the local
+// method with rows repaired in place is enqueued once on the handle's
+// stream under stream capture and run as ONE graph launch: the batch
+// arrays' upload, the deletion check or the insertion capacity check, the
+// list updates, the kmax and row-0 updates, the row bound, the repair of
+// rows 1..R, the skyline merge and the read-back of the batch's status.
+// Every branch the host-driven batch takes between kernels is taken on the
+// device (BatchStatus): kernels behind a branch act only while its run flag
+// is set.  What the graph cannot finish -- a list without free slots (the
+// store is rebuilt), a repair that is not expected to pay or gives up, a
+// merged skyline larger than its buffer -- the host finishes after the
+// launch from the state the graph left (the graph never half-applies a
+// batch: nothing is written before both checks pass).  The graph is
+// re-captured per batch (its grids and buffers change) and applied to the
+// handle's executable graph by cudaGraphExecUpdate, so it is instantiated
+// once per kind.  Its timing events are event-record nodes (recorded with
+// cudaEventRecordExternal; a plain record inside a capture only orders
+// streams).
+static constexpr uint32_t kCapturedMax = 1536;
+
+void free_captured_batches(dc_graph* h) {
+    for (auto& e : h->cb_exec)
+        if (e) {
+            cudaGraphExecDestroy(e);
+            e = nullptr;
+        }
+    if (h->cb_host) cudaFreeHost(h->cb_host);
+    if (h->cb_dev) cudaFreeAsync(h->cb_dev, h->stream);
+    h->cb_host = nullptr;
+    h->cb_dev = nullptr;
+    h->cb_status = nullptr;
+    h->cb_words = 0;
+}
+
+// Staging for `words` words of batch arrays plus the status block.
+static int captured_buffers(dc_graph* h, uint64_t words) {
+    if (words <= h->cb_words && h->cb_host) return DC_OK;
+    const uint64_t want = (std::max<uint64_t>(4096, 2 * words) + 63) & ~63ull;
+    const uint64_t status_words = (sizeof(BatchStatus) + 255) / 4;
+    if (h->cb_host) cudaFreeHost(h->cb_host);
+    if (h->cb_dev) cudaFreeAsync(h->cb_dev, h->stream);
+    h->cb_host = nullptr;
+    h->cb_dev = nullptr;
+    h->cb_words = 0;
+    if (cudaHostAlloc((void**)&h->cb_host, 4 * (want + status_words), cudaHostAllocDefault) != cudaSuccess ||
+        cudaMallocAsync((void**)&h->cb_dev, 4 * (want + status_words), h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(DC_ERR_NOMEM, "captured batch: staging allocation failed");
+    }
+    h->cb_status = reinterpret_cast<BatchStatus*>(h->cb_dev + want);
+    h->cb_words = want;
+    return DC_OK;
+}
+
+// Enqueues the whole batch (no host waits).  Arrays: u/v of the batch's
+// edges (deletions: distinct pairs with their counts in cnt; insertions:
+// one entry per occurrence), deletions grouped per list side in g*.
+struct CapturedArgs {
+    bool ins;
+    uint32_t n;
+    const uint32_t *u, *v, *cnt;
+    uint32_t ng[2];
+    const uint32_t *gv[2], *go[2], *gn[2];
+    int rmode;
+    uint64_t log_cap;
+    uint64_t cap1;  // corners the merged skyline's buffer holds
+    uint32_t *coff, *noff;
+    int32_t *ck, *cl, *nk, *nl;
+    CoreParams cp[2];
+};
+
+static int captured_enqueue(dc_graph* h, CapturedArgs& a, uint64_t words) {
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    cudaStream_t st = h->stream;
+    BatchStatus* bs = h->cb_status;
+    int* dbuf = (int*)s->cursor;
+    cudaEvent_t* ev = h->ev;
+    MT_CUDA(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
+    MT_CUDA(cudaMemcpyAsync(h->cb_dev, h->cb_host, 4 * words, cudaMemcpyHostToDevice, st));
+    ++g_launches;
+    k_gb_init<<<1, 1, 0, st>>>(bs, a.cap1, dbuf);
+    MT_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(EngineCtl), st));
+    // ---- checks before anything is written
+    if (!a.ins) {
+        ++g_launches;
+        k_del_validate<<<mgrid(h, (uint64_t)a.n * 32), kMThreads, 0, st>>>(a.n, a.u, a.v, (const int32_t*)a.cnt,
+                                                                          g.out_off, g.out_len, g.out_nbr, h->ctl);
+    } else {
+        MT_CUDA(cudaMemsetAsync(s->key2, 0, 4ull * V, st));
+        MT_CUDA(cudaMemsetAsync(s->cdeg2, 0, 4ull * V, st));
+        g_launches += 2;
+        k_ins_need<<<mgrid(h, a.n), kMThreads, 0, st>>>(a.n, a.u, a.v, s->key2, s->cdeg2);
+        k_ins_fits<<<mgrid(h, V), kMThreads, 0, st>>>(V, g.out_off, g.out_len, s->key2, g.in_off, g.in_len, s->cdeg2,
+                                                      h->ctl);
+    }
+    ++g_launches;
+    k_gb_gate<<<1, 1, 0, st>>>(h->ctl, bs);
+    if (a.rmode == 1) {
+        ++g_launches;
+        k_gb_work<<<mgrid(h, a.n), kMThreads, 0, st>>>(a.n, a.u, a.v, d.kmax_v, g.in_len, g.out_len, bs);
+    }
+    MT_CUDA(cudaMemcpyAsync(s->kmax_old, d.kmax_v, 4ull * V, cudaMemcpyDeviceToDevice, st));
+    // ---- list updates
+    if (!a.ins) {
+        for (int side = 0; side < 2; ++side) {
+            if (!a.ng[side]) continue;
+            ++g_launches;
+            k_del_apply<<<mgrid(h, (uint64_t)a.ng[side] * 32), kMThreads, 0, st>>>(
+                a.ng[side], a.gv[side], a.go[side], a.gn[side], side == 0 ? g.out_off : g.in_off,
+                side == 0 ? g.out_len : g.in_len, side == 0 ? g.out_nbr : g.in_nbr, h->ctl, &bs->run_apply);
+        }
+    } else {
+        ++g_launches;
+        k_ins_apply<<<mgrid(h, a.n), kMThreads, 0, st>>>(a.n, a.u, a.v, g.out_off, g.out_len, g.out_nbr, g.in_off,
+                                                         g.in_len, g.in_nbr, &bs->run_apply);
+    }
+    // ---- kmax and row 0, locally
+    if (!a.ins) {
+        MT_CUDA(cudaMemcpyAsync(s->row0_old, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, st));
+    } else {
+        MT_CUDA(cudaMemcpyAsync(s->cdeg2, d.kmax_v, 4ull * V, cudaMemcpyDeviceToDevice, st));
+        MT_CUDA(cudaMemcpyAsync(s->key2, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, st));
+    }
+    for (int which = 0; which < 2; ++which) {
+        if (a.ins) MT_CUDA(cudaMemsetAsync(s->stamp, 0xFF, 4ull * V, st));
+        void* args[] = {&a.cp[which]};
+        if (int rc = persistent_enqueue(h, (const void*)k_core_local, args, "core update", h->ctl, st)) return rc;
+        ++g_launches;
+        k_gb_collect<<<1, 1, 0, st>>>(h->ctl, bs, a.ins ? 1 : 0);
+    }
+    MT_CUDA(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
+    MT_CUDA(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
+    // ---- the rows a batch can change, and what to do with them
+    g_launches += 3;
+    k_rows_bound_edges<<<mgrid(h, a.n), kMThreads, 0, st>>>(a.n, a.u, a.v, s->kmax_old, d.kmax_v, dbuf);
+    k_rows_bound_changed<<<mgrid(h, V), kMThreads, 0, st>>>(V, s->kmax_old, d.kmax_v, dbuf, dbuf + 1);
+    k_vmax<<<mgrid(h, V), kMThreads, 0, st>>>(V, d.row0, dbuf + 2);
+    if (int rc = decide_enqueue(h, bs, dbuf, a.rmode, a.n, a.ins)) return rc;
+    MT_CUDA(cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal));
+    if (int rc = repair_enqueue(h, a.ins, a.u, a.v, a.n, a.log_cap, bs)) return rc;
+    MT_CUDA(cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal));
+    if (int rc = merge_enqueue(h, bs, a.coff, a.ck, a.cl, a.noff, a.nk, a.nl)) return rc;
+    MT_CUDA(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
+    MT_CUDA(cudaMemcpyAsync(h->cb_host + h->cb_words, bs, sizeof(BatchStatus), cudaMemcpyDeviceToHost, st));
+    return DC_OK;
+}
+
+// Runs a one-kind batch as one captured graph.  *handled = false (and
+// nothing changed) when the batch needs the host path: a list without free
+// slots, or a graph the driver does not accept (the handle then stops
+// capturing).
+static int maintain_captured(dc_graph* h, const NetBatch& nb, int rmode, dc_maint_stats* st, bool* handled) {
+    *handled = false;
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    CapturedArgs a;
+    memset(&a, 0, sizeof(a));
+    a.ins = nb.del_u.empty();
+    a.rmode = rmode;
+    // ---- batch arrays packed into one upload
+    std::vector<uint32_t> w;
+    size_t o_u = 0, o_v = 0, o_c = 0, o_g[2][3] = {};
+    if (a.ins) {
+        a.n = (uint32_t)nb.ins_u.size();
+        w.insert(w.end(), nb.ins_u.begin(), nb.ins_u.end());
+        o_v = w.size();
+        w.insert(w.end(), nb.ins_v.begin(), nb.ins_v.end());
+    } else {
+        a.n = (uint32_t)nb.del_u.size();
+        w.insert(w.end(), nb.del_u.begin(), nb.del_u.end());
+        o_v = w.size();
+        w.insert(w.end(), nb.del_v.begin(), nb.del_v.end());
+        o_c = w.size();
+        for (int32_t c : nb.del_n) w.push_back((uint32_t)c);
+        for (int side = 0; side < 2; ++side) {
+            std::vector<uint32_t> gv, go, gn;
+            if (side == 0) group_by(nb.del_u, nb.del_v, nb.del_n, gv, go, gn);
+            else group_by(nb.del_v, nb.del_u, nb.del_n, gv, go, gn);
+            a.ng[side] = (uint32_t)gv.size();
+            o_g[side][0] = w.size();
+            w.insert(w.end(), gv.begin(), gv.end());
+            o_g[side][1] = w.size();
+            w.insert(w.end(), go.begin(), go.end());
+            o_g[side][2] = w.size();
+            w.insert(w.end(), gn.begin(), gn.end());
+        }
+    }
+    if (int rc = captured_buffers(h, w.size())) return rc;
+    memcpy(h->cb_host, w.data(), 4 * w.size());
+    a.u = h->cb_dev + o_u;
+    a.v = h->cb_dev + o_v;
+    a.cnt = h->cb_dev + o_c;
+    for (int side = 0; side < 2; ++side) {
+        a.gv[side] = h->cb_dev + o_g[side][0];
+        a.go[side] = h->cb_dev + o_g[side][1];
+        a.gn[side] = h->cb_dev + o_g[side][2];
+    }
+    // ---- everything the graph uses, allocated before the capture
+    if (!s->kmax_old && (mt_malloc(h->stream, &s->kmax_old, (uint64_t)V + 1) ||
+                         mt_malloc(h->stream, &s->row0_old, (uint64_t)V + 1)))
+        return DC_ERR_NOMEM;
+    uint64_t log_cap = 0;
+    if (int rc = ensure_change_log(h, &log_cap)) return rc;
+    a.log_cap = std::min<uint64_t>(log_cap, 1ull << 22);
+    if (int rc = repair_prepare(h)) return rc;
+    const int32_t bb = (int32_t)std::min<uint64_t>(nb.n_ins, 0x3FFFFFFF);
+    if (!a.ins) {
+        if (int rc = core_params(h, 0, d.kmax_v, s->kmax_old, a.v, a.n, 0, 0, &a.cp[0])) return rc;
+        if (int rc = core_params(h, 1, d.row0, s->row0_old, a.u, a.n, 0, 0, &a.cp[1])) return rc;
+    } else {
+        if (int rc = core_params(h, 0, d.kmax_v, s->cdeg2, a.v, a.n, 1, bb, &a.cp[0])) return rc;
+        if (int rc = core_params(h, 1, d.row0, s->key2, a.u, a.n, 1, bb, &a.cp[1])) return rc;
+    }
+    a.cp[0].run = a.cp[1].run = &h->cb_status->run_apply;
+    uint64_t cap0 = 0;
+    if (int rc = sky_take_spare(h, 0, a.log_cap, &a.coff, &a.ck, &a.cl, &cap0)) return rc;
+    int rc = sky_take_spare(h, 1, d.n_corners + d.n_corners / 8 + V / 4 + 4096, &a.noff, &a.nk, &a.nl, &a.cap1);
+    if (rc != DC_OK) {
+        sky_put_spare(h, 0, a.coff, a.ck, a.cl, cap0);
+        return rc;
+    }
+    auto put_back = [&](bool slot1) {
+        sky_put_spare(h, 0, a.coff, a.ck, a.cl, cap0);
+        if (slot1) sky_put_spare(h, 1, a.noff, a.nk, a.nl, a.cap1);
+    };
+    MT_CUDA(cudaStreamSynchronize(h->stream));  // allocations done before the capture
+    // ---- capture, update the executable graph, launch
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        cudaGetLastError();
+        put_back(true);
+        h->captured_batches = false;
+        return DC_OK;
+    }
+    const unsigned long long launches0 = g_launches.load();
+    rc = captured_enqueue(h, a, w.size());
+    cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
+    cudaGraphExec_t& ex = h->cb_exec[a.ins ? 1 : 0];
+    if (rc == DC_OK && ec == cudaSuccess && ex) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(ex, graph, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(ex);
+            ex = nullptr;
+        }
+    }
+    if (rc == DC_OK && ec == cudaSuccess && !ex && cudaGraphInstantiate(&ex, graph, 0) != cudaSuccess) ec = cudaErrorUnknown;
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != DC_OK || ec != cudaSuccess) {
+        // the graph was not built: nothing ran; the host path takes the batch
+        // and the handle's later batches (reported once per handle)
+        fprintf(stderr, "dcore_b200: maintenance batches run host-driven on this graph: capture failed (%s; %s)\n",
+                rc != DC_OK ? dc_last_error() : "", cudaGetErrorString(ec));
+        cudaGetLastError();
+        g_launches = launches0;
+        put_back(true);
+        h->captured_batches = false;
+        set_error(DC_OK, "%s", "");
+        return DC_OK;
+    }
+    MT_CUDA(cudaGraphLaunch(ex, h->stream));
+    MT_CUDA(cudaStreamSynchronize(h->stream));
+    const BatchStatus r = *reinterpret_cast<const BatchStatus*>(h->cb_host + h->cb_words);
+    // ---- what the graph decided
+    if (r.notfound) {
+        put_back(true);
+        return set_error(DC_ERR_NOT_FOUND, "dc_maintain: a deleted edge is not in the graph (batch not applied)");
+    }
+    if (r.need_rebuild) {  // nothing applied: the host path rebuilds the store
+        put_back(true);
+        return DC_OK;
+    }
+    *handled = true;
+    if (r.err) {
+        put_back(true);
+        d.valid = false;
+        d.peel_valid = false;
+        if (r.err & DC_DEV_ERR_TIMEOUT)
+            return set_error(DC_ERR_TIMEOUT, "captured batch: bounded device wait expired (site %u)", r.err_where);
+        return set_error(DC_ERR_CUDA, "captured batch: device error 0x%x (site %u)", r.err, r.err_where);
+    }
+    if (a.ins) g.E += nb.n_ins;
+    else g.E -= nb.n_del;
+    g.sorted_kmax = false;
+    st->method = DC_MAINT_LOCAL;
+    st->region = r.region + (a.ins ? 0 : 2ull * a.n);
+    st->rows_recomputed = r.R + 1;
+    st->ins_scanned = a.ins ? r.scanned : 0;
+    st->captured = 1;
+    cudaEvent_t* ev = h->ev;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    st->apply_ms = ms;
+    cudaEventElapsedTime(&ms, ev[1], ev[2]);
+    st->core_ms = ms;
+    cudaEventElapsedTime(&ms, ev[2], ev[3]);
+    st->rows_ms = ms;
+    cudaEventElapsedTime(&ms, ev[0], ev[3]);
+    st->total_ms = ms;
+    if (r.R > 0) {
+        cudaEventElapsedTime(&ms, ev[4], ev[5]);
+        if (a.ins) st->ins_repair_ms = ms;
+        else st->del_repair_ms = ms;
+    }
+    cudaGetLastError();  // a timing query that failed leaves no error behind
+    if (r.R >= 0 && r.run_merge) {
+        // the merged skyline is current; the old one becomes a spare
+        sky_put_spare(h, 0, a.coff, a.ck, a.cl, cap0);
+        sky_put_spare(h, 1, d.sky_off, d.sky_k, d.sky_l, d.corner_cap);
+        d.sky_off = a.noff;
+        d.sky_k = a.nk;
+        d.sky_l = a.nl;
+        d.corner_cap = a.cap1;
+        d.n_corners = r.total;
+        if (r.R > 0) st->rows_local = a.ins ? 2 : 1;
+    } else {
+        put_back(true);
+        if (r.R >= 0 && (r.merge_overflow || r.fallback)) {
+            // the host finishes the rows (timed apart, added to the batch)
+            cudaEventRecord(ev[6], h->stream);
+            bool applied = false;
+            if (r.merge_overflow) {
+                if ((rc = apply_change_log(h, r.nlog, &applied)) != DC_OK) {
+                    d.valid = false;
+                    return rc;
+                }
+                if (applied && r.R > 0) st->rows_local = a.ins ? 2 : 1;
+            }
+            if (!applied && (rc = recompute_rows(h, r.R, r.Knew, r.lmax)) != DC_OK) return rc;
+            cudaEventRecord(ev[7], h->stream);
+            MT_CUDA(cudaStreamSynchronize(h->stream));
+            cudaEventElapsedTime(&ms, ev[6], ev[7]);
+            st->rows_ms += ms;
+            st->total_ms += ms;
+        }
+    }
+    d.kmax = r.Knew;
+    d.lmax = r.lmax;
+    d.rows_valid = false;
+    d.valid = true;
+    d.row_lo = 1;
+    d.row_hi = d.kmax;
+    st->kmax = d.kmax;
+    st->lmax = d.lmax;
+    return DC_OK;
 }
 
 // repair_mode: the row maintenance mode of this batch (-1: the handle's);
@@ -997,6 +1471,28 @@ static int maintain_impl(dc_graph* h, const uint32_t* pairs, const uint8_t* is_d
     // updates the expected-work estimate misses the cascades that deletions
     // near the dense core start, and a recomputation is the safer bet
     if (rmode == 1 && nb.n_ins + nb.n_del > kRuleRepairMax) rmode = 0;
+    // ---- one kind of update, local method, rows in place: one graph launch
+    const uint64_t n_one = nb.del_u.empty() ? nb.ins_u.size() : nb.del_u.size();
+    if (h->captured_batches && method == DC_MAINT_LOCAL && rmode != 0 && nb.del_u.empty() != nb.ins_u.empty() &&
+        n_one <= kCapturedMax && !h->trace_dev && h->barrier_fault_block < 0 && d.kmax_v && d.sky_off) {
+        bool handled = false;
+        st->deleted = nb.n_del;
+        st->inserted = nb.n_ins;
+        int rc = maintain_captured(h, nb, rmode, st, &handled);
+        if (rc != DC_OK) {
+            if (handled) {
+                d.valid = false;
+                d.peel_valid = false;
+            }
+            return rc;
+        }
+        if (handled) {
+            h->mtimes.total_ms = st->total_ms;
+            if (h->log_maint && want_feat) log_batch(h, feat, st);
+            return DC_OK;
+        }
+        memset(st, 0, sizeof(*st));
+    }
     bool repair_del = false;  // rows of the deletions repaired in place
     if (rmode && !nb.del_u.empty() && nb.del_u.size() <= row_repair_max_deletions() && d.kmax_v) {
         uint32_t *eu = nullptr, *ev = nullptr;
@@ -1190,56 +1686,7 @@ static int maintain_impl(dc_graph* h, const uint32_t* pairs, const uint8_t* is_d
             }
         }
         // ---- rows 0..R from the new row 0, rows above R from the old skyline
-        MT_CUDA(cudaMemcpyAsync(s->row0, d.row0, 4ull * V, cudaMemcpyDeviceToDevice, h->stream));
-        uint64_t nlog = 0;
-        if ((rc = rows_from_row0(h, Knew, R, R > 48, &nlog, 1, false))) goto out;
-        // the old skyline stays readable while rows 0..R are assembled in
-        // spare slot 0 and merged into spare slot 1; then the merged one is
-        // current and the other two go back to the slots (no allocation
-        // once the slots have grown to the graph's size)
-        uint32_t* o_off = d.sky_off;
-        int32_t* o_k = d.sky_k;
-        int32_t* o_l = d.sky_l;
-        const uint64_t o_cap = d.corner_cap;
-        if ((rc = sky_take_spare(h, 0, 0, &d.sky_off, &d.sky_k, &d.sky_l, &d.corner_cap)) == DC_OK)
-            rc = build_skyline_from_log(h, nlog);
-        if (rc == DC_OK) {
-            unsigned long long* cnt = (unsigned long long*)s->tmp64;
-            ++g_launches;
-            k_merge_count<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, R, d.kmax_v, d.sky_off, d.sky_k, d.sky_l, o_off,
-                                                                    o_k, o_l, cnt);
-            rc = scan_tmp64(h, V);
-            unsigned long long total = 0;
-            if (rc == DC_OK) {
-                cudaMemcpyAsync(&total, s->tmp64 + V, sizeof(total), cudaMemcpyDeviceToHost, h->stream);
-                cudaStreamSynchronize(h->stream);
-            }
-            uint32_t* m_off = nullptr;
-            int32_t *m_k = nullptr, *m_l = nullptr;
-            uint64_t m_cap = 0;
-            if (rc == DC_OK) rc = sky_take_spare(h, 1, total, &m_off, &m_k, &m_l, &m_cap);
-            if (rc == DC_OK) {
-                ++g_launches;
-                k_merge_fill<<<mgrid(h, V), kMThreads, 0, h->stream>>>(V, R, d.kmax_v, d.sky_off, d.sky_k, d.sky_l,
-                                                                       o_off, o_k, o_l, cnt, m_k, m_l, m_off);
-                cudaStreamSynchronize(h->stream);
-                sky_put_spare(h, 0, d.sky_off, d.sky_k, d.sky_l, d.corner_cap);
-                d.sky_off = m_off;
-                d.sky_k = m_k;
-                d.sky_l = m_l;
-                d.corner_cap = m_cap;
-                d.n_corners = total;
-            }
-        }
-        sky_put_spare(h, 1, o_off, o_k, o_l, o_cap);
-        if (rc != DC_OK) {
-            d.valid = false;
-            goto out;
-        }
-        d.kmax = Knew;
-        d.lmax = res[2];
-        d.rows_valid = false;
-        d.valid = true;
+        if ((rc = recompute_rows(h, R, Knew, res[2]))) goto out;
         st->kmax = d.kmax;
         st->lmax = d.lmax;
     }

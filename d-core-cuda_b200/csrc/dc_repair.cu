@@ -76,6 +76,7 @@ struct RepairParams {
     // when set, and a flag that must be nonzero for the kernel to act
     const int32_t* R_dev;
     const unsigned* n_leave_dev;
+    const unsigned long long* deadline_dev;
     const int* run;
     uint32_t* log_v;
     int32_t* log_k;
@@ -250,8 +251,9 @@ __device__ bool r_take(const RepairParams& p, St& S, unsigned* slot) {
 
 __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
     if (p.run && !*p.run) return;
-    if (p.R_dev) p.R = *p.R_dev;
-    if (p.n_leave_dev) p.n_leave = *p.n_leave_dev;
+    const int32_t R = p.R_dev ? *p.R_dev : p.R;
+    const uint32_t n_leave = p.n_leave_dev ? *p.n_leave_dev : p.n_leave;
+    const unsigned long long deadline = p.deadline_dev ? *p.deadline_dev : p.deadline_ns;
     extern __shared__ __align__(16) unsigned char s_raw[];
     RowState& S = *reinterpret_cast<RowState*>(s_raw);
     const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
     int* hi_ = S.hist[wib][1];
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) S.k = ld_vol(&p.ctl->error) ? p.R + 1 : atomicAdd(&p.ctl->level, 1) + 1;
+        if (threadIdx.x == 0) S.k = ld_vol(&p.ctl->error) ? R + 1 : atomicAdd(&p.ctl->level, 1) + 1;
         for (int i = threadIdx.x; i < kHash; i += kRThreads) {
             S.key[i] = kEmptyKey;
             S.cur[i] = kUnset;
@@ -274,7 +276,7 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
         }
         __syncthreads();
         const int k = S.k;
-        if (k > p.R) break;
+        if (k > R) break;
         // ---- seeds: endpoints of deleted edges still in C_k
         for (uint32_t i = threadIdx.x; i < p.n_del && !vld(&S.abort); i += kRThreads) {
             uint32_t u = p.del_u[i], v = p.del_v[i];
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
             if (p.kmax_new[v] >= k) push(S, v);
         }
         // ---- vertices leaving C_k: the neighbours they supported
-        for (uint32_t i = wib; i < p.n_leave; i += kRWarps) {
+        for (uint32_t i = wib; i < n_leave; i += kRWarps) {
             if (__any_sync(0xFFFFFFFFu, vld(&S.abort))) break;
             uint32_t x = p.leave[i];
             if (!(p.kmax_old[x] >= k && p.kmax_new[x] < k)) continue;
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
             // ---- drain
             unsigned slot;
             while (r_take(p, S, &slot)) {
-                if (lane == 0 && p.deadline_ns && gtimer() - t_start > p.deadline_ns) atomicExch(&S.abort, 1);
+                if (lane == 0 && deadline && gtimer() - t_start > deadline) atomicExch(&S.abort, 1);
                 const uint32_t x = vldu(&S.key[slot]);
                 int cap = vld(&S.cur[slot]);
                 if (cap == kUnset) cap = sky_at(p, x, k);
@@ -586,8 +588,9 @@ __device__ int r_eval(const RepairParams& p, St& S, uint32_t x, int k, int cap, 
 
 __global__ void __launch_bounds__(kIThreads) k_row_repair_ins(RepairParams p) {
     if (p.run && !*p.run) return;
-    if (p.R_dev) p.R = *p.R_dev;
-    if (p.n_leave_dev) p.n_leave = *p.n_leave_dev;
+    const int32_t R = p.R_dev ? *p.R_dev : p.R;
+    const uint32_t n_leave = p.n_leave_dev ? *p.n_leave_dev : p.n_leave;
+    const unsigned long long deadline = p.deadline_dev ? *p.deadline_dev : p.deadline_ns;
     extern __shared__ __align__(16) unsigned char s_raw[];
     InsState& I = *reinterpret_cast<InsState*>(s_raw);
     auto& S = I.S;
@@ -607,7 +610,7 @@ __global__ void __launch_bounds__(kIThreads) k_row_repair_ins(RepairParams p) {
         I.scanned = 0;
         I.pused = 0;
     }
-    for (int k = 1; k <= p.R; ++k) {
+    for (int k = 1; k <= R; ++k) {
         __syncthreads();
         if (threadIdx.x == 0 && ld_vol(&p.ctl->error)) S.abort = 1;
         __syncthreads();
@@ -637,7 +640,7 @@ __global__ void __launch_bounds__(kIThreads) k_row_repair_ins(RepairParams p) {
             u = prev_val(p, I, b, k);
             if (u > old_val(p, b, k)) ins_add(I, b, u);
         }
-        for (uint32_t i = threadIdx.x; i < p.n_leave && !vld(&S.abort); i += kIThreads) {
+        for (uint32_t i = threadIdx.x; i < n_leave && !vld(&S.abort); i += kIThreads) {
             const uint32_t x = p.leave[i];
             if (p.kmax_old[x] < k && p.kmax_new[x] >= k) ins_add(I, x, prev_val(p, I, x, k));
         }
@@ -669,7 +672,7 @@ __global__ void __launch_bounds__(kIThreads) k_row_repair_ins(RepairParams p) {
             __syncwarp();
             if (lane == 0) {
                 atomicAdd(&I.scanned, (unsigned long long)(p.out_len[x] + p.in_len[x]));
-                if (p.deadline_ns && gtimer() - t_start > p.deadline_ns) atomicExch(&S.abort, 1);
+                if (deadline && gtimer() - t_start > deadline) atomicExch(&S.abort, 1);
                 __threadfence_block();
                 atomicSub(&S.out, 1);
             }
@@ -711,7 +714,7 @@ __global__ void __launch_bounds__(kIThreads) k_row_repair_ins(RepairParams p) {
                 __syncwarp();
                 if (lane == 0) {
                     atomicAdd(&I.scanned, 2ull * (unsigned long long)(p.out_len[x] + p.in_len[x]));
-                    if (p.deadline_ns && gtimer() - t_start > p.deadline_ns) atomicExch(&S.abort, 1);
+                    if (deadline && gtimer() - t_start > deadline) atomicExch(&S.abort, 1);
                     if (atomicCAS(&S.st[slot], 1u, 0u) == 2u) {
                         atomicExch(&S.st[slot], 1u);
                         enqueue(S, slot);
@@ -919,6 +922,67 @@ __global__ void k_rep_merge(uint32_t V, const int32_t* kmax, const int32_t* row0
     }
 }
 
+// ---------------------------------------------------------------------------
+// decisions of a captured batch (BatchStatus)
+// ---------------------------------------------------------------------------
+// After the kmax / row-0 update: R, and whether rows 1..R are repaired in
+// place, only row 0's corners merged, or recomputed by the host -- the
+// decisions rows_repair / rows_repair_ins and the maintenance driver take.
+__global__ void k_gb_decide(BatchStatus* st, const int* dbuf, unsigned long long full_work, int rmode,
+                            uint32_t n_edges, float full_rows_ms, int K_old) {
+    if (!st->run_apply) return;
+    const int Knew = dbuf[1];
+    const int R = min(dbuf[0], Knew);
+    st->R = R;
+    st->Knew = Knew;
+    st->lmax = dbuf[2];
+    if (R < 0) return;  // nothing changed
+    if (R == 0) {       // rows above 0 keep their values
+        st->run_merge = 1;
+        st->nlog = 0;
+        return;
+    }
+    const bool fits = 2ull * n_edges + st->n_leave <= kHashLimit;
+    const bool worth = rmode >= 2 || (full_work > 0 && 160ull * st->work < full_work);
+    if (fits && worth) {
+        st->run_repair = 1;
+        // the time limit repair_deadline_ns sets on the host path
+        const float ms = 2.f + full_rows_ms * fminf(1.f, (float)R / (float)max(K_old, 1)) + 0.1f * full_rows_ms;
+        st->deadline_ns = rmode == 2 ? 0ull : (unsigned long long)(ms * 1e6f);
+    } else {
+        st->fallback = 1;
+    }
+}
+
+// After the repair: merge its log, or hand the rows to the host.
+__global__ void k_gb_after_repair(const EngineCtl* c, BatchStatus* st) {
+    if (!st->run_repair) return;
+    const unsigned e = c->error;
+    st->run_repair = 0;
+    if (e & DC_DEV_ERR_TIMEOUT) {
+        st->err |= e;
+        st->err_where = c->err_where;
+        return;
+    }
+    if (e) {  // table full or past the time limit: recompute
+        st->fallback = 1;
+        return;
+    }
+    st->run_merge = 1;
+    st->nlog = c->log_count;
+    st->scanned = c->edges_scanned;
+}
+
+// The merged skyline's size against its buffer.
+__global__ void k_gb_total(BatchStatus* st, const unsigned long long* cnt, uint32_t V) {
+    if (!st->run_merge) return;
+    st->total = cnt[V];
+    if (st->total > st->cap) {
+        st->run_merge = 0;
+        st->merge_overflow = 1;
+    }
+}
+
 }  // namespace
 
 
@@ -966,7 +1030,7 @@ bool row_repair_worthwhile(dc_graph* h, const uint32_t* d_u, const uint32_t* d_v
 
 // The change log of a repair: the scratch corner log (sized by the last
 // decomposition), at least 2^20 entries.
-static int ensure_change_log(dc_graph* h, uint64_t* cap_out) {
+int ensure_change_log(dc_graph* h, uint64_t* cap_out) {
     Scratch* s = h->scratch;
     uint64_t cap = s->log_cap;
     if (cap < (1u << 20)) {
@@ -1097,6 +1161,7 @@ int rows_repair(dc_graph* h, int32_t R, const uint32_t* d_du, const uint32_t* d_
     p.R = R;
     p.R_dev = nullptr;
     p.n_leave_dev = nullptr;
+    p.deadline_dev = nullptr;
     p.run = nullptr;
     p.log_v = s->log_v; p.log_k = s->log_k; p.log_l = s->log_l; p.log_cap = cap;
     p.ctl = h->ctl;
@@ -1175,6 +1240,98 @@ int rows_repair_ins(dc_graph* h, int32_t R, const uint32_t* d_iu, const uint32_t
         return set_error(DC_ERR_TIMEOUT, "row repair: bounded device wait expired (site %u)", hc.err_where);
     if (hc.error) return DC_OK;  // capacity or budget: the caller recomputes the rows
     return apply_change_log(h, hc.log_count, applied);
+}
+
+// ---------------------------------------------------------------------------
+// captured batches: the same row maintenance with its decisions on the device
+// ---------------------------------------------------------------------------
+int repair_prepare(dc_graph* h) {
+    (void)h;
+    RP_CUDA(cudaFuncSetAttribute(k_row_repair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RowState)));
+    RP_CUDA(cudaFuncSetAttribute(k_row_repair_ins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InsState)));
+    return DC_OK;
+}
+
+int decide_enqueue(dc_graph* h, BatchStatus* st, const int* dbuf, int rmode, uint32_t n_edges, bool insertions) {
+    g_launches += 2;
+    k_collect_leave<<<rgrid(h, h->g.V), kRThreads, 0, h->stream>>>(h->g.V, h->scratch->kmax_old, h->d.kmax_v,
+                                                                   h->scratch->rem0, &st->n_leave, insertions);
+    k_gb_decide<<<1, 1, 0, h->stream>>>(st, dbuf, h->full_work, rmode, n_edges, h->full_rows_ms, h->d.kmax);
+    RP_CUDA(cudaGetLastError());
+    return DC_OK;
+}
+
+// The repair of rows 1..st->R (deletions or insertions; the vertices whose
+// kmax fell / rose already in scratch rem0, their count in st->n_leave),
+// acting only when st->run_repair, within st->deadline_ns; its change log
+// holds at most log_cap entries.
+int repair_enqueue(dc_graph* h, bool insertions, const uint32_t* d_u, const uint32_t* d_v, uint32_t n,
+                   uint64_t log_cap, BatchStatus* st) {
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    RepairParams p;
+    memset(&p, 0, sizeof(p));
+    p.V = g.V;
+    p.out_off = g.out_off; p.out_len = g.out_len; p.out_nbr = g.out_nbr;
+    p.in_off = g.in_off; p.in_len = g.in_len; p.in_nbr = g.in_nbr;
+    p.kmax_new = d.kmax_v;
+    p.kmax_old = s->kmax_old;
+    p.sky_off = d.sky_off; p.sky_k = d.sky_k; p.sky_l = d.sky_l;
+    p.del_u = d_u; p.del_v = d_v; p.n_del = n;
+    p.leave = s->rem0;
+    p.row0_new = insertions ? d.row0 : nullptr;
+    p.deadline_ns = 0;
+    p.deadline_dev = &st->deadline_ns;
+    p.R = 0;
+    p.R_dev = &st->R;
+    p.n_leave_dev = &st->n_leave;
+    p.run = &st->run_repair;
+    p.log_v = s->log_v; p.log_k = s->log_k; p.log_l = s->log_l; p.log_cap = log_cap;
+    p.ctl = h->ctl;
+    if (int rc = ctl_init_enqueue(h, h->ctl, h->stream)) return rc;
+    ++g_launches;
+    if (insertions) k_row_repair_ins<<<1, kIThreads, sizeof(InsState), h->stream>>>(p);
+    else k_row_repair<<<std::max(1, h->geom.sms), kRThreads, sizeof(RowState), h->stream>>>(p);
+    RP_CUDA(cudaGetLastError());
+    ++g_launches;
+    k_gb_after_repair<<<1, 1, 0, h->stream>>>(h->ctl, st);
+    RP_CUDA(cudaGetLastError());
+    return DC_OK;
+}
+
+// apply_change_log's passes with the log length read from st->nlog, acting
+// only when st->run_merge: change lists into (coff, ck, cl), the merged
+// skyline into (noff, nk, nl) of st->cap corners (a larger result clears
+// run_merge and sets merge_overflow).
+int merge_enqueue(dc_graph* h, BatchStatus* st, uint32_t* coff, int32_t* ck, int32_t* cl, uint32_t* noff,
+                  int32_t* nk, int32_t* nl) {
+    DevGraph& g = h->g;
+    Decomp& d = h->d;
+    Scratch* s = h->scratch;
+    const uint32_t V = g.V;
+    unsigned long long* cnt = (unsigned long long*)s->tmp64;
+    uint32_t* fill = s->cursor;
+    const int grid_log = rgrid(h, s->log_cap);
+    RP_CUDA(cudaMemsetAsync(cnt, 0, 8ull * (V + 1), h->stream));
+    RP_CUDA(cudaMemsetAsync(fill, 0, 4ull * V, h->stream));
+    g_launches += 2;
+    k_chg_count<<<grid_log, kRThreads, 0, h->stream>>>(0, s->log_v, cnt, &st->nlog, &st->run_merge);
+    if (int rc = scan_tmp64(h, V)) return rc;
+    g_launches += 3;
+    k_chg_fill<<<grid_log, kRThreads, 0, h->stream>>>(0, s->log_v, s->log_k, s->log_l, cnt, fill, ck, cl, &st->nlog,
+                                                      &st->run_merge);
+    k_chg_sort<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, cnt, ck, cl, coff, &st->run_merge);
+    k_rep_merge<false><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
+                                                                 coff, ck, cl, cnt, nullptr, nullptr, nullptr,
+                                                                 &st->run_merge);
+    if (int rc = scan_tmp64(h, V)) return rc;
+    g_launches += 2;
+    k_gb_total<<<1, 1, 0, h->stream>>>(st, cnt, V);
+    k_rep_merge<true><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
+                                                                coff, ck, cl, cnt, nk, nl, noff, &st->run_merge);
+    RP_CUDA(cudaGetLastError());
+    return DC_OK;
 }
 
 }  // namespace dc

@@ -58,7 +58,7 @@ class MaintStats(ctypes.Structure):
                 ("rebuilt", ctypes.c_uint32), ("rows_local", ctypes.c_uint32), ("region", ctypes.c_uint64),
                 ("apply_ms", ctypes.c_float), ("core_ms", ctypes.c_float), ("rows_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float), ("del_repair_ms", ctypes.c_float), ("ins_repair_ms", ctypes.c_float),
-                ("ins_scanned", ctypes.c_uint64)]
+                ("ins_scanned", ctypes.c_uint64), ("captured", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 MAINT_AUTO, MAINT_LOCAL, MAINT_REPEEL = 0, 1, 2
@@ -111,6 +111,7 @@ SIGNATURES = {
     "dc_decompose_rows": [vp, ctypes.c_uint32, ctypes.c_uint32, i32p, i32p],
     "dc_row_weights": [vp, u64p, ctypes.c_uint64],
     "dc_set_row_repair": [vp, ctypes.c_int],
+    "dc_set_captured_batches": [vp, ctypes.c_int],
     "dc_maintain": [vp, u32p, u8p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(MaintStats)],
     "dc_decomp_info_get": [vp, ctypes.POINTER(DecompInfo)],
     "dc_get_kmaxes": [vp, i32p],
@@ -499,6 +500,10 @@ class Graph:
         _check(lib().dc_maintain(self._h, _p(pairs, u32p), None if dl is None else _p(dl, u8p), len(src), method,
                                  ctypes.byref(st)))
         return {f: getattr(st, f) for f, _ in MaintStats._fields_}
+
+    def set_captured_batches(self, on):
+        """Run eligible maintenance batches as one captured CUDA graph (default on)."""
+        _check(lib().dc_set_captured_batches(self._h, 1 if on else 0))
 
     def set_row_repair(self, mode):
         """0 recompute rows, 1 repair deletions in place when worthwhile, 2 always when they fit."""

@@ -230,6 +230,8 @@ typedef struct dc_maint_stats {
     float del_repair_ms;        /* in-place row repair of the deletions (0: none ran) */
     float ins_repair_ms;        /* in-place row repair of the insertions (0: none ran) */
     uint64_t ins_scanned;       /* list entries the insertion repair read             */
+    uint32_t captured;          /* 1 when the batch ran as one captured CUDA graph    */
+    uint32_t reserved;
 } dc_maint_stats;
 
 /* maintenanceFast (main.cu:1665-1751) / maintenance (main.cu:1536-1663):
@@ -262,6 +264,20 @@ int dc_maintain(dc_graph* g, const uint32_t* pairs, const uint8_t* is_delete, ui
  * l-list maintenance (kListFindUpperBound / kListRefineHIndex, main.cu:929-1242,
  * hInIndex src/cuda_utils.cuh:68-77) is the specification this replaces. */
 int dc_set_row_repair(dc_graph* g, int on);
+/* Captured batches (default 1): a batch of one kind of update (deletions or
+ * insertions, after its net effect) on the local method with rows repaired
+ * in place (row mode 1 and at most 64 net updates, or modes 2 and 3 and at
+ * most 1536) runs as ONE CUDA graph launch -- upload, checks, list updates,
+ * kmax / row-0 update, row bound, row repair, skyline merge and the status
+ * read-back -- with every branch between its kernels taken on the device.
+ * A batch whose lists lack free slots, whose repair is not expected to pay
+ * or gives up, or whose merged skyline outgrows its buffer is finished on
+ * the host from the state the graph left (dc_maint_stats.captured tells
+ * which ran).  A mixed batch split into deletions and insertions (row
+ * repair) runs as two graphs.  0 keeps every batch host-driven.  Results are
+ * identical.  No counterpart in the reference (a host loop drives every
+ * kernel and polls the device between them, main.cu:741-746, 1735-1743). */
+int dc_set_captured_batches(dc_graph* g, int on);
 
 /* ---- learned maintenance scheduler -------------------------------------- */
 /* A BF16 MLP (16 -> 64 -> 64 -> 2, ReLU) predicting the log of the time of
