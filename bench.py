@@ -63,7 +63,7 @@ WORKLOADS = {
                           "150 GB HBM admission budget; continuous batching"),
     # learned scheduler against the rule of thumb on R-MAT 23
     "sched-rmat23": dict(sched=True, scale=23, ef=16, seed=1, train_scales=(20, 21, 22, 23), train_batches=40,
-                         train_max=65_536, eval_batches=60, eval_max=1_000_000, hot_frac=0.1,
+                         train_max=65_536, train_hot_frac=0.25, eval_batches=60, eval_max=1_000_000, hot_frac=0.1,
                          desc="R-MAT scale 23, edge factor 16; batches of log-uniform 1..1e6 updates "
                               "(50% insert / 50% delete), 10% of batches on the top-1% out-degree vertices"),
 }
@@ -707,13 +707,16 @@ def run_row_sharded(args, w, rank, world, local, dist):
 def _stream_times(dc, g, u, v, dl, sizes, method):
     """Per batch: device ms, method, rows repaired in place (bit 0
     deletions, bit 1 insertions)."""
-    pos, ms, methods, local = 0, [], [], []
+    pos, ms, methods, local, phases = 0, [], [], [], []
     for bs in sizes:
         st = g.maintain(u[pos:pos + bs], v[pos:pos + bs], dl[pos:pos + bs], method)
         ms.append(st["total_ms"])
         methods.append(st["method"])
         local.append(st["rows_local"])
+        phases.append([round(st["apply_ms"], 2), round(st["core_ms"], 2), round(st["rows_ms"], 2), st["rebuilt"],
+                       st["captured"]])
         pos += bs
+    _stream_times.phases = phases
     return np.array(ms), np.array(methods), np.array(local)
 
 
@@ -747,7 +750,7 @@ def run_sched(args, w, rank, world, local):
     for j, scale in enumerate(w["train_scales"]):
         V, s, d = dc.gen_rmat(scale, w["ef"], w["seed"] + 100 + 10 * j + rank)
         tr_sizes = _log_uniform(rng, w["train_batches"], w["train_max"])
-        u, v, dl, _ = _hot_stream(dc, V, s, d, tr_sizes, w["hot_frac"], rng, w["seed"] + 200 + j)
+        u, v, dl, _ = _hot_stream(dc, V, s, d, tr_sizes, w["train_hot_frac"], rng, w["seed"] + 200 + j)
         logs = []
         for method, mode in ((dc.MAINT_LOCAL, 3), (dc.MAINT_REPEEL, 0)):
             with dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16) as g:
@@ -773,16 +776,37 @@ def run_sched(args, w, rank, world, local):
     sampler = ClockSampler(local)
     sampler.start()
     launches0 = dc.launch_count()
+    # the two policies take the batches in turn on their own copies (each
+    # batch timed on the wall clock around dc_maintain, which returns after
+    # the batch): both see the same device state -- memory pool growth, L2 --
+    # so neither pays a one-time cost the other skips
+    graphs = {}
     for name, sch in (("learned", sched), ("rule", None)):
         g = dc.Graph.from_edges(V, s, d, device=local, gap_min=2, gap_div=16)
         g.decompose()  # default row mode: the rule's rows; the network sets the path per batch
         g.set_scheduler(sch)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ms, methods, rows_local = _stream_times(dc, g, u, v, dl, ev_sizes, dc.MAINT_AUTO)
-        wall = time.perf_counter() - t0
-        res[name] = {"wall_s": wall, "device_ms": float(ms.sum()), "ms": ms, "methods": methods,
-                     "rows_local": rows_local, "graph": g}
+        graphs[name] = g
+        res[name] = {"wall": [], "ms": [], "methods": [], "rows_local": [], "phases": [], "graph": g}
+    torch.cuda.synchronize()
+    pos = 0
+    for i, bs in enumerate(ev_sizes):
+        order = ("learned", "rule") if i % 2 == 0 else ("rule", "learned")
+        for name in order:
+            t0 = time.perf_counter()
+            st = graphs[name].maintain(u[pos:pos + bs], v[pos:pos + bs], dl[pos:pos + bs], dc.MAINT_AUTO)
+            r = res[name]
+            r["wall"].append(time.perf_counter() - t0)
+            r["ms"].append(st["total_ms"])
+            r["methods"].append(st["method"])
+            r["rows_local"].append(st["rows_local"])
+            r["phases"].append([round(st["apply_ms"], 2), round(st["core_ms"], 2), round(st["rows_ms"], 2),
+                                st["rebuilt"], st["captured"]])
+        pos += bs
+    for name, r in res.items():
+        for k in ("ms", "methods", "rows_local"):
+            r[k] = np.array(r[k])
+        r["wall_s"] = float(np.sum(r["wall"]))
+        r["device_ms"] = float(r["ms"].sum())
     launches = dc.launch_count() - launches0
     clocks = sampler.stop()
     fs, fd = _final_edges(s, d, u, v, dl)
@@ -804,7 +828,9 @@ def run_sched(args, w, rank, world, local):
                        "train": {"graphs": f"R-MAT scales {list(w['train_scales'])}, edge factor {w['ef']}, "
                                            "fresh seeds",
                                  "batches": int(w["train_batches"]) * len(w["train_scales"]),
-                                 "max_batch": w["train_max"],
+                                 "max_batch": w["train_max"], "hot_fraction": w["train_hot_frac"],
+                                 "paths": "incremental (local, row mode 3) and full (re-peel, row mode 0), "
+                                          "one copy of the graph each",
                                  "final_loss": float(loss), "seconds": t_train}},
             "parity": parity or None,
             "scheduler": {"learned_wall_s": L["wall_s"], "rule_wall_s": Rr["wall_s"],
@@ -820,11 +846,13 @@ def run_sched(args, w, rank, world, local):
                                            "repeel": int((Rr["methods"] == 2).sum())},
                           "batch_detail": {"fields": ["updates", "hot", "learned_ms", "learned_method",
                                                       "learned_rows_in_place", "rule_ms", "rule_method",
-                                                      "rule_rows_in_place"],
+                                                      "rule_rows_in_place", "learned [apply, core, rows ms, rebuilt, "
+                                                      "captured]", "rule [same]"],
                                            "batches": [[int(ev_sizes[i]), int(hot_batch[i]),
                                                         round(float(L["ms"][i]), 2), int(L["methods"][i]),
                                                         int(L["rows_local"][i]), round(float(Rr["ms"][i]), 2),
-                                                        int(Rr["methods"][i]), int(Rr["rows_local"][i])]
+                                                        int(Rr["methods"][i]), int(Rr["rows_local"][i]),
+                                                        L["phases"][i], Rr["phases"][i]]
                                                        for i in range(len(ev_sizes))]}},
             "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": float(9 * updates / len(ev_sizes)),
                     "d2h_bytes_per_step": 0, "timing": "wall clock of dc_maintain calls with host batches"},
