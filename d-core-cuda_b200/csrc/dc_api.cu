@@ -83,6 +83,41 @@ extern "C" int dc_device_count(int* n) {
     return DC_OK;
 }
 
+extern "C" int dc_reserve_device_memory(int device, uint64_t bytes) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        return set_error(DC_ERR_NO_DEVICE, "dc_reserve_device_memory: no CUDA device");
+    }
+    if (device < 0 || device >= n) return set_error(DC_ERR_INVALID, "dc_reserve_device_memory: bad device %d", device);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    int rc = DC_OK;
+    cudaMemPool_t pool;
+    uint64_t keep = ~0ull;
+    cudaStream_t st = nullptr;
+    void* p = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess ||
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        rc = set_error(DC_ERR_CUDA, "dc_reserve_device_memory: pool setup failed");
+    } else if (bytes) {
+        if (cudaMallocAsync(&p, bytes, st) != cudaSuccess) {
+            rc = set_error(DC_ERR_NOMEM, "dc_reserve_device_memory: %llu bytes not available",
+                           (unsigned long long)bytes);
+        } else {
+            cudaFreeAsync(p, st);
+        }
+        if (cudaStreamSynchronize(st) != cudaSuccess && rc == DC_OK)
+            rc = set_error(DC_ERR_CUDA, "dc_reserve_device_memory: synchronisation failed");
+    }
+    if (st) cudaStreamDestroy(st);
+    cudaGetLastError();
+    cudaSetDevice(cur);
+    return rc;
+}
+
 extern "C" int dc_graph_create_device(uint32_t V, uint64_t E, const uint32_t* d_src, const uint32_t* d_dst,
                                       const dc_graph_opts* opts, dc_graph** out) {
     if (E && (!d_src || !d_dst)) return set_error(DC_ERR_INVALID, "dc_graph_create_device: null edge arrays");

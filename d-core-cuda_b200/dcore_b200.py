@@ -112,6 +112,7 @@ SIGNATURES = {
     "dc_row_weights": [vp, u64p, ctypes.c_uint64],
     "dc_set_row_repair": [vp, ctypes.c_int],
     "dc_set_captured_batches": [vp, ctypes.c_int],
+    "dc_reserve_device_memory": [ctypes.c_int, ctypes.c_uint64],
     "dc_maintain": [vp, u32p, u8p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(MaintStats)],
     "dc_decomp_info_get": [vp, ctypes.POINTER(DecompInfo)],
     "dc_get_kmaxes": [vp, i32p],
@@ -225,6 +226,12 @@ def device_count():
     n = ctypes.c_int(0)
     _check(lib().dc_device_count(ctypes.byref(n)))
     return n.value
+
+
+def reserve_device_memory(device, nbytes):
+    """Grow the device's memory pool (which the engine allocates from) to at
+    least nbytes, so later calls map no new memory."""
+    _check(lib().dc_reserve_device_memory(int(device), int(nbytes)))
 
 
 # ---------------------------------------------------------------- pinned host memory

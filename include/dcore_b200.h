@@ -122,6 +122,14 @@ typedef struct dc_graph_opts {
 void dc_graph_opts_default(dc_graph_opts* opts);
 /* Number of visible CUDA devices (0 when none; never fails). */
 int dc_device_count(int* n);
+/* Grows the device's stream-ordered memory pool -- the engine allocates all
+ * device memory from it and keeps freed blocks there -- to hold at least
+ * `bytes`: allocations inside later calls (a store rebuild, a larger
+ * skyline) then reuse that memory instead of mapping new pages into the
+ * pool, which costs up to hundreds of ms per call for tens of GB.  The memory
+ * stays reserved for the process.  No counterpart in the reference (it
+ * allocates with cudaMalloc per call, src/cuda_memory.h:5-93). */
+int dc_reserve_device_memory(int device, uint64_t bytes);
 
 /* Builds the device CSR (out) + CSC (in) from host edge arrays; the copy to
  * the device is part of the call.  Replaces Graph construction plus

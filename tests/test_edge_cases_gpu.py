@@ -56,3 +56,12 @@ def test_row_repair_mode_validation(dc, gpu):
             g.set_row_repair(4)
         with pytest.raises(dc.DCoreError):
             g.set_row_repair(-1)
+
+
+def test_reserve_device_memory(dc, gpu):
+    dc.reserve_device_memory(0, 1 << 30)  # grows the pool; the memory stays for reuse
+    with pytest.raises(dc.DCoreError):
+        dc.reserve_device_memory(dc.device_count(), 1 << 20)
+    V, s, d = dc.gen_rmat(10, 8, 3)
+    with dc.Graph.from_edges(V, s, d) as g:  # allocations after the reservation work as before
+        g.decompose()
