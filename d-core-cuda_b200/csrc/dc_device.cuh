@@ -98,6 +98,7 @@ struct BatchStatus {
     int run_apply;      // the batch is valid: no missing deletion, insertions fit their free slots
     int run_repair;     // rows 1..R are repaired in place
     int run_merge;      // a new skyline is merged (the repair's changes, or new row-0 corners only)
+    int run_chg;        // the merge reads change lists (the repair logged changes)
     int fallback;       // rows 1..R must be recomputed (repair not expected to pay, or it gave up)
     int merge_overflow; // the merged skyline outgrew its buffer: the host merges instead
     int notfound;       // a deleted edge is not in the graph (nothing applied)

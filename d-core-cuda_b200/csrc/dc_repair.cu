@@ -867,26 +867,46 @@ __global__ void k_chg_sort(uint32_t V, const unsigned long long* off, int32_t* c
 // New skyline of v: corner (0, new row 0), then at every row k <= new kmax
 // where the old skyline has a corner, the change list has an entry, or a
 // change run ends, the new value (change or old value) when it differs from
-// the previous corner's.  FILL = false counts, true writes.
+// the previous corner's.  FILL = false counts, true writes.  Change lists:
+// none when coff is null or *chg_run is 0.  A vertex with no change, the
+// same row 0 and every old corner at or below its kmax keeps its corners as
+// they are (counted from the offsets, copied without the merge walk).
 template <bool FILL>
 __global__ void k_rep_merge(uint32_t V, const int32_t* kmax, const int32_t* row0, const uint32_t* ooff,
                             const int32_t* ok, const int32_t* ol, const uint32_t* coff, const int32_t* ck,
                             const int32_t* cl, unsigned long long* cnt_off, int32_t* nk, int32_t* nl,
-                            uint32_t* noff, const int* run) {
+                            uint32_t* noff, const int* run, const int* chg_run) {
     if (run && !*run) return;
+    const bool chg = coff && (!chg_run || *chg_run);
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
         const int km = kmax[v];
-        uint32_t i = ooff[v], ie = ooff[v + 1];
-        uint32_t j = coff[v], je = coff[v + 1];
+        const uint32_t i0 = ooff[v], ie = ooff[v + 1];
+        uint32_t i = i0;
+        uint32_t j = chg ? coff[v] : 0, je = chg ? coff[v + 1] : 0;
         uint64_t o = FILL ? cnt_off[v] : 0;
         uint64_t c = 0;
         int last = row0[v];
+        int oldv = (i < ie) ? ol[i] : 0;  // old row-0 corner
+        if (j == je && i < ie && oldv == last && ok[ie - 1] <= km) {
+            // unchanged: the old corners as they are
+            c = ie - i0;
+            if (FILL) {
+                for (uint32_t t = 0; t < c; ++t) {
+                    nk[o + t] = ok[i0 + t];
+                    nl[o + t] = ol[i0 + t];
+                }
+                noff[v] = (uint32_t)o;
+                if (v == V - 1) noff[V] = (uint32_t)(o + c);
+            } else {
+                cnt_off[v] = c;
+            }
+            continue;
+        }
         if (FILL) {
             nk[o] = 0;
             nl[o] = last;
         }
         ++c;
-        int oldv = (i < ie) ? ol[i] : 0;  // old row-0 corner
         ++i;
         // row after a change run; a changed row 0 is one (an unchanged row 1
         // keeps its old value, which may now differ from row 0)
@@ -970,6 +990,7 @@ __global__ void k_gb_after_repair(const EngineCtl* c, BatchStatus* st) {
     }
     st->run_merge = 1;
     st->nlog = c->log_count;
+    st->run_chg = st->nlog > 0;
     st->scanned = c->edges_scanned;
 }
 
@@ -1069,24 +1090,27 @@ int apply_change_log(dc_graph* h, uint64_t nlog, bool* applied) {
     uint32_t *coff = nullptr, *fill = s->cursor, *noff = nullptr;
     int32_t *ck = nullptr, *cl = nullptr, *nk = nullptr, *nl = nullptr;
     uint64_t ccap = 0, ncap = 0;
-    int rc = sky_take_spare(h, 0, nlog, &coff, &ck, &cl, &ccap);
+    // (no change lists when only row 0 changed)
+    int rc = nlog ? sky_take_spare(h, 0, nlog, &coff, &ck, &cl, &ccap) : DC_OK;
     unsigned long long total = 0;
-    if (rc == DC_OK) {
+    if (rc == DC_OK && nlog) {
         cudaMemsetAsync(cnt, 0, 8ull * (V + 1), h->stream);
         cudaMemsetAsync(fill, 0, 4ull * V, h->stream);
         g_launches += 3;
-        if (nlog) k_chg_count<<<rgrid(h, nlog), kRThreads, 0, h->stream>>>(nlog, s->log_v, cnt, nullptr, nullptr);
+        k_chg_count<<<rgrid(h, nlog), kRThreads, 0, h->stream>>>(nlog, s->log_v, cnt, nullptr, nullptr);
         rc = scan_tmp64(h, V);
-    }
-    if (rc == DC_OK) {
-        if (nlog)
+        if (rc == DC_OK) {
             k_chg_fill<<<rgrid(h, nlog), kRThreads, 0, h->stream>>>(nlog, s->log_v, s->log_k, s->log_l, cnt, fill, ck,
                                                                     cl, nullptr, nullptr);
-        k_chg_sort<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, cnt, ck, cl, coff, nullptr);
+            k_chg_sort<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, cnt, ck, cl, coff, nullptr);
+        }
+    }
+    if (rc == DC_OK) {
         // new skyline: count, scan, fill
+        ++g_launches;
         k_rep_merge<false><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
                                                                      coff, ck, cl, cnt, nullptr, nullptr, nullptr,
-                                                                     nullptr);
+                                                                     nullptr, nullptr);
         rc = scan_tmp64(h, V);
     }
     if (rc == DC_OK) {
@@ -1100,7 +1124,7 @@ int apply_change_log(dc_graph* h, uint64_t nlog, bool* applied) {
     if (rc == DC_OK) {
         ++g_launches;
         k_rep_merge<true><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
-                                                                    coff, ck, cl, cnt, nk, nl, noff, nullptr);
+                                                                    coff, ck, cl, cnt, nk, nl, noff, nullptr, nullptr);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(DC_ERR_CUDA, "row repair: merge launch failed");
     }
     if (coff || ck) sky_put_spare(h, 0, coff, ck, cl, ccap);
@@ -1313,23 +1337,25 @@ int merge_enqueue(dc_graph* h, BatchStatus* st, uint32_t* coff, int32_t* ck, int
     unsigned long long* cnt = (unsigned long long*)s->tmp64;
     uint32_t* fill = s->cursor;
     const int grid_log = rgrid(h, s->log_cap);
+    // change lists only when the repair logged changes (st->run_chg)
     RP_CUDA(cudaMemsetAsync(cnt, 0, 8ull * (V + 1), h->stream));
     RP_CUDA(cudaMemsetAsync(fill, 0, 4ull * V, h->stream));
     g_launches += 2;
-    k_chg_count<<<grid_log, kRThreads, 0, h->stream>>>(0, s->log_v, cnt, &st->nlog, &st->run_merge);
+    k_chg_count<<<grid_log, kRThreads, 0, h->stream>>>(0, s->log_v, cnt, &st->nlog, &st->run_chg);
     if (int rc = scan_tmp64(h, V)) return rc;
     g_launches += 3;
     k_chg_fill<<<grid_log, kRThreads, 0, h->stream>>>(0, s->log_v, s->log_k, s->log_l, cnt, fill, ck, cl, &st->nlog,
-                                                      &st->run_merge);
-    k_chg_sort<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, cnt, ck, cl, coff, &st->run_merge);
+                                                      &st->run_chg);
+    k_chg_sort<<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, cnt, ck, cl, coff, &st->run_chg);
     k_rep_merge<false><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
                                                                  coff, ck, cl, cnt, nullptr, nullptr, nullptr,
-                                                                 &st->run_merge);
+                                                                 &st->run_merge, &st->run_chg);
     if (int rc = scan_tmp64(h, V)) return rc;
     g_launches += 2;
     k_gb_total<<<1, 1, 0, h->stream>>>(st, cnt, V);
     k_rep_merge<true><<<rgrid(h, V), kRThreads, 0, h->stream>>>(V, d.kmax_v, d.row0, d.sky_off, d.sky_k, d.sky_l,
-                                                                coff, ck, cl, cnt, nk, nl, noff, &st->run_merge);
+                                                                coff, ck, cl, cnt, nk, nl, noff, &st->run_merge,
+                                                                &st->run_chg);
     RP_CUDA(cudaGetLastError());
     return DC_OK;
 }
