@@ -172,22 +172,112 @@ __device__ __forceinline__ void push(St& S, uint32_t w) {
     else if (old == 1u) atomicCAS(&S.st[slot], 1u, 2u);
 }
 
+// Row-k values of up to four vertices at once (rv for each w[q] with
+// ok[q]; -1 elsewhere): the table probes first, then the four binary
+// searches over the old skyline in lockstep, so a lane has four independent
+// chains of loads in flight instead of one.
+template <class St>
+__device__ __forceinline__ void rv4(const RepairParams& p, St& S, const uint32_t w[4], const bool ok[4], int k,
+                                    int out[4]) {
+    uint32_t lo[4], hi[4];
+    int val[4];
+    bool need[4];
+    int km[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) km[q] = ok[q] ? p.kmax_new[w[q]] : -1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        out[q] = -1;
+        need[q] = false;
+        lo[q] = hi[q] = 0;
+        val[q] = 0;
+        if (km[q] < k) continue;
+        const int i = h_slot(S, w[q], false);
+        if (i >= 0) {
+            const int c = vld(&S.cur[i]);
+            if (c != kUnset) {
+                out[q] = c;
+                continue;
+            }
+        }
+        need[q] = true;
+        lo[q] = p.sky_off[w[q]];
+        hi[q] = p.sky_off[w[q] + 1];
+    }
+    for (;;) {
+        bool any = false;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (need[q] && lo[q] < hi[q]) {
+                any = true;
+                const uint32_t m = (lo[q] + hi[q]) >> 1;
+                if (p.sky_k[m] <= k) {
+                    val[q] = p.sky_l[m];
+                    lo[q] = m + 1;
+                } else {
+                    hi[q] = m;
+                }
+            }
+        }
+        if (!any) break;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        if (need[q]) out[q] = val[q];
+}
+
 // Converged warp: one histogram pass over a list for the window [lo, hi];
-// values above hi land in the top bin on the first window only.
+// values above hi land in the top bin on the first window only.  Four
+// entries per lane and step (rv4).
 template <class St>
 __device__ __forceinline__ void r_hist(const RepairParams& p, St& S, const uint32_t* a, int n, int k, int lo,
                                        int hi, bool first, int* bins) {
     const unsigned lane = threadIdx.x & 31u;
     int top = 0;
-    for (int e = (int)lane; e < n; e += 32) {
-        int x = rv(p, S, a[e], k);
-        if (x > hi) top += first;
-        else if (x == hi) ++top;
-        else if (x >= lo) atomicAdd(&bins[x - lo], 1);
+    for (int b = 0; b < n; b += 128) {
+        uint32_t w[4];
+        bool ok[4];
+        int x[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = b + 32 * q + (int)lane;
+            ok[q] = e < n;
+            w[q] = ok[q] ? a[e] : 0;
+        }
+        rv4(p, S, w, ok, k, x);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (!ok[q]) continue;
+            if (x[q] > hi) top += first;
+            else if (x[q] == hi) ++top;
+            else if (x[q] >= lo) atomicAdd(&bins[x[q] - lo], 1);
+        }
     }
 #pragma unroll
     for (int s = 16; s; s >>= 1) top += __shfl_xor_sync(0xFFFFFFFFu, top, s);
     if (lane == 0 && top) atomicAdd(&bins[hi - lo], top);
+}
+
+// Converged warp: how many entries of a list hold at least val (rv4).
+template <class St>
+__device__ __forceinline__ int r_count_at_least(const RepairParams& p, St& S, const uint32_t* a, int n, int k,
+                                                int val) {
+    int cnt = 0;
+    for (int b = 0; b < n; b += 128) {
+        uint32_t w[4];
+        bool ok[4];
+        int x[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = b + 32 * q + (int)(threadIdx.x & 31u);
+            ok[q] = e < n;
+            w[q] = ok[q] ? a[e] : 0;
+        }
+        rv4(p, S, w, ok, k, x);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cnt += ok[q] && x[q] >= val;
+    }
+    return cnt;
 }
 
 // Converged warp, after x dropped from cap to nv (value already written):
@@ -199,11 +289,23 @@ template <class St>
 __device__ __forceinline__ int r_release(const RepairParams& p, St& S, const uint32_t* a, int n, int k, int nv,
                                          int cap) {
     int support = 0;
-    for (int e = (int)(threadIdx.x & 31u); e < n && !vld(&S.abort); e += 32) {
-        uint32_t w = a[e];
-        int x = rv(p, S, w, k);
-        support += x >= nv;
-        if (x > nv && x <= cap) push(S, w);
+    for (int b = 0; b < n && !vld(&S.abort); b += 128) {
+        uint32_t w[4];
+        bool ok[4];
+        int x[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = b + 32 * q + (int)(threadIdx.x & 31u);
+            ok[q] = e < n;
+            w[q] = ok[q] ? a[e] : 0;
+        }
+        rv4(p, S, w, ok, k, x);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (!ok[q]) continue;
+            support += x[q] >= nv;
+            if (x[q] > nv && x[q] <= cap) push(S, w[q]);
+        }
     }
 #pragma unroll
     for (int s = 16; s; s >>= 1) support += __shfl_xor_sync(0xFFFFFFFFu, support, s);
@@ -405,8 +507,8 @@ __global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
                 int so = 0, si = 0;
                 const uint32_t* ao = p.out_nbr + p.out_off[x];
                 const uint32_t* ai = p.in_nbr + p.in_off[x];
-                for (int e = (int)lane; e < p.out_len[x]; e += 32) so += rv(p, S, ao[e], k) >= val;
-                for (int e = (int)lane; e < p.in_len[x]; e += 32) si += rv(p, S, ai[e], k) >= val;
+                so = r_count_at_least(p, S, ao, p.out_len[x], k, val);
+                si = r_count_at_least(p, S, ai, p.in_len[x], k, val);
     #pragma unroll
                 for (int s = 16; s; s >>= 1) {
                     so += __shfl_xor_sync(0xFFFFFFFFu, so, s);
@@ -748,8 +850,8 @@ __global__ void __launch_bounds__(kIThreads) k_row_repair_ins(RepairParams p) {
                 int so = 0, si = 0;
                 const uint32_t* ao = p.out_nbr + p.out_off[x];
                 const uint32_t* ai = p.in_nbr + p.in_off[x];
-                for (int e = (int)lane; e < p.out_len[x]; e += 32) so += rv(p, S, ao[e], k) >= val;
-                for (int e = (int)lane; e < p.in_len[x]; e += 32) si += rv(p, S, ai[e], k) >= val;
+                so = r_count_at_least(p, S, ao, p.out_len[x], k, val);
+                si = r_count_at_least(p, S, ai, p.in_len[x], k, val);
 #pragma unroll
                 for (int s = 16; s; s >>= 1) {
                     so += __shfl_xor_sync(0xFFFFFFFFu, so, s);
