@@ -172,21 +172,21 @@ __device__ __forceinline__ void push(St& S, uint32_t w) {
     else if (old == 1u) atomicCAS(&S.st[slot], 1u, 2u);
 }
 
-// Row-k values of up to four vertices at once (rv for each w[q] with
-// ok[q]; -1 elsewhere): the table probes first, then the four binary
-// searches over the old skyline in lockstep, so a lane has four independent
-// chains of loads in flight instead of one.
-template <class St>
-__device__ __forceinline__ void rv4(const RepairParams& p, St& S, const uint32_t w[4], const bool ok[4], int k,
-                                    int out[4]) {
-    uint32_t lo[4], hi[4];
-    int val[4];
-    bool need[4];
-    int km[4];
+// Row-k values of up to W vertices at once (rv for each w[q] with ok[q];
+// -1 elsewhere): the table probes first, then the W binary searches over the
+// old skyline in lockstep, so a lane has W independent chains of loads in
+// flight instead of one.
+template <int W, class St>
+__device__ __forceinline__ void rvw(const RepairParams& p, St& S, const uint32_t w[W], const bool ok[W], int k,
+                                    int out[W]) {
+    uint32_t lo[W], hi[W];
+    int val[W];
+    bool need[W];
+    int km[W];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) km[q] = ok[q] ? p.kmax_new[w[q]] : -1;
+    for (int q = 0; q < W; ++q) km[q] = ok[q] ? p.kmax_new[w[q]] : -1;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < W; ++q) {
         out[q] = -1;
         need[q] = false;
         lo[q] = hi[q] = 0;
@@ -207,7 +207,7 @@ __device__ __forceinline__ void rv4(const RepairParams& p, St& S, const uint32_t
     for (;;) {
         bool any = false;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < W; ++q) {
             if (need[q] && lo[q] < hi[q]) {
                 any = true;
                 const uint32_t m = (lo[q] + hi[q]) >> 1;
@@ -222,31 +222,32 @@ __device__ __forceinline__ void rv4(const RepairParams& p, St& S, const uint32_t
         if (!any) break;
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < W; ++q)
         if (need[q]) out[q] = val[q];
 }
+constexpr int kRv = 8;  // lookups per lane in flight
 
 // Converged warp: one histogram pass over a list for the window [lo, hi];
-// values above hi land in the top bin on the first window only.  Four
-// entries per lane and step (rv4).
+// values above hi land in the top bin on the first window only.  kRv
+// entries per lane and step (rvw).
 template <class St>
 __device__ __forceinline__ void r_hist(const RepairParams& p, St& S, const uint32_t* a, int n, int k, int lo,
                                        int hi, bool first, int* bins) {
     const unsigned lane = threadIdx.x & 31u;
     int top = 0;
-    for (int b = 0; b < n; b += 128) {
-        uint32_t w[4];
-        bool ok[4];
-        int x[4];
+    for (int b = 0; b < n; b += 32 * kRv) {
+        uint32_t w[kRv];
+        bool ok[kRv];
+        int x[kRv];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kRv; ++q) {
             const int e = b + 32 * q + (int)lane;
             ok[q] = e < n;
             w[q] = ok[q] ? a[e] : 0;
         }
-        rv4(p, S, w, ok, k, x);
+        rvw<kRv>(p, S, w, ok, k, x);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kRv; ++q) {
             if (!ok[q]) continue;
             if (x[q] > hi) top += first;
             else if (x[q] == hi) ++top;
@@ -258,24 +259,24 @@ __device__ __forceinline__ void r_hist(const RepairParams& p, St& S, const uint3
     if (lane == 0 && top) atomicAdd(&bins[hi - lo], top);
 }
 
-// Converged warp: how many entries of a list hold at least val (rv4).
+// Converged warp: how many entries of a list hold at least val (rvw).
 template <class St>
 __device__ __forceinline__ int r_count_at_least(const RepairParams& p, St& S, const uint32_t* a, int n, int k,
                                                 int val) {
     int cnt = 0;
-    for (int b = 0; b < n; b += 128) {
-        uint32_t w[4];
-        bool ok[4];
-        int x[4];
+    for (int b = 0; b < n; b += 32 * kRv) {
+        uint32_t w[kRv];
+        bool ok[kRv];
+        int x[kRv];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kRv; ++q) {
             const int e = b + 32 * q + (int)(threadIdx.x & 31u);
             ok[q] = e < n;
             w[q] = ok[q] ? a[e] : 0;
         }
-        rv4(p, S, w, ok, k, x);
+        rvw<kRv>(p, S, w, ok, k, x);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) cnt += ok[q] && x[q] >= val;
+        for (int q = 0; q < kRv; ++q) cnt += ok[q] && x[q] >= val;
     }
     return cnt;
 }
@@ -289,19 +290,19 @@ template <class St>
 __device__ __forceinline__ int r_release(const RepairParams& p, St& S, const uint32_t* a, int n, int k, int nv,
                                          int cap) {
     int support = 0;
-    for (int b = 0; b < n && !vld(&S.abort); b += 128) {
-        uint32_t w[4];
-        bool ok[4];
-        int x[4];
+    for (int b = 0; b < n && !vld(&S.abort); b += 32 * kRv) {
+        uint32_t w[kRv];
+        bool ok[kRv];
+        int x[kRv];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kRv; ++q) {
             const int e = b + 32 * q + (int)(threadIdx.x & 31u);
             ok[q] = e < n;
             w[q] = ok[q] ? a[e] : 0;
         }
-        rv4(p, S, w, ok, k, x);
+        rvw<kRv>(p, S, w, ok, k, x);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kRv; ++q) {
             if (!ok[q]) continue;
             support += x[q] >= nv;
             if (x[q] > nv && x[q] <= cap) push(S, w[q]);
@@ -351,7 +352,7 @@ __device__ bool r_take(const RepairParams& p, St& S, unsigned* slot) {
     return state == 1;
 }
 
-__global__ void __launch_bounds__(kRThreads) k_row_repair(RepairParams p) {
+__global__ void __launch_bounds__(kRThreads, 1) k_row_repair(RepairParams p) {
     if (p.run && !*p.run) return;
     const int32_t R = p.R_dev ? *p.R_dev : p.R;
     const uint32_t n_leave = p.n_leave_dev ? *p.n_leave_dev : p.n_leave;
@@ -688,7 +689,7 @@ __device__ int r_eval(const RepairParams& p, St& S, uint32_t x, int k, int cap, 
     }
 }
 
-__global__ void __launch_bounds__(kIThreads) k_row_repair_ins(RepairParams p) {
+__global__ void __launch_bounds__(kIThreads, 1) k_row_repair_ins(RepairParams p) {
     if (p.run && !*p.run) return;
     const int32_t R = p.R_dev ? *p.R_dev : p.R;
     const uint32_t n_leave = p.n_leave_dev ? *p.n_leave_dev : p.n_leave;
