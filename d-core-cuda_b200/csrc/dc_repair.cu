@@ -96,6 +96,21 @@ struct RowStateT {
     int abort;  // table full, a wait ran out, or (insertions) the scan budget is spent
     int k;
     int hist[NW][2][kRWin];
+    // one list scan shared by the block's idle warps (a hub's list): the
+    // owner posts it, every warp waiting for work claims chunks of it
+    unsigned job_busy;            // 0 free, 1 posted
+    unsigned job_id;              // bumped per posted scan
+    unsigned long long job_ctr;   // (job id << 32) | next chunk to claim
+    unsigned job_done;            // chunks finished
+    int job_support;              // release scans: neighbours at or above nv
+    const uint32_t* job_a;
+    int job_n, job_kind, job_k, job_lo, job_hi, job_first, job_nv, job_cap;
+    unsigned job_nchunks;
+    int* job_bins;
+    // re-check sweep: hubs checked by the whole block after the others
+    unsigned nbig;
+    uint32_t bigv[32];
+    int big_so, big_si;
 };
 using RowState = RowStateT<kRWarps>;
 
@@ -313,43 +328,233 @@ __device__ __forceinline__ int r_release(const RepairParams& p, St& S, const uin
     return support;
 }
 
+// ---- list scans shared by the block -------------------------------------
+// A hub's lists hold up to ~10^5 entries; one warp scanning them leaves the
+// block's other warps idle in the queue.  A warp about to scan a list longer
+// than kHubMin posts the scan in the block's job slot instead; warps waiting
+// for work claim chunks of it (r_take), the owner claims chunks too and then
+// waits until every chunk is done.  A chunk is claimed by a CAS on
+// (job id, next chunk), so a warp that read an older job's fields can never
+// claim a chunk of a newer one; the owner reuses the slot only after all
+// chunks of its job are done, so no claimer still reads its fields.
+constexpr int kHubMin = 4096;
+constexpr int kChunk = 2048;
+
+// Converged warp: chunk [c0, c1) of the posted scan.  kind 0: histogram of
+// the window [lo, hi] into bins (r_hist); kind 1: release (r_release), the
+// support count added to job_support.
+template <class St>
+__device__ void job_chunk(const RepairParams& p, St& S, int kind, const uint32_t* a, int c0, int c1, int k, int lo,
+                          int hi, bool first, int nv, int cap, int* bins) {
+    const unsigned lane = threadIdx.x & 31u;
+    int acc = 0;  // histogram: top-bin count; release: support
+    for (int b = c0; b < c1 && !vld(&S.abort); b += 32 * kRv) {
+        uint32_t w[kRv];
+        bool ok[kRv];
+        int x[kRv];
+#pragma unroll
+        for (int q = 0; q < kRv; ++q) {
+            const int e = b + 32 * q + (int)lane;
+            ok[q] = e < c1;
+            w[q] = ok[q] ? a[e] : 0;
+        }
+        rvw<kRv>(p, S, w, ok, k, x);
+#pragma unroll
+        for (int q = 0; q < kRv; ++q) {
+            if (!ok[q]) continue;
+            if (kind == 0) {
+                if (x[q] > hi) acc += first;
+                else if (x[q] == hi) ++acc;
+                else if (x[q] >= lo) atomicAdd(&bins[x[q] - lo], 1);
+            } else {
+                acc += x[q] >= nv;
+                if (x[q] > nv && x[q] <= cap) push(S, w[q]);
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 16; s; s >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, s);
+    if (lane == 0 && acc) {
+        if (kind == 0) atomicAdd(&bins[hi - lo], acc);
+        else atomicAdd(&S.job_support, acc);
+    }
+}
+
+// Converged warp: claims and scans chunks of the posted job until none is
+// left.
+template <class St>
+__device__ void job_help(const RepairParams& p, St& S) {
+    const unsigned lane = threadIdx.x & 31u;
+    for (;;) {
+        int chunk = -1;
+        unsigned long long aptr = 0;
+        int n = 0, kind = 0, k = 0, lo = 0, hi = 0, first = 0, nv = 0, cap = 0;
+        unsigned long long bptr = 0;
+        if (lane == 0 && vldu(&S.job_busy)) {
+            const unsigned id = vldu(&S.job_id);
+            __threadfence_block();
+            aptr = (unsigned long long)*(const uint32_t* volatile*)&S.job_a;
+            n = vld(&S.job_n);
+            kind = vld(&S.job_kind);
+            k = vld(&S.job_k);
+            lo = vld(&S.job_lo);
+            hi = vld(&S.job_hi);
+            first = vld(&S.job_first);
+            nv = vld(&S.job_nv);
+            cap = vld(&S.job_cap);
+            bptr = (unsigned long long)*(int* volatile*)&S.job_bins;
+            const unsigned nch = vldu(&S.job_nchunks);
+            __threadfence_block();
+            for (int tries = 0; tries < 64; ++tries) {
+                const unsigned long long c = *(volatile unsigned long long*)&S.job_ctr;
+                if ((unsigned)(c >> 32) != id || (unsigned)c >= nch) break;
+                if (atomicCAS(&S.job_ctr, c, c + 1) == c) {
+                    chunk = (int)(unsigned)c;
+                    break;
+                }
+            }
+        }
+        chunk = __shfl_sync(0xFFFFFFFFu, chunk, 0);
+        if (chunk < 0) return;
+        aptr = __shfl_sync(0xFFFFFFFFu, aptr, 0);
+        bptr = __shfl_sync(0xFFFFFFFFu, bptr, 0);
+        n = __shfl_sync(0xFFFFFFFFu, n, 0);
+        kind = __shfl_sync(0xFFFFFFFFu, kind, 0);
+        k = __shfl_sync(0xFFFFFFFFu, k, 0);
+        lo = __shfl_sync(0xFFFFFFFFu, lo, 0);
+        hi = __shfl_sync(0xFFFFFFFFu, hi, 0);
+        first = __shfl_sync(0xFFFFFFFFu, first, 0);
+        nv = __shfl_sync(0xFFFFFFFFu, nv, 0);
+        cap = __shfl_sync(0xFFFFFFFFu, cap, 0);
+        const int c0 = chunk * kChunk, c1 = min(n, c0 + kChunk);
+        job_chunk(p, S, kind, (const uint32_t*)aptr, c0, c1, k, lo, hi, first != 0, nv, cap, (int*)bptr);
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            atomicAdd(&S.job_done, 1u);
+        }
+    }
+}
+
+// A posted job with chunks left to claim (a hint; the claim decides).
+template <class St>
+__device__ __forceinline__ bool job_open(St& S) {
+    if (!vldu(&S.job_busy)) return false;
+    const unsigned long long c = *(volatile unsigned long long*)&S.job_ctr;
+    return (unsigned)(c >> 32) == vldu(&S.job_id) && (unsigned)c < vldu(&S.job_nchunks);
+}
+
+// Converged warp: a scan of list a (kind 0 histogram, kind 1 release) shared
+// with the block's idle warps when the list is long and the job slot free,
+// else scanned alone.  Returns the release's support count (kind 1).
+template <class St>
+__device__ int scan_shared(const RepairParams& p, St& S, int kind, const uint32_t* a, int n, int k, int lo, int hi,
+                           bool first, int nv, int cap, int* bins) {
+    const unsigned lane = threadIdx.x & 31u;
+    bool mine = false;
+    if (n > kHubMin) {
+        if (lane == 0) mine = atomicCAS(&S.job_busy, 0u, 1u) == 0u;
+        mine = __shfl_sync(0xFFFFFFFFu, mine, 0);
+    }
+    if (!mine) {
+        if (kind == 0) {
+            r_hist(p, S, a, n, k, lo, hi, first, bins);
+            return 0;
+        }
+        return r_release(p, S, a, n, k, nv, cap);
+    }
+    const unsigned nch = (unsigned)((n + kChunk - 1) / kChunk);
+    if (lane == 0) {
+        S.job_a = a;
+        S.job_n = n;
+        S.job_kind = kind;
+        S.job_k = k;
+        S.job_lo = lo;
+        S.job_hi = hi;
+        S.job_first = first;
+        S.job_nv = nv;
+        S.job_cap = cap;
+        S.job_bins = bins;
+        S.job_nchunks = nch;
+        S.job_done = 0;
+        S.job_support = 0;
+        const unsigned id = S.job_id + 1;
+        __threadfence_block();
+        *(volatile unsigned*)&S.job_id = id;
+        __threadfence_block();
+        atomicExch(&S.job_ctr, (unsigned long long)id << 32);
+    }
+    __syncwarp();
+    job_help(p, S);  // the owner scans chunks too
+    int support = 0;
+    if (lane == 0) {
+        const unsigned long long t0 = gtimer();
+        for (unsigned spins = 0; vldu(&S.job_done) < nch; ++spins) {
+            if ((spins & 63) == 63 && gtimer() - t0 > wait_limit(p.ctl)) {
+                set_dev_error(p.ctl, DC_DEV_ERR_TIMEOUT, 43);
+                atomicExch(&S.abort, 1);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence_block();
+        support = vld(&S.job_support);
+        atomicExch(&S.job_busy, 0u);
+    }
+    __syncwarp();
+    return __shfl_sync(0xFFFFFFFFu, support, 0);
+}
+
 // Converged warp: takes a queued slot; false when the row is finished or
 // abandoned.
 template <class St>
 __device__ bool r_take(const RepairParams& p, St& S, unsigned* slot) {
     const unsigned lane = threadIdx.x & 31u;
-    int state = 0;
-    unsigned got = 0;
-    if (lane == 0) {
-        unsigned t = atomicAdd(&S.qhead, 1u);
-        volatile uint32_t* cell = (volatile uint32_t*)&S.ring[t & (kHash - 1)];
-        unsigned long long t0 = 0;
-        for (unsigned spins = 0;; ++spins) {
-            uint32_t it = *cell;
-            if (it != kEmptySlot) {
-                *cell = kEmptySlot;
-                got = it;
-                state = 1;
-                break;
+    unsigned t = 0;
+    if (lane == 0) t = atomicAdd(&S.qhead, 1u);
+    unsigned long long t0 = 0;
+    unsigned spins = 0;
+    for (;;) {
+        int state = 0;  // 1 item, 2 row finished or abandoned, 3 help with a shared scan
+        unsigned got = 0;
+        if (lane == 0) {
+            volatile uint32_t* cell = (volatile uint32_t*)&S.ring[t & (kHash - 1)];
+            for (;; ++spins) {
+                uint32_t it = *cell;
+                if (it != kEmptySlot) {
+                    *cell = kEmptySlot;
+                    got = it;
+                    state = 1;
+                    break;
+                }
+                if (vld(&S.out) == 0 || vld(&S.abort) || ld_vol(&p.ctl->error)) {
+                    state = 2;
+                    break;
+                }
+                if (job_open(S)) {
+                    state = 3;
+                    spins = 0;  // helping is progress: the wait's clock restarts
+                    break;
+                }
+                if (spins == 64) t0 = gtimer();
+                if (spins > 64 && (spins & 63) == 0 && gtimer() - t0 > wait_limit(p.ctl)) {
+                    set_dev_error(p.ctl, DC_DEV_ERR_TIMEOUT, 40);
+                    atomicExch(&S.abort, 1);
+                    state = 2;
+                    break;
+                }
+                if (spins > 16) __nanosleep(64);
             }
-            if (vld(&S.out) == 0 || vld(&S.abort) || ld_vol(&p.ctl->error)) {
-                state = 2;
-                break;
-            }
-            if (spins == 64) t0 = gtimer();
-            if (spins > 64 && (spins & 63) == 0 && gtimer() - t0 > wait_limit(p.ctl)) {
-                set_dev_error(p.ctl, DC_DEV_ERR_TIMEOUT, 40);
-                atomicExch(&S.abort, 1);
-                state = 2;
-                break;
-            }
-            if (spins > 16) __nanosleep(64);
         }
+        state = __shfl_sync(0xFFFFFFFFu, state, 0);
+        if (state == 3) {
+            job_help(p, S);
+            continue;
+        }
+        *slot = __shfl_sync(0xFFFFFFFFu, got, 0);
+        __threadfence_block();
+        return state == 1;
     }
-    state = __shfl_sync(0xFFFFFFFFu, state, 0);
-    *slot = __shfl_sync(0xFFFFFFFFu, got, 0);
-    __threadfence_block();
-    return state == 1;
 }
 
 __global__ void __launch_bounds__(kRThreads, 1) k_row_repair(RepairParams p) {
@@ -363,6 +568,12 @@ __global__ void __launch_bounds__(kRThreads, 1) k_row_repair(RepairParams p) {
     const unsigned long long t_start = gtimer();
     int* ho = S.hist[wib][0];
     int* hi_ = S.hist[wib][1];
+    if (threadIdx.x == 0) {
+        S.job_busy = 0;
+        S.job_id = 0;
+        S.job_ctr = 0;
+        S.job_nchunks = 0;
+    }
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) S.k = ld_vol(&p.ctl->error) ? R + 1 : atomicAdd(&p.ctl->level, 1) + 1;
@@ -432,8 +643,8 @@ __global__ void __launch_bounds__(kRThreads, 1) k_row_repair(RepairParams p) {
                         hi_[lane] = 0;
                         hi_[lane + 32] = 0;
                         __syncwarp();
-                        r_hist(p, S, ao, no, k, lo, hi, first, ho);
-                        r_hist(p, S, ai, ni, k, lo, hi, first, hi_);
+                        scan_shared(p, S, 0, ao, no, k, lo, hi, first, 0, 0, ho);
+                        scan_shared(p, S, 0, ai, ni, k, lo, hi, first, 0, 0, hi_);
                         __syncwarp();
                         int found = -1;
                         if (lane == 0) {
@@ -465,8 +676,8 @@ __global__ void __launch_bounds__(kRThreads, 1) k_row_repair(RepairParams p) {
                         if (lane == 0) atomicExch(&S.cur[slot], nv);
                         __syncwarp();
                         __threadfence_block();
-                        const int so = r_release(p, S, ao, no, k, nv, cap);
-                        const int si = r_release(p, S, ai, ni, k, nv, cap);
+                        const int so = scan_shared(p, S, 1, ao, no, k, 0, 0, false, nv, cap, nullptr);
+                        const int si = scan_shared(p, S, 1, ai, ni, k, 0, 0, false, nv, cap, nullptr);
                         // a neighbour fell below nv meanwhile: evaluate x again
                         if (lane == 0 && nv >= 1 && (so < nv || si < k)) atomicCAS(&S.st[slot], 1u, 2u);
                     }
@@ -498,6 +709,7 @@ __global__ void __launch_bounds__(kRThreads, 1) k_row_repair(RepairParams p) {
                 S.k = 0;    // vertices found unstable
             }
             for (int i = threadIdx.x; i < kHash; i += kRThreads) S.ring[i] = kEmptySlot;
+            if (threadIdx.x == 0) S.nbig = 0;
             __syncthreads();
             for (int i = wib; i < kHash; i += kRWarps) {
                 const uint32_t x = S.key[i];
@@ -505,6 +717,16 @@ __global__ void __launch_bounds__(kRThreads, 1) k_row_repair(RepairParams p) {
                 int val = S.cur[i];
                 if (val == kUnset) val = sky_at(p, x, k);
                 if (val < 1) continue;
+                // a hub is checked by the whole block below (up to 32 per sweep)
+                if (p.out_len[x] + p.in_len[x] > 2 * kHubMin) {
+                    unsigned b = 0;
+                    if (lane == 0) b = atomicAdd(&S.nbig, 1u);
+                    b = __shfl_sync(0xFFFFFFFFu, b, 0);
+                    if (b < 32u) {
+                        if (lane == 0) S.bigv[b] = (uint32_t)i;
+                        continue;
+                    }
+                }
                 int so = 0, si = 0;
                 const uint32_t* ao = p.out_nbr + p.out_off[x];
                 const uint32_t* ai = p.in_nbr + p.in_off[x];
@@ -521,6 +743,47 @@ __global__ void __launch_bounds__(kRThreads, 1) k_row_repair(RepairParams p) {
                 }
             }
             __syncthreads();
+            const unsigned nbig = min(S.nbig, 32u);
+            for (unsigned bi = 0; bi < nbig; ++bi) {
+                const uint32_t slot = S.bigv[bi];
+                const uint32_t x = S.key[slot];
+                int val = S.cur[slot];
+                if (val == kUnset) val = sky_at(p, x, k);
+                if (threadIdx.x == 0) {
+                    S.big_so = 0;
+                    S.big_si = 0;
+                }
+                __syncthreads();
+                // every warp counts its share of both lists
+                for (int side = 0; side < 2; ++side) {
+                    const uint32_t* a = side ? p.in_nbr + p.in_off[x] : p.out_nbr + p.out_off[x];
+                    const int n = side ? p.in_len[x] : p.out_len[x];
+                    int cnt = 0;
+                    for (int b = (int)wib * 32 * kRv; b < n; b += kRWarps * 32 * kRv) {
+                        uint32_t w[kRv];
+                        bool ok[kRv];
+                        int xv[kRv];
+#pragma unroll
+                        for (int q = 0; q < kRv; ++q) {
+                            const int e = b + 32 * q + (int)lane;
+                            ok[q] = e < n;
+                            w[q] = ok[q] ? a[e] : 0;
+                        }
+                        rvw<kRv>(p, S, w, ok, k, xv);
+#pragma unroll
+                        for (int q = 0; q < kRv; ++q) cnt += ok[q] && xv[q] >= val;
+                    }
+#pragma unroll
+                    for (int s = 16; s; s >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, s);
+                    if (lane == 0 && cnt) atomicAdd(side ? &S.big_si : &S.big_so, cnt);
+                }
+                __syncthreads();
+                if (threadIdx.x == 0 && (S.big_so < val || S.big_si < k)) {
+                    atomicAdd(&S.k, 1);
+                    push(S, x);
+                }
+                __syncthreads();
+            }
             const bool again = S.k != 0;
             __syncthreads();
             if (threadIdx.x == 0) S.k = k;
@@ -710,6 +973,10 @@ __global__ void __launch_bounds__(kIThreads, 1) k_row_repair_ins(RepairParams p)
     if (threadIdx.x == 0) {
         S.used = 0;
         S.abort = 0;
+        S.job_busy = 0;  // no shared scans in this kernel
+        S.job_id = 0;
+        S.job_ctr = 0;
+        S.job_nchunks = 0;
         I.scanned = 0;
         I.pused = 0;
     }
